@@ -1,0 +1,381 @@
+"""Benchmark: batched smdisk + PSF/LSF + chi^2 cube evaluations per second on B200.
+
+Workload (the batched objective configuration): 512 parameter sets of a thin
+smooth disk with 30 radial nodes (node-wise surface brightness exp(N(0,0.5)),
+rotation ~U(50,300) km/s, dispersion ~U(5,40) km/s; incl ~U(20,80),
+PA ~U(0,360)), each evaluated on a 128x128x96 cube (10 km/s channels),
+convolved with a Gaussian PSF (FWHM 3 px) x Gaussian LSF (FWHM 1.5 channels)
+and scored with chi^2 against a seeded synthetic data cube with Gaussian noise
+of sigma = 2% of the peak.  Synthetic data (no datasets).
+
+A step is one evaluation of all 512 sets.  `value` is evals/s with the
+parameter sets resident in HBM; `e2e` is the same through the public API
+(host parameter dicts -> packing -> pinned H2D -> chi^2 D2H).  With
+--gpus N (torchrun) every rank evaluates its own 512 sets (weak scaling).
+
+--impl reference times the reference's own CPU implementation of the path
+(its smdisk/residual templates compiled with OpenMP in oracle/_ref, with
+scipy's FFT standing in for FFTW, which is not installed) on the host cores.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "smdisk+PSF/LSF cube evals/s (batched, 512 sets, 128x128x96)"
+UNIT = "evals/s"
+
+
+def staged_bytes_per_eval(geom):
+    """Algorithmic bytes of one staged evaluation with the reference padding
+    P: 12 V(P) + 40 C(P) + 12 V(N) + 4 (model write, r2c, spectrum multiply,
+    c2r, crop + data + error reads, chi^2)."""
+    px, py, pz = geom.size_hi
+    vp = px * py * pz
+    cp = (px // 2 + 1) * py * pz
+    vn = int(np.prod(geom.size))
+    return 12 * vp + 40 * cp + 12 * vn + 4
+
+
+def fft_flops_per_eval(geom):
+    px, py, pz = geom.size_hi
+    vp = px * py * pz
+    cp = (px // 2 + 1) * py * pz
+    return 2 * 2.5 * vp * np.log2(vp) + 6 * cp
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.FIELDS}',
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=['nvidia-smi unavailable'])
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(n)
+        return dict(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=smax,
+                    reasons=sorted(reasons), samples=len(sm))
+
+
+def peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d['hbm_gbs'], 'measured'
+    return 6650.0, 'fallback'
+
+
+def setup_dist(args):
+    import torch
+    import torch.distributed as dist
+    rank, world = int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device('cuda', local))
+    torch.cuda.set_device(local)
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def autotune(w, data, err, nsets, budget_s=60.0):
+    """Time candidate pipeline shapes (chunk, rows per K1 group, FFT grid);
+    returns the fastest configuration."""
+    import torch
+    from gbkfit_b200.autotune import tune_batched
+    return tune_batched(w, data, err, nsets, budget_s=budget_s)
+
+
+def run_b200(args):
+    import torch
+    from gbkfit_b200 import workloads
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    rank, world, local = setup_dist(args)
+    nsets = args.nsets
+    w = workloads.smdisk_batch128(nsets=nsets, seed=1234 + rank)
+    data, err, _ = synthetic_data(w, device=local)
+    cfg = autotune(w, data, err, nsets, budget_s=args.tune_budget) if args.tune else {}
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
+    bufs = ev.alloc_inputs(nsets)
+    ev.upload(ev.pack(w.params, nsets), bufs, nsets)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+    use_graph = not args.no_graph
+    if use_graph:
+        ev.capture(bufs, nsets)
+        run = ev.replay
+    else:
+        run = lambda: ev.evaluate_device(bufs, nsets)
+    for _ in range(args.warmup):
+        run()
+    torch.cuda.synchronize()
+    barrier(world)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    barrier(world)
+    for i in range(args.steps):
+        flush.fill_(float(i))            # evict L2 between timed steps
+        ev0[i].record(stream)
+        run()
+        ev1[i].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
+    ms_step = max_over_ranks(float(np.mean(ms)), world)
+    value = world * nsets / (ms_step / 1e3)
+    chi2 = ev.chi2[:nsets].cpu().numpy()
+    assert np.all(np.isfinite(chi2)) and np.all(chi2 > 0)
+
+    # end to end through the public API: host dicts -> pinned H2D -> chi^2 D2H
+    ev_api = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
+    packed = ev_api.pack(w.params, nsets)
+    h2d = int(sum(v.nbytes for v in packed.values()))
+    d2h = nsets * 4
+    for _ in range(max(1, args.warmup)):
+        ev_api.evaluate(w.params, nsets)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ev_api.evaluate(w.params, nsets)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, world)
+    e2e = dict(value=world * nsets / e2e_s, unit=UNIT, h2d_bytes_per_step=h2d,
+               d2h_bytes_per_step=d2h, ms_per_step=e2e_s * 1e3)
+
+    out = None
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        b_eval = staged_bytes_per_eval(w.geom)
+        achieved = b_eval * nsets / (ms_step / 1e3) / 1e9
+        n_chunks = (nsets + ev.chunk - 1) // ev.chunk
+        plain = plain_per_call(w, data, err) if args.plain else None
+        cpu = cpu_baseline(w, data, err) if args.cpu_baseline else None
+        out = dict(
+            metric=METRIC, value=round(value, 1), unit=UNIT, n_gpus=world, steps=args.steps,
+            warmup=args.warmup, ms_per_step=round(ms_step, 4), higher_is_better=True,
+            scaling='weak', vs_baseline=None, dtype='f32', data='synthetic',
+            config=dict(workload='smdisk_batch128: 512 sets x 128x128x96 cube, 30 rings, '
+                                 'Gaussian PSF FWHM 3 px x Gaussian LSF FWHM 1.5 ch, chi^2',
+                        nsets_per_gpu=nsets, fft_grid=list(ev.fft_size), chunk=ev.chunk,
+                        tuned=cfg, cuda_graph=use_graph, l2='flushed between steps (256 MB write)',
+                        parallelism=f'dp{world} (independent parameter sets per GPU)'),
+            e2e=e2e,
+            roofline=dict(bound='hbm', achieved=round(achieved, 1), peak=hbm,
+                          unit='GB/s', frac=round(achieved / hbm, 3), traffic=None,
+                          peak_kind=peak_kind,
+                          basis=f'staged algorithmic bytes per evaluation ({b_eval} B, '
+                                f'reference padding {list(w.geom.size_hi)}) x 512 / step time',
+                          fp32_tflops=round(fft_flops_per_eval(w.geom) * nsets
+                                            / (ms_step / 1e3) / 1e12, 2)),
+            clocks=clocks,
+            gpu_launches=args.steps * (5 * n_chunks + 1),
+            plain_per_call=plain,
+            cpu_baseline=cpu,
+        )
+    if world > 1:
+        import torch.distributed as dist
+        ev._graph = None
+        dist.destroy_process_group()
+    return out
+
+
+def plain_per_call(w, data, err, nsets=16):
+    """The reference-style per-call path on the GPU: one synchronous
+    DModelSCube evaluation + Objective.log_likelihood per parameter set."""
+    import torch
+    from gbkfit_b200 import model as M, workloads
+    from gbkfit_b200.driver import DriverB200
+    drv = DriverB200(torch.cuda.current_device())
+    comp = M.SpectralSMDisk2D(False, False, w.disk.traits['rpt'], w.disk.traits['vpt'],
+                              w.disk.traits['dpt'], rnodes=w.disk.rnodes)
+    g = w.geom
+    dm = M.DModelSCube(g.size, g.step, rpix=(0, 0, (g.size[2] - 1) / 2), rval=(0, 0, 0),
+                       psf=g.psf, lsf=g.lsf)
+    obj = M.Objective(M.Model(drv, dm, M.GModelKinematics2D([comp])), data, err)
+    for i in range(3):
+        obj.log_likelihood(workloads.set_params(w, i))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(nsets):
+        obj.log_likelihood(workloads.set_params(w, i % w.nsets))
+    dt = time.perf_counter() - t0
+    return dict(value=round(nsets / dt, 1), unit=UNIT, sets=nsets,
+                path='DModelSCube + Objective.log_likelihood, one synchronous call chain per set')
+
+
+def reference_eval(ref, w, data, err, i, workers):
+    """One evaluation with the reference's own CPU code: smdisk and the
+    residual/sum from oracle/_ref, FFT convolution with scipy (FFTW stand-in)."""
+    from oracle.oracle import fft_convolve_cached
+    from gbkfit_b200 import workloads
+    g = w.geom
+    p = w.disk.pack(workloads.set_params(w, i))
+    ss, st, sz = g.spat(False)
+    nz = g.size_hi[2]
+    geo = dict(loose=False, tilted=False, spat_size=ss, spat_step=st, spat_zero=sz,
+               spec_size=nz, spec_step=g.step[2], spec_zero=g.zero_hi[2], opacity=None)
+    cube = np.zeros((nz, ss[1], ss[0]), np.float32)
+    ref.smdisk_evaluate(p, geo, dict(scube=cube))
+    conv = fft_convolve_cached(cube, w._pcube, dtype=np.float32, workers=workers)
+    ex, ey, ez = g.edge
+    nx, ny, nzl = g.size
+    crop = np.ascontiguousarray(conv[ez:ez + nzl, ey:ey + ny, ex:ex + nx], np.float32)
+    res = ref.residual(data, err, None, crop, None, None, 1.0)
+    return ref.residual_sum(res, True)
+
+
+def cpu_baseline(w, data, err, sample_sets=4):
+    """Bounded sample of the workload on the reference CPU path."""
+    from oracle.oracle import Reference, build
+    if not Reference.available():
+        build()
+    ref = Reference()
+    workers = os.cpu_count()
+    w._pcube = w.geom.pcube(np.float32)
+    reference_eval(ref, w, data, err, 0, workers)
+    t0 = time.perf_counter()
+    for i in range(sample_sets):
+        reference_eval(ref, w, data, err, i, workers)
+    dt = time.perf_counter() - t0
+    return dict(value=round(sample_sets / dt, 2), unit=UNIT, cores=ref.num_threads(),
+                kind='reference',
+                sample=f'{sample_sets} of the 512 parameter sets; smdisk and residual sum '
+                       f'from the reference templates (OpenMP, {ref.num_threads()} threads), '
+                       f'FFT convolution with scipy.fft ({workers} workers) standing in for '
+                       f'FFTW on the reference padded grid {list(w.geom.size_hi)}')
+
+
+def run_reference(args):
+    rank, world = int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1))
+    if rank != 0:
+        return None
+    from gbkfit_b200 import workloads
+    from oracle.oracle import Reference, build, scube_pipeline
+    if not Reference.available():
+        build()
+    ref = Reference()
+    w = workloads.smdisk_batch128(nsets=args.nsets)
+    # data: the fp64 oracle model of the truth parameters plus the seeded noise
+    truth = w.disk.pack(w.extra['truth'])
+    m = scube_pipeline(truth, w.geom)
+    rng = np.random.default_rng(w.extra['noise_seed'])
+    sigma = w.extra['noise_frac'] * float(np.max(m))
+    data = (m + rng.normal(0.0, sigma, m.shape)).astype(np.float32)
+    err = np.full(m.shape, sigma, np.float32)
+    workers = os.cpu_count()
+    w._pcube = w.geom.pcube(np.float32)
+    per_step = 2
+    for i in range(args.warmup):
+        reference_eval(ref, w, data, err, i, workers)
+    t0 = time.perf_counter()
+    k = 0
+    for s in range(args.steps):
+        for j in range(per_step):
+            reference_eval(ref, w, data, err, k % args.nsets, workers)
+            k += 1
+    dt = time.perf_counter() - t0
+    value = k / dt
+    cpu = dict(value=round(value, 2), unit=UNIT, cores=ref.num_threads(), kind='reference',
+               sample=f'{per_step} parameter sets per step of the 512-set workload')
+    return dict(metric=METRIC, value=round(value, 2), unit=UNIT, n_gpus=world,
+                steps=args.steps, warmup=args.warmup,
+                ms_per_step=round(dt / args.steps * 1e3, 2), higher_is_better=True,
+                scaling='weak', vs_baseline=None, dtype='f32', data='synthetic',
+                config=dict(workload='smdisk_batch128: 512 sets x 128x128x96 cube, 30 rings, '
+                                     'Gaussian PSF FWHM 3 px x Gaussian LSF FWHM 1.5 ch, chi^2',
+                            sets_per_step=per_step),
+                impl='reference', cpu_baseline=cpu,
+                e2e=dict(value=round(value, 2), unit=UNIT, h2d_bytes_per_step=0,
+                         d2h_bytes_per_step=0))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--nsets', type=int, default=512)
+    ap.add_argument('--no-graph', action='store_true')
+    ap.add_argument('--no-tune', dest='tune', action='store_false')
+    ap.add_argument('--tune-budget', type=float, default=40.0)
+    ap.add_argument('--no-plain', dest='plain', action='store_false')
+    ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == 'reference':
+        out = run_reference(args)
+    else:
+        out = run_b200(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == '__main__':
+    main()

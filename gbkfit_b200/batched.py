@@ -1,0 +1,237 @@
+"""Batched evaluation of many parameter sets of one thin smooth disk.
+
+``BatchedSMDisk`` evaluates, per parameter set, smdisk -> PSF x LSF FFT
+convolution -> crop -> residual -> chi^2 against one data cube, for up to
+``max_sets`` sets per call (sampler walkers), through gbkb200_batch_* of
+libgbkb200.so.  Per set the result equals the reference chain
+``DModelSCube.evaluate`` + ``Objective.residual_scalar(squared=True)``
+(dmodels/scube.py:95-122, objective/objective.py:187-206).
+
+Inputs can be host parameter dicts (packed with ``Disk.pack_batch`` and
+copied from pinned memory) or device tensors already resident in HBM.  A
+fixed-size call can be captured once in a CUDA graph and replayed.
+"""
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native
+from ._native import c_int, c_float, c_void_p, check
+from .disk import KINDS
+
+_lib = _native.lib()
+
+
+class BatchDesc(ctypes.Structure):
+    """include/gbkb200.h gbkb200_batch_desc."""
+    _fields_ = [
+        ('size', c_int * 3), ('kernel_size', c_int * 3), ('fft_size', c_int * 3),
+        ('spat_step', c_float * 2), ('spat_zero', c_float * 2),
+        ('spec_step', c_float), ('spec_zero', c_float),
+        ('loose', c_int), ('tilted', c_int), ('nrnodes', c_int), ('rnodes', c_void_p),
+        ('ntraits', c_int * 9), ('uids', c_void_p * 9), ('cvalues', c_void_p * 9),
+        ('ccounts', c_void_p * 9), ('pcounts', c_void_p * 9), ('npvalues', c_int * 9),
+        ('psf', ctypes.POINTER(ctypes.c_double)), ('lsf', ctypes.POINTER(ctypes.c_double)),
+        ('obs_d', c_void_p), ('obs_e', c_void_p), ('obs_m', c_void_p), ('weight', c_float),
+        ('max_sets', c_int), ('chunk', c_int), ('rows_k1', c_int), ('rows_k5', c_int),
+    ]
+
+
+_lib.gbkb200_batch_create.argtypes = [c_void_p, ctypes.POINTER(BatchDesc),
+                                      ctypes.POINTER(c_void_p)]
+_lib.gbkb200_batch_create.restype = c_int
+_lib.gbkb200_batch_evaluate.argtypes = [c_void_p, c_int] + [c_void_p] * 5 + [
+    c_void_p * 9, c_void_p, c_void_p]
+_lib.gbkb200_batch_evaluate.restype = c_int
+_lib.gbkb200_batch_info.argtypes = [c_void_p, c_int * 3, ctypes.POINTER(c_int),
+                                    ctypes.POINTER(ctypes.c_size_t)]
+_lib.gbkb200_batch_info.restype = c_int
+_lib.gbkb200_batch_destroy.argtypes = [c_void_p]
+_lib.gbkb200_batch_destroy.restype = c_int
+
+BATCH_EXPORTED = ['gbkb200_batch_create', 'gbkb200_batch_evaluate', 'gbkb200_batch_info',
+                  'gbkb200_batch_destroy']
+
+
+def kernel_boxes(geom):
+    """PSF image (Ky, Kx) and LSF (Kz) on their own odd-sized boxes, with the
+    reference's sampling, truncation and normalisation (psfs.py, lsfs.py)."""
+    from .psflsf import LSFPoint, PSFPoint
+    kx, ky, kz = geom.kernel_size
+    psf = (geom.psf or PSFPoint()).asarray(geom.step[:2], (kx, ky), (0, 0))
+    lsf = (geom.lsf or LSFPoint()).asarray(geom.step[2], kz, 0)
+    return np.ascontiguousarray(psf, np.float64), np.ascontiguousarray(lsf, np.float64)
+
+
+class BatchedSMDisk:
+    """One thin disk, one data cube, up to max_sets parameter sets per call.
+
+    disk: gbkfit_b200.disk.Disk; geom: gbkfit_b200.workloads.Geometry;
+    data/error/mask: (nz, ny, nx) arrays (host or device) or None."""
+
+    def __init__(self, disk, geom, data, error=None, mask=None, weight=1.0, max_sets=512,
+                 chunk=0, fft_size=(0, 0, 0), rows_k1=0, rows_k5=0, device=0, stream=None):
+        if disk.traits['rht']:
+            raise ValueError("the batched evaluator takes thin disks only")
+        self.disk = disk
+        self.geom = geom
+        self.max_sets = int(max_sets)
+        self.dev = torch.device('cuda', device)
+        self.stream = stream or torch.cuda.current_stream(self.dev)
+        self.ctx = _native.Context(device=device, stream=self.stream, sync=False)
+        dev = self.dev
+        f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32)).to(dev) \
+            if not torch.is_tensor(a) else a.to(dev, torch.float32).contiguous()
+        self._keep = []
+        self.obs = f32(data)
+        self.err = None if error is None else f32(error)
+        self.msk = None if mask is None else f32(mask)
+        self.rnodes = f32(disk.subrnodes)
+        d = BatchDesc()
+        d.size[:] = list(geom.size)
+        d.kernel_size[:] = list(geom.kernel_size)
+        d.fft_size[:] = list(fft_size)
+        d.spat_step[:] = [geom.step[0], geom.step[1]]
+        d.spat_zero[:] = [geom.zero_hi[0], geom.zero_hi[1]]
+        d.spec_step = geom.step[2]
+        d.spec_zero = geom.zero_hi[2]
+        d.loose, d.tilted, d.nrnodes = int(disk.loose), int(disk.tilted), disk.nsub
+        d.rnodes = self.rnodes.data_ptr()
+        self.npv = []
+        for k, kind in enumerate(KINDS):
+            t = disk.tables[kind]
+            if t is None:
+                d.ntraits[k] = 0
+                d.npvalues[k] = 0
+                self.npv.append(0)
+                continue
+            arrs = [torch.as_tensor(t['uids']).to(dev),
+                    torch.as_tensor(t['cvalues'] if len(t['cvalues']) else np.zeros(1, np.float32)).to(dev),
+                    torch.as_tensor(t['ccounts']).to(dev), torch.as_tensor(t['pcounts']).to(dev)]
+            self._keep += arrs
+            d.ntraits[k] = len(t['uids'])
+            d.uids[k], d.cvalues[k], d.ccounts[k], d.pcounts[k] = [a.data_ptr() for a in arrs]
+            d.npvalues[k] = t['npv']
+            self.npv.append(t['npv'])
+        psf, lsf = kernel_boxes(geom)
+        self._psf, self._lsf = psf, lsf
+        d.psf = psf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        d.lsf = lsf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        d.obs_d = self.obs.data_ptr()
+        d.obs_e = self.err.data_ptr() if self.err is not None else None
+        d.obs_m = self.msk.data_ptr() if self.msk is not None else None
+        d.weight = float(weight)
+        d.max_sets, d.chunk, d.rows_k1, d.rows_k5 = self.max_sets, chunk, rows_k1, rows_k5
+        h = c_void_p()
+        check(_lib.gbkb200_batch_create(self.ctx.handle, ctypes.byref(d), ctypes.byref(h)),
+              'gbkb200_batch_create')
+        self.handle = h
+        fs = (c_int * 3)()
+        ch = c_int()
+        wb = ctypes.c_size_t()
+        check(_lib.gbkb200_batch_info(h, fs, ctypes.byref(ch), ctypes.byref(wb)), 'batch_info')
+        self.fft_size, self.chunk, self.work_bytes = tuple(fs), ch.value, wb.value
+        self.chi2 = torch.zeros(self.max_sets, device=dev)
+        self._graph = None
+        self._inputs = None
+
+    # ---- inputs -------------------------------------------------------------
+    def pack(self, params, nsets):
+        """Host parameter dict (per-set leading axis) -> dict of pinned host arrays."""
+        p = self.disk.pack_batch(params, nsets)
+        out = {}
+        for name in ('vsys', 'xpos', 'ypos', 'posa', 'incl'):
+            if p[name] is not None:
+                out[name] = np.ascontiguousarray(p[name], np.float32).reshape(nsets, -1)
+        for kind in KINDS:
+            if p[kind] is not None:
+                out[kind] = np.ascontiguousarray(p[kind]['pvalues'], np.float32).reshape(nsets, -1)
+        return out
+
+    def alloc_inputs(self, nsets=None):
+        """Device input buffers (resident) for nsets sets."""
+        n = self.max_sets if nsets is None else nsets
+        d = self.disk
+        bufs = {}
+        for name in ('vsys', 'xpos', 'ypos', 'posa', 'incl'):
+            if name in d.pdescs:
+                bufs[name] = torch.zeros((n, d.common_size(name)), device=self.dev)
+        for k, kind in enumerate(KINDS):
+            if self.npv[k]:
+                bufs[kind] = torch.zeros((n, self.npv[k]), device=self.dev)
+        return bufs
+
+    def upload(self, packed, bufs, nsets):
+        for k, v in packed.items():
+            bufs[k][:nsets].copy_(torch.from_numpy(v), non_blocking=True)
+
+    # ---- evaluation ---------------------------------------------------------
+    def evaluate_device(self, bufs, nsets, chi2=None, model=None):
+        """chi^2 of nsets resident parameter sets (enqueued, not synchronised)."""
+        chi2 = self.chi2 if chi2 is None else chi2
+        g = lambda n: bufs[n].data_ptr() if n in bufs else None
+        pv = (c_void_p * 9)(*[bufs[k].data_ptr() if k in bufs else None for k in KINDS])
+        check(_lib.gbkb200_batch_evaluate(self.handle, int(nsets), g('vsys'), g('xpos'),
+                                          g('ypos'), g('posa'), g('incl'), pv, chi2.data_ptr(),
+                                          model.data_ptr() if model is not None else None),
+              'gbkb200_batch_evaluate')
+        return chi2[:nsets]
+
+    def evaluate(self, params, nsets):
+        """Host parameters -> host chi^2 (numpy), end to end."""
+        if self._inputs is None:
+            self._inputs = self.alloc_inputs()
+        self.upload(self.pack(params, nsets), self._inputs, nsets)
+        out = self.evaluate_device(self._inputs, nsets)
+        return out.cpu().numpy()
+
+    def capture(self, bufs, nsets):
+        """Capture one evaluate_device call for nsets sets in a CUDA graph."""
+        s = torch.cuda.Stream(self.dev)
+        s.wait_stream(torch.cuda.current_stream(self.dev))
+        self.ctx.set_stream(s)
+        with torch.cuda.stream(s):
+            self.evaluate_device(bufs, nsets)   # warm-up outside capture
+        torch.cuda.current_stream(self.dev).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            self.evaluate_device(bufs, nsets)
+        self.ctx.set_stream(self.stream)
+        self._graph = g
+        return g
+
+    def replay(self):
+        self._graph.replay()
+        return self.chi2
+
+    def close(self):
+        if getattr(self, 'handle', None):
+            _lib.gbkb200_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def synthetic_data(w, device=0, seed=None):
+    """Data cube of a batched workload: the model of w.extra['truth'] (cropped
+    cube from the batched evaluator itself) plus Gaussian noise of sigma =
+    noise_frac x peak (seeded)."""
+    truth = w.extra['truth']
+    zeros = np.zeros(w.geom.size[::-1], np.float32)
+    ev = BatchedSMDisk(w.disk, w.geom, zeros, max_sets=1, device=device)
+    bufs = ev.alloc_inputs(1)
+    ev.upload(ev.pack({k: np.asarray(v)[None] for k, v in truth.items()}, 1), bufs, 1)
+    model = torch.zeros((1,) + tuple(w.geom.size[::-1]), device=ev.dev)
+    ev.evaluate_device(bufs, 1, model=model)
+    m = model[0].cpu().numpy().astype(np.float64)
+    ev.close()
+    rng = np.random.default_rng(w.extra['noise_seed'] if seed is None else seed)
+    sigma = w.extra['noise_frac'] * float(np.max(m))
+    data = m + rng.normal(0.0, sigma, m.shape)
+    return data.astype(np.float32), np.full(m.shape, sigma, np.float32), m

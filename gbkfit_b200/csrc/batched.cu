@@ -1,0 +1,583 @@
+// Batched smdisk -> PSF x LSF convolution -> chi^2 pipeline for many
+// parameter sets of one thin disk (sampler walkers).
+//
+// No reference counterpart as one call: per set it computes what the
+// reference computes with smdisk_evaluate (gmodels.hpp:645-958), DCube's
+// fft_convolve_cached + crop (_dcube.py:245-289, fft.hpp:98-207,
+// dmodels.hpp:7-46), Objective.residual and residual_sum (objective.hpp:7-31,
+// host/kernels.hpp:502-514).
+//
+// Pruning: the crop window [e, e + N) of the convolution only reads model
+// voxels in [0, W), W = N + K - 1 (no wrap-around, since P >= W), so the model
+// is evaluated on the W window only and the FFT grid P is chosen freely
+// (P >= W, factors 2, 3, 5, 7).  Per set:
+//   K1  one block per (set, y < Wy): the spaxel row is evaluated once, its
+//       lines are written into a shared-memory (z, x) slab in row groups,
+//       each group gets its x-axis r2c in shared memory and is stored as
+//       complex rows (z, y, kx);
+//   K2  y-axis FFT of the (z < Wz, kx) columns (rows y >= Wy are zero);
+//   K3  z-axis FFT of the (y, kx) columns, multiply by the PSF x LSF
+//       spectrum and 1/(Px Py Pz), inverse z-axis FFT; only the crop rows
+//       z in [ez, ez + Nz) are stored;
+//   K4  inverse y-axis FFT of the (z < Nz, kx) columns; crop rows stored;
+//   K5  x-axis c2r of the rows, crop, residual against the data and the
+//       per-row fp32 partial of sum r^2 (warp shuffles);
+//   K6  per set, the partials summed in a fixed order in fp64.
+// Sets run in chunks whose intermediates (Wz x Py x hx complex each) stay in
+// the 126 MB L2 between stages.
+#include "gbk_disk.cuh"
+#include "gbk_fft.cuh"
+
+#include <climits>
+#include <cmath>
+#include <vector>
+
+namespace gbk {
+
+struct BatchKernelArgs {
+    int Nx, Ny, Nz, Wx, Wy, Wz, Px, Py, Pz, hx, ex, ey, ez;
+    int rows_k1;     // z rows per shared-memory group in K1
+    int rows_k5;     // y rows per block in K5
+    DiskArgs disk;   // per-set pointers are offset from set 0 by the strides
+    int vstride[5];  // vsys, xpos, ypos, posa, incl values per set
+    int pstride[9];  // trait parameter values per set, per kind
+    AxisDev ax, ay, az;
+    const float2* post;   // exp(-2 pi i k / Px), k in [0, Px/2]
+    const float2* kspec;  // PSF x LSF spectrum (Pz, Py, hx)
+    float scale;          // 1 / (Px Py Pz)
+    const float *obs, *err, *msk;
+    float weight;
+    float2* work;         // (chunk, Wz, Py, hx)
+    float* model;         // optional (nsets, Nz, Ny, Nx)
+    double* partials;     // (nsets, Nz, ceil(Ny / rows_k5))
+    int set0;
+    // element counts of the buffers (bounds of the checked build)
+    long long lim_work, lim_model, lim_part, lim_obs, lim_smem1, lim_smem5;
+};
+
+__device__ __forceinline__ DiskArgs set_disk(const BatchKernelArgs& P, int b)
+{
+    DiskArgs a = P.disk;
+    if (a.vsys) a.vsys += (long long)b * P.vstride[0];
+    a.xpos += (long long)b * P.vstride[1];
+    a.ypos += (long long)b * P.vstride[2];
+    a.posa += (long long)b * P.vstride[3];
+    a.incl += (long long)b * P.vstride[4];
+    TraitSet* ts[9] = {&a.rpt, &a.rht, &a.vpt, &a.vht, &a.dpt, &a.dht, &a.zpt, &a.spt, &a.wpt};
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+        if (ts[k]->pv) ts[k]->pv += (long long)b * P.pstride[k];
+    return a;
+}
+
+// K1: model row + x-axis r2c.  Shared memory: two (rows_k1 x Px/2) complex
+// buffers, the x twiddles, the post twiddles and 5 floats + 2 ints per spaxel.
+__global__ void __launch_bounds__(512) k1_model_xfft(BatchKernelArgs P, int* status)
+{
+    extern __shared__ float2 sm[];
+    const int M = P.Px / 2;
+    const int G = P.rows_k1;
+    float2* b0 = sm;
+    float2* b1 = b0 + G * M;
+    float2* s_tw = b1 + G * M;
+    float2* s_post = s_tw + M;
+    float* s_v = reinterpret_cast<float*>(s_post + P.hx);
+    float* s_amp = s_v + P.Wx;
+    float* s_i2 = s_amp + P.Wx;
+    float* s_orv = s_i2 + P.Wx;
+    int* s_lo = reinterpret_cast<int*>(s_orv + P.Wx);
+    int* s_hi = s_lo + P.Wx;
+
+    const int y = blockIdx.x;
+    const int c = blockIdx.y;
+    const int b = P.set0 + c;
+    const DiskArgs a = set_disk(P, b);
+    int bad = 0;
+    for (int i = threadIdx.x; i < M; i += blockDim.x) s_tw[i] = P.ax.tw[i];
+    for (int i = threadIdx.x; i < P.hx; i += blockDim.x) s_post[i] = P.post[i];
+    const DiskConst kc = disk_const(a);
+    for (int x = threadIdx.x; x < P.Wx; x += blockDim.x) {
+        SpaxelOut o;
+        int lo = INT_MAX, hi = -1;
+        float amp = 0, i2 = 1;
+        if (smdisk_spaxel(a, kc, x, y, 0, o, bad) &&
+            line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo, hi)) {
+            amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
+            i2 = 2 * o.dv * o.dv;
+        } else {
+            lo = INT_MAX;
+            hi = -1;
+        }
+        s_v[x] = o.vv;
+        s_amp[x] = amp;
+        s_i2[x] = i2;
+        s_orv[x] = o.orv;
+        s_lo[x] = lo;
+        s_hi[x] = hi;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    float* slab = reinterpret_cast<float*>(b0);   // (G, Px) reals = (G, M) complex
+    for (int g0 = 0; g0 < P.Wz; g0 += G) {
+        const int gn = min(G, P.Wz - g0);
+        for (int i = threadIdx.x; i < G * M; i += blockDim.x) b0[i] = make_float2(0.f, 0.f);
+        __syncthreads();
+        // lines: a warp per spaxel, lanes along the channel window
+        for (int x = warp; x < P.Wx; x += nwarps) {
+            int lo = max(s_lo[x], g0), hi = min(s_hi[x], g0 + gn - 1);
+            // empty windows carry lo = INT_MAX: skip them before adding the
+            // lane offset (lo + lane would overflow)
+            if (lo > hi) continue;
+            float v = s_v[x], amp = s_amp[x], i2 = s_i2[x], orv = s_orv[x];
+            for (int z = lo + lane; z <= hi; z += 32) {
+                float zv = a.spec_zero + z * a.spec_step;
+                float d = zv - v;
+                const int si = (z - g0) * P.Px + x;
+                if (GBK_OK_IDX(si, 2 * G * M, 1)) slab[si] = orv * (amp * expf(-d * d / i2));
+            }
+        }
+        __syncthreads();
+        float2* r = fft_smem(b0, b1, P.ax, G, 1, M, true, s_tw, false);
+        // even/odd split into hx = M + 1 bins, stored as rows (z, y, kx)
+        float2* out = P.work + (((long long)c * P.Wz + g0) * P.Py + y) * P.hx;
+        const long long zs = (long long)P.Py * P.hx;
+        for (int e = threadIdx.x; e < gn * P.hx; e += blockDim.x) {
+            int l = e / P.hx, k = e % P.hx;
+            float2 zk = r[l * M + (k % M)];
+            float2 zc = conjf2(r[l * M + ((M - k) % M)]);
+            float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+            float2 od = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
+            float2 t = cmul(s_post[k], make_float2(od.y, -od.x));
+            const long long oi = (out - P.work) + l * zs + k;
+            if (GBK_OK_IDX(oi, P.lim_work, 2)) out[l * zs + k] = cadd(ev, t);
+        }
+        __syncthreads();
+    }
+    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
+}
+
+// K2/K3/K4: transforms of columns (o, i) of the chunk's complex cubes,
+// element k at set * set_stride + o * so + i + k * sk.  Rows k >= nload are
+// zero on input.  mode 0: one transform; mode 1: forward, multiply by
+// spec[o * spec_so + i + k * spec_sk] * scale, inverse.  Output rows
+// [s0, s0 + ns) are stored to rows [0, ns).
+constexpr int BLT = 16;
+
+__global__ void __launch_bounds__(256) k_lines(float2* data, long long set_stride, int inner,
+                                                long long so, long long sk, AxisDev ax, int inv,
+                                                int mode, const float2* spec, long long spec_so,
+                                                long long spec_sk, float scale, int nload, int s0,
+                                                int ns, long long lim_data, long long lim_spec)
+{
+    (void)lim_data;
+    (void)lim_spec;
+    extern __shared__ float2 sm[];
+    const int n = ax.n;
+    float2* b0 = sm;
+    float2* b1 = b0 + BLT * n;
+    float2* s_tw = b1 + BLT * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_tw[i] = ax.tw[i];
+    const int tiles = (inner + BLT - 1) / BLT;
+    const int o = blockIdx.x / tiles;
+    const int i0 = (blockIdx.x % tiles) * BLT;
+    const long long base = (long long)blockIdx.y * set_stride + (long long)o * so + i0;
+    for (int e = threadIdx.x; e < BLT * n; e += blockDim.x) {
+        int l = e % BLT, k = e / BLT;
+        const long long gi = base + l + k * sk;
+        b0[k * BLT + l] = (i0 + l < inner && k < nload && GBK_OK_IDX(gi, lim_data, 10))
+                              ? data[gi] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* res = fft_smem(b0, b1, ax, BLT, BLT, 1, false, s_tw, mode == 0 ? inv != 0 : false);
+    if (mode == 1) {
+        const long long sbase = (long long)o * spec_so + i0;
+        for (int e = threadIdx.x; e < BLT * n; e += blockDim.x) {
+            int l = e % BLT, k = e / BLT;
+            if (i0 + l < inner && GBK_OK_IDX(sbase + l + k * spec_sk, lim_spec, 11)) {
+                float2 a = res[k * BLT + l];
+                float2 w = spec[sbase + l + k * spec_sk];
+                res[k * BLT + l] = make_float2((a.x * w.x - a.y * w.y) * scale,
+                                               (a.x * w.y + a.y * w.x) * scale);
+            }
+        }
+        __syncthreads();
+        res = fft_smem(res, res == b0 ? b1 : b0, ax, BLT, BLT, 1, false, s_tw, true);
+    }
+    for (int e = threadIdx.x; e < BLT * ns; e += blockDim.x) {
+        int l = e % BLT, k = e / BLT;
+        if (i0 + l < inner && GBK_OK_IDX(base + l + k * sk, lim_data, 12) &&
+            GBK_OK_IDX((k + s0) * BLT + l, BLT * n, 13))
+            data[base + l + k * sk] = res[(k + s0) * BLT + l];
+    }
+}
+
+// K5: x-axis c2r of rows_k5 rows (z, y), crop, residual and r^2 partials.
+__global__ void __launch_bounds__(256) k5_c2r_residual(BatchKernelArgs P)
+{
+    extern __shared__ float2 sm[];
+    const int M = P.Px / 2;
+    const int G = P.rows_k5;
+    float2* b0 = sm;
+    float2* b1 = b0 + G * M;
+    float2* s_tw = b1 + G * M;
+    float2* s_post = s_tw + M;
+    __shared__ float warp_part[8];
+    const int yg = blockIdx.x, z = blockIdx.y, c = blockIdx.z;
+    const int b = P.set0 + c;
+    const int y0 = yg * G;
+    const int gn = min(G, P.Ny - y0);
+    for (int i = threadIdx.x; i < M; i += blockDim.x) s_tw[i] = P.ax.tw[i];
+    for (int i = threadIdx.x; i < P.hx; i += blockDim.x) s_post[i] = P.post[i];
+    __syncthreads();
+    const float2* rows = P.work + (((long long)c * P.Wz + z) * P.Py + y0) * P.hx;
+    for (int e = threadIdx.x; e < G * M; e += blockDim.x) {
+        int l = e / M, k = e % M;
+        float2 v = make_float2(0.f, 0.f);
+        if (l < gn && GBK_OK_IDX((rows - P.work) + (long long)l * P.hx + M, P.lim_work, 20)) {
+            const float2* r = rows + (long long)l * P.hx;
+            float2 a = r[k], bb = conjf2(r[M - k]);
+            float2 s = cadd(a, bb), d = csub(a, bb);
+            float2 t = cmul(conjf2(s_post[k]), d);
+            v = make_float2(s.x - t.y, s.y + t.x);
+        }
+        b0[l * M + k] = v;
+    }
+    __syncthreads();
+    float2* res = fft_smem(b0, b1, P.ax, G, 1, M, true, s_tw, true);
+    const float* real = reinterpret_cast<const float*>(res);   // (G, Px) reals
+    float acc = 0.f;
+    for (int e = threadIdx.x; e < gn * P.Nx; e += blockDim.x) {
+        int l = e / P.Nx, x = e % P.Nx;
+        if (!GBK_OK_IDX(l * P.Px + x + P.ex, 2 * G * M, 21)) continue;
+        float m = real[l * P.Px + x + P.ex];
+        long long vi = ((long long)z * P.Ny + (y0 + l)) * P.Nx + x;
+        if (!GBK_OK_IDX(vi, P.lim_obs, 22)) continue;
+        if (P.model && GBK_OK_IDX((long long)b * P.Nz * P.Ny * P.Nx + vi, P.lim_model, 23))
+            P.model[(long long)b * P.Nz * P.Ny * P.Nx + vi] = m;
+        // objective.hpp:7-31
+        float r = m - P.obs[vi];
+        if (P.err) r /= P.err[vi];
+        if (P.msk) r *= P.msk[vi];
+        r *= P.weight;
+        acc += r * r;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += warp_part[w];
+        const int ngroups = (P.Ny + G - 1) / G;
+        if (GBK_OK_IDX(((long long)b * P.Nz + z) * ngroups + yg, P.lim_part, 24))
+            P.partials[((long long)b * P.Nz + z) * ngroups + yg] = (double)s;
+    }
+}
+
+// K6: per set, fixed-order fp64 sum of its partials.
+__global__ void __launch_bounds__(256) k6_sum(const double* partials, int nper, int set0,
+                                               float* chi2)
+{
+    __shared__ double sh[256];
+    const int b = set0 + blockIdx.x;
+    double s = 0;
+    for (int i = threadIdx.x; i < nper; i += blockDim.x) s += partials[(long long)b * nper + i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) chi2[b] = (float)sh[0];
+}
+
+}  // namespace gbk
+
+using namespace gbk;
+
+#ifdef GBK_CHECKED
+// checked builds only: copies and clears the first violation recorded by the
+// kernels of this file
+extern "C" int gbkb200_debug_record(long long out[4])
+{
+    long long zero[4] = {0, 0, 0, 0};
+    GBK_CUDA_TRY(cudaDeviceSynchronize());
+    GBK_CUDA_TRY(cudaMemcpyFromSymbol(out, gbk_debug_record, sizeof(zero)));
+    GBK_CUDA_TRY(cudaMemcpyToSymbol(gbk_debug_record, zero, sizeof(zero)));
+    return GBKB200_OK;
+}
+#endif
+
+struct gbkb200_batch {
+    gbkb200_ctx* ctx = nullptr;
+    BatchKernelArgs P{};
+    int max_sets = 0, chunk = 0;
+    size_t smem1 = 0, smem5 = 0, smem_y = 0, smem_z = 0;
+    float2* tw[3] = {nullptr, nullptr, nullptr};
+    float2* post = nullptr;
+    float2* kspec = nullptr;
+    float2* work = nullptr;
+    double* partials = nullptr;
+    int nper = 0;
+};
+
+static bool fft_factor_ok(int n)
+{
+    for (int p : {2, 3, 5, 7})
+        while (n % p == 0) n /= p;
+    return n == 1;
+}
+
+static int auto_fft_size(int w, bool even)
+{
+    for (int n = w;; ++n)
+        if ((!even || n % 2 == 0) && fft_factor_ok(n)) return n;
+}
+
+static int make_axis_dev(AxisDev& a, float2*& tw, int n)
+{
+    a.n = n;
+    int m = n, nr = 0;
+    int r[FFT_MAX_PASSES];
+    while (m % 8 == 0 && m > 8) { r[nr++] = 8; m /= 8; }
+    while (m % 4 == 0) { r[nr++] = 4; m /= 4; }
+    while (m % 2 == 0) { r[nr++] = 2; m /= 2; }
+    for (int p = 3; p <= 7 && m > 1; p += 2)
+        while (m % p == 0) { r[nr++] = p; m /= p; }
+    if (m != 1) return GBKB200_ERR_UNSUPPORTED;
+    a.nr = nr;
+    for (int i = 0; i < nr; ++i) a.r[i] = r[i];
+    std::vector<float2> h(n);
+    for (int k = 0; k < n; ++k) {
+        double ang = -2.0 * M_PI * (double)k / (double)n;
+        h[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
+    if (cudaMalloc(&tw, n * sizeof(float2)) != cudaSuccess) return GBKB200_ERR_OOM;
+    GBK_CUDA_TRY(cudaMemcpy(tw, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    a.tw = tw;
+    return GBKB200_OK;
+}
+
+extern "C" int gbkb200_batch_destroy(gbkb200_batch* bt)
+{
+    if (!bt) return GBKB200_OK;
+    if (bt->ctx) cudaStreamSynchronize(bt->ctx->stream);
+    for (auto* p : bt->tw) cudaFree(p);
+    cudaFree(bt->post);
+    cudaFree(bt->kspec);
+    cudaFree(bt->work);
+    cudaFree(bt->partials);
+    delete bt;
+    return GBKB200_OK;
+}
+
+extern "C" int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* d,
+                                    gbkb200_batch** out)
+{
+    if (!ctx || !d || !out) return GBKB200_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (d->uids[1] || d->nrnodes < 2 || !d->rnodes || !d->obs_d || !d->psf || !d->lsf)
+        return GBKB200_ERR_INVALID_ARG;   // thin disks only
+    for (int i = 0; i < 3; ++i)
+        if (d->size[i] < 1 || d->kernel_size[i] < 1 || d->kernel_size[i] % 2 == 0)
+            return GBKB200_ERR_INVALID_ARG;
+    if (d->max_sets < 1) return GBKB200_ERR_INVALID_ARG;
+    auto* bt = new gbkb200_batch();
+    bt->ctx = ctx;
+    BatchKernelArgs& P = bt->P;
+    P.Nx = d->size[0]; P.Ny = d->size[1]; P.Nz = d->size[2];
+    P.Wx = P.Nx + d->kernel_size[0] - 1;
+    P.Wy = P.Ny + d->kernel_size[1] - 1;
+    P.Wz = P.Nz + d->kernel_size[2] - 1;
+    P.ex = d->kernel_size[0] / 2; P.ey = d->kernel_size[1] / 2; P.ez = d->kernel_size[2] / 2;
+    P.Px = d->fft_size[0] > 0 ? d->fft_size[0] : auto_fft_size(P.Wx, true);
+    P.Py = d->fft_size[1] > 0 ? d->fft_size[1] : auto_fft_size(P.Wy, false);
+    P.Pz = d->fft_size[2] > 0 ? d->fft_size[2] : auto_fft_size(P.Wz, false);
+    if (P.Px < P.Wx || P.Py < P.Wy || P.Pz < P.Wz || P.Px % 2) {
+        gbkb200_batch_destroy(bt);
+        return GBKB200_ERR_INVALID_ARG;
+    }
+    P.hx = P.Px / 2 + 1;
+    P.rows_k1 = d->rows_k1 > 0 ? d->rows_k1 : 16;
+    P.rows_k5 = d->rows_k5 > 0 ? d->rows_k5 : 8;
+    bt->max_sets = d->max_sets;
+    bt->chunk = d->chunk > 0 ? std::min(d->chunk, d->max_sets) : std::min(8, d->max_sets);
+    int rc;
+    if ((rc = make_axis_dev(P.ax, bt->tw[0], P.Px / 2)) ||
+        (rc = make_axis_dev(P.ay, bt->tw[1], P.Py)) ||
+        (rc = make_axis_dev(P.az, bt->tw[2], P.Pz))) {
+        gbkb200_batch_destroy(bt);
+        return rc;
+    }
+    // disk tables (per-set pointers are offset in set_disk)
+    DiskArgs& a = P.disk;
+    a.loose = d->loose; a.tilted = d->tilted; a.nrnodes = d->nrnodes; a.rnodes = d->rnodes;
+    TraitSet* ts[9] = {&a.rpt, &a.rht, &a.vpt, &a.vht, &a.dpt, &a.dht, &a.zpt, &a.spt, &a.wpt};
+    for (int k = 0; k < 9; ++k) {
+        ts[k]->n = d->ntraits[k];
+        ts[k]->uids = d->uids[k];
+        ts[k]->cv = d->cvalues[k];
+        ts[k]->cc = d->ccounts[k];
+        ts[k]->pc = d->pcounts[k];
+        ts[k]->pv = nullptr;
+        P.pstride[k] = d->npvalues[k];
+        if (ts[k]->n < 0 || ts[k]->n > GBK_TRAIT_NUM_MAX) {
+            gbkb200_batch_destroy(bt);
+            return GBKB200_ERR_INVALID_ARG;
+        }
+    }
+    a.opacity = nullptr;
+    a.sx = P.Wx; a.sy = P.Wy; a.sz = 1;
+    a.stx = d->spat_step[0]; a.sty = d->spat_step[1]; a.stz = 0;
+    a.zx = d->spat_zero[0]; a.zy = d->spat_zero[1]; a.zz = 0;
+    a.spec_size = P.Wz; a.spec_step = d->spec_step; a.spec_zero = d->spec_zero;
+    a.image = a.scube = a.wdata = a.wdata_cmp = a.rdata = a.rdata_cmp = nullptr;
+    a.ordata = a.ordata_cmp = a.vdata_cmp = a.ddata_cmp = nullptr;
+    const int nv = d->loose ? d->nrnodes : 1, nt = d->tilted ? d->nrnodes : 1;
+    P.vstride[0] = nv; P.vstride[1] = nv; P.vstride[2] = nv; P.vstride[3] = nt; P.vstride[4] = nt;
+    P.obs = d->obs_d; P.err = d->obs_e; P.msk = d->obs_m; P.weight = d->weight;
+    P.scale = 1.0f / (float)((long long)P.Px * P.Py * P.Pz);
+    // post twiddles of the x axis
+    {
+        std::vector<float2> h(P.hx);
+        for (int k = 0; k < P.hx; ++k) {
+            double ang = -2.0 * M_PI * (double)k / (double)P.Px;
+            h[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+        }
+        if (cudaMalloc(&bt->post, P.hx * sizeof(float2)) != cudaSuccess) {
+            gbkb200_batch_destroy(bt);
+            return GBKB200_ERR_OOM;
+        }
+        GBK_CUDA_TRY(cudaMemcpy(bt->post, h.data(), P.hx * sizeof(float2), cudaMemcpyHostToDevice));
+        P.post = bt->post;
+    }
+    // PSF x LSF kernel cube on the FFT grid, centre rolled to the origin,
+    // and its spectrum (the same r2c as the drop-in FFT path)
+    {
+        const int kx = d->kernel_size[0], ky = d->kernel_size[1], kz = d->kernel_size[2];
+        std::vector<float> cube((size_t)P.Px * P.Py * P.Pz, 0.f);
+        for (int z = 0; z < kz; ++z)
+            for (int y = 0; y < ky; ++y)
+                for (int x = 0; x < kx; ++x) {
+                    int X = ((x - kx / 2) % P.Px + P.Px) % P.Px;
+                    int Y = ((y - ky / 2) % P.Py + P.Py) % P.Py;
+                    int Z = ((z - kz / 2) % P.Pz + P.Pz) % P.Pz;
+                    // _dcube.py:205: (psf * lsf) in float64, then cast
+                    cube[((size_t)Z * P.Py + Y) * P.Px + X] = (float)(d->psf[y * kx + x] * d->lsf[z]);
+                }
+        float* dcube = nullptr;
+        size_t cbytes = (size_t)P.Pz * P.Py * P.hx * sizeof(float2);
+        if (cudaMalloc(&dcube, cube.size() * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&bt->kspec, cbytes) != cudaSuccess) {
+            cudaFree(dcube);
+            gbkb200_batch_destroy(bt);
+            return GBKB200_ERR_OOM;
+        }
+        GBK_CUDA_TRY(cudaMemcpy(dcube, cube.data(), cube.size() * sizeof(float),
+                                cudaMemcpyHostToDevice));
+        int size[3] = {P.Px, P.Py, P.Pz};
+        int sync = ctx->sync;
+        ctx->sync = 1;
+        rc = gbkb200_fft_r2c_f32(ctx, size, dcube, bt->kspec);
+        ctx->sync = sync;
+        cudaFree(dcube);
+        if (rc) {
+            gbkb200_batch_destroy(bt);
+            return rc;
+        }
+        P.kspec = bt->kspec;
+    }
+    // work space and partials
+    size_t wbytes = (size_t)bt->chunk * P.Wz * P.Py * P.hx * sizeof(float2);
+    bt->nper = P.Nz * ((P.Ny + P.rows_k5 - 1) / P.rows_k5);
+    if (cudaMalloc(&bt->work, wbytes) != cudaSuccess ||
+        cudaMalloc(&bt->partials, (size_t)bt->max_sets * bt->nper * sizeof(double)) != cudaSuccess) {
+        gbkb200_batch_destroy(bt);
+        return GBKB200_ERR_OOM;
+    }
+    P.work = bt->work;
+    P.partials = bt->partials;
+    P.lim_work = (long long)bt->chunk * P.Wz * P.Py * P.hx;
+    P.lim_part = (long long)bt->max_sets * bt->nper;
+    P.lim_obs = (long long)P.Nx * P.Ny * P.Nz;
+    // shared memory sizes, set once here so evaluate() can be captured
+    const int M = P.Px / 2;
+    bt->smem1 = (size_t)(2 * P.rows_k1 * M + M + P.hx) * sizeof(float2) +
+                (size_t)P.Wx * (4 * sizeof(float) + 2 * sizeof(int));
+    bt->smem5 = (size_t)(2 * P.rows_k5 * M + M + P.hx) * sizeof(float2);
+    bt->smem_y = (size_t)(2 * BLT * P.Py + P.Py) * sizeof(float2);
+    bt->smem_z = (size_t)(2 * BLT * P.Pz + P.Pz) * sizeof(float2);
+    const size_t lim = 227 * 1024;
+    if (bt->smem1 > lim || bt->smem5 > lim || bt->smem_y > lim || bt->smem_z > lim) {
+        gbkb200_batch_destroy(bt);
+        return GBKB200_ERR_UNSUPPORTED;
+    }
+    cudaFuncSetAttribute(k1_model_xfft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bt->smem1);
+    cudaFuncSetAttribute(k5_c2r_residual, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)bt->smem5);
+    cudaFuncSetAttribute(k_lines, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)std::max(bt->smem_y, bt->smem_z));
+    GBK_CUDA_TRY(cudaGetLastError());
+    *out = bt;
+    return GBKB200_OK;
+}
+
+extern "C" int gbkb200_batch_info(const gbkb200_batch* bt, int fft_size[3], int* chunk,
+                                  size_t* work_bytes)
+{
+    if (!bt) return GBKB200_ERR_INVALID_ARG;
+    if (fft_size) {
+        fft_size[0] = bt->P.Px; fft_size[1] = bt->P.Py; fft_size[2] = bt->P.Pz;
+    }
+    if (chunk) *chunk = bt->chunk;
+    if (work_bytes)
+        *work_bytes = (size_t)bt->chunk * bt->P.Wz * bt->P.Py * bt->P.hx * sizeof(float2);
+    return GBKB200_OK;
+}
+
+extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float* vsys,
+                                      const float* xpos, const float* ypos, const float* posa,
+                                      const float* incl, const float* const pvalues[9],
+                                      float* chi2, float* model)
+{
+    if (!bt || nsets < 0 || nsets > bt->max_sets || !xpos || !ypos || !posa || !incl || !chi2 ||
+        !pvalues)
+        return GBKB200_ERR_INVALID_ARG;
+    BatchKernelArgs P = bt->P;
+    cudaStream_t st = bt->ctx->stream;
+    DiskArgs& a = P.disk;
+    a.vsys = vsys; a.xpos = xpos; a.ypos = ypos; a.posa = posa; a.incl = incl;
+    TraitSet* ts[9] = {&a.rpt, &a.rht, &a.vpt, &a.vht, &a.dpt, &a.dht, &a.zpt, &a.spt, &a.wpt};
+    for (int k = 0; k < 9; ++k) {
+        if (ts[k]->n > 0 && !pvalues[k] && P.pstride[k] > 0) return GBKB200_ERR_INVALID_ARG;
+        ts[k]->pv = pvalues[k];
+        if (ts[k]->n == 0) ts[k]->uids = nullptr;
+    }
+    P.model = model;
+    P.lim_model = model ? (long long)nsets * P.Nz * P.Ny * P.Nx : 0;
+    const long long set_stride = (long long)P.Wz * P.Py * P.hx;
+    const long long lim_spec = (long long)P.Pz * P.Py * P.hx;
+    const int tiles = (P.hx + BLT - 1) / BLT;
+    for (int s0 = 0; s0 < nsets; s0 += bt->chunk) {
+        const int cn = std::min(bt->chunk, nsets - s0);
+        P.set0 = s0;
+        k1_model_xfft<<<dim3(P.Wy, cn), 512, bt->smem1, st>>>(P, bt->ctx->d_status);
+        // K2: y forward over (z < Wz, kx); columns stride hx, outer stride Py * hx
+        k_lines<<<dim3(tiles * P.Wz, cn), 256, bt->smem_y, st>>>(
+            P.work, set_stride, P.hx, (long long)P.Py * P.hx, P.hx, P.ay, 0, 0, nullptr, 0, 0,
+            1.f, P.Wy, 0, P.Py, P.lim_work, lim_spec);
+        // K3: z conv over (y < Py, kx); element stride Py * hx
+        k_lines<<<dim3(tiles * P.Py, cn), 256, bt->smem_z, st>>>(
+            P.work, set_stride, P.hx, P.hx, (long long)P.Py * P.hx, P.az, 0, 1, P.kspec, P.hx,
+            (long long)P.Py * P.hx, P.scale, P.Wz, P.ez, P.Nz, P.lim_work, lim_spec);
+        // K4: y inverse over (z < Nz, kx)
+        k_lines<<<dim3(tiles * P.Nz, cn), 256, bt->smem_y, st>>>(
+            P.work, set_stride, P.hx, (long long)P.Py * P.hx, P.hx, P.ay, 1, 0, nullptr, 0, 0,
+            1.f, P.Py, P.ey, P.Ny, P.lim_work, lim_spec);
+        k5_c2r_residual<<<dim3((P.Ny + P.rows_k5 - 1) / P.rows_k5, P.Nz, cn), 256, bt->smem5,
+                          st>>>(P);
+    }
+    if (nsets > 0) k6_sum<<<nsets, 256, 0, st>>>(P.partials, bt->nper, 0, chi2);
+    GBK_CUDA_TRY(cudaGetLastError());
+    return gbk_finish(bt->ctx);
+}

@@ -1,0 +1,503 @@
+// smdisk / mcdisk / wcube evaluation kernels and their C-ABI entry points.
+//
+// Reference: gbkfit/include/gbkfit/gmodel/gmodels.hpp (per-spaxel and
+// per-cloud arithmetic, restated in gbk_traits.cuh and below) and the drivers
+// gbkfit_host/include/gbkfit/host/kernels.hpp:160-423 (OpenMP) and
+// gbkfit_cuda/src/wrapper.cu:82-324 (one thread per item, global atomics).
+//
+// Design:
+//  * thin disks (spatial z = 1): one thread per spaxel; a warp (32 adjacent x)
+//    walks the union of its lanes' channel windows so every channel step is one
+//    coalesced 128-byte row update; each voxel has a single writer, so the
+//    accumulation needs no atomics;
+//  * thick disks: a block owns a 32-spaxel row segment, its warps walk the
+//    spatial z axis and accumulate the spectral columns in shared memory
+//    (shared atomics), then add each column to HBM once;
+//  * mcdisk: one thread per cloud, Philox counter-based random numbers keyed by
+//    (seed, cloud), red.global.add into the cube (mode 0) or an ordered
+//    two-pass fixed-point accumulation (mode 1, deterministic).
+#include "gbk_disk.cuh"
+
+#include <climits>
+
+namespace gbk {
+
+// Thin disk: one thread per spaxel (spatial z = 1).  Block (32, 8): a warp is
+// a run of 32 adjacent x at one y.
+__global__ void __launch_bounds__(256) smdisk_thin_kernel(DiskArgs a, int* status)
+{
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const bool inside = x < a.sx && y < a.sy;
+    int bad = 0;
+    DiskConst kc = disk_const(a);
+    SpaxelOut o;
+    bool on = inside && smdisk_spaxel(a, kc, x, y, 0, o, bad);
+    int zlo = INT_MAX, zhi = -1;
+    float amp = 0, inv2c2 = 0;
+    if (on) {
+        if (a.image) a.image[x + (long long)a.sx * y] += o.orv;
+        smdisk_side_outputs(a, x, y, 0, o);
+        if (a.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
+            amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
+            inv2c2 = 2 * o.dv * o.dv;
+        } else {
+            zlo = INT_MAX;
+            zhi = -1;
+        }
+    }
+    // channel loop over the union of the warp's windows: coalesced rows
+    const unsigned full = 0xffffffffu;
+    int wlo = __reduce_min_sync(full, zlo);
+    int whi = __reduce_max_sync(full, zhi);
+    if (a.scube) {
+        const long long plane = (long long)a.sx * a.sy;
+        float* col = a.scube + (x + (long long)a.sx * y);
+        for (int z = wlo; z <= whi; ++z) {
+            if (z >= zlo && z <= zhi) {
+                float zv = a.spec_zero + z * a.spec_step;
+                float d = zv - o.vv;
+                col[plane * z] += o.orv * (amp * expf(-d * d / inv2c2));
+            }
+        }
+    }
+    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
+}
+
+// Thick disk (or thin with spatial z > 1): block (32, 8) owns 32 adjacent
+// spaxel columns of one row; each warp takes every 8th spatial z and adds its
+// lines into a shared (spec_size x 32) column tile; the tile is then added to
+// the cube.  With USE_SMEM = false (spectra too long for shared memory) the
+// lines go straight to HBM with atomics.
+template<bool USE_SMEM>
+__global__ void __launch_bounds__(256) smdisk_thick_kernel(DiskArgs a, int* status)
+{
+    extern __shared__ float tile[];
+    const int tx = threadIdx.x, tz = threadIdx.y;
+    const int x = blockIdx.x * 32 + tx;
+    const int y = blockIdx.y;
+    const long long plane = (long long)a.sx * a.sy;
+    int bad = 0;
+    if (USE_SMEM && a.scube) {
+        for (int i = tz * 32 + tx; i < a.spec_size * 32; i += 256) tile[i] = 0.f;
+        __syncthreads();
+    }
+    DiskConst kc = disk_const(a);
+    if (x < a.sx) {
+        for (int z = tz; z < a.sz; z += 8) {
+            SpaxelOut o;
+            if (!smdisk_spaxel(a, kc, x, y, z, o, bad)) continue;
+            if (a.image) atomicAdd(&a.image[x + (long long)a.sx * y], o.orv);
+            smdisk_side_outputs(a, x, y, z, o);
+            int zlo, zhi;
+            if (a.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
+                float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
+                float inv2c2 = 2 * o.dv * o.dv;
+                for (int zs = zlo; zs <= zhi; ++zs) {
+                    float zv = a.spec_zero + zs * a.spec_step;
+                    float d = zv - o.vv;
+                    float f = o.orv * (amp * expf(-d * d / inv2c2));
+                    if (USE_SMEM) atomicAdd(&tile[zs * 32 + tx], f);
+                    else atomicAdd(&a.scube[x + (long long)a.sx * y + plane * zs], f);
+                }
+            }
+        }
+    }
+    if (USE_SMEM && a.scube) {
+        __syncthreads();
+        if (x < a.sx) {
+            float* col = a.scube + (x + (long long)a.sx * y);
+            for (int zs = tz; zs < a.spec_size; zs += 8) {
+                float v = tile[zs * 32 + tx];
+                if (v != 0.f) col[plane * zs] += v;
+            }
+        }
+    }
+    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
+}
+
+// ---- mcdisk ------------------------------------------------------------------
+
+// Philox-4x32-10 (Salmon et al., SC'11), counter {ci, k/4, 0, 0}, key = seed
+struct Philox {
+    unsigned ci, k0, k1, k, w[4];
+    __device__ void block(unsigned j)
+    {
+        unsigned c0 = ci, c1 = j, c2 = 0, c3 = 0, a = k0, b = k1;
+#pragma unroll
+        for (int r = 0; r < 10; ++r) {
+            unsigned hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+            unsigned hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+            unsigned n0 = hi1 ^ c1 ^ a, n2 = hi0 ^ c3 ^ b;
+            c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+            a += 0x9E3779B9u;
+            b += 0xBB67AE85u;
+        }
+        w[0] = c0; w[1] = c1; w[2] = c2; w[3] = c3;
+    }
+    __device__ float next()
+    {
+        if ((k & 3u) == 0) block(k >> 2);
+        unsigned v = w[k & 3u];
+        ++k;
+        return (float)(((double)(v >> 8) + 0.5) * (1.0 / 16777216.0));
+    }
+};
+
+// traits.hpp:310-326
+__device__ __forceinline__ void sample_polar(float& r, float& t, Philox& rng, float rmin, float rmax)
+{
+    float u1 = rng.next();
+    r = sqrtf(rmax * rmax + (rmin * rmin - rmax * rmax) * u1);
+    float u2 = rng.next();
+    t = 2 * GBK_PI * u2;
+}
+
+// math.hpp:207-217 (rejection sampling of ggauss; the moffat pdf is a stub 0
+// in the reference, so its loop always accepts the first x)
+__device__ float rejection(int kind, Philox& rng, float trunc, float c, float d)
+{
+    // bounded: after 4096 rejections the last proposal is kept (the reference
+    // loops without a limit; its acceptance rate here is >= 1/10)
+    float x = 0;
+    for (int it = 0; it < 4096; ++it) {
+        x = (0 - trunc) + rng.next() * ((0 + trunc) - (0 - trunc));
+        float u = rng.next();
+        float y = (kind == 4 ? ggauss_pdf(0, 0, c, d) : 0.f) * u;
+        float z = kind == 4 ? ggauss_pdf(x, 0, c, d) : 0.f;
+        if (!(y > z)) break;
+    }
+    return x;
+}
+
+// math.hpp:152-498 samplers as selected by traits.hpp:596-631, 1516-1590
+__device__ float rh_trait_rnd(Philox& rng, int uid, const float* c, const float* p, const Ring& g,
+                              int& bad)
+{
+    int off = uid >= 1000 ? 1 : 0;
+    int kind = uid - 1000 * off;
+    if (kind < 1 || kind > 7) { bad = 1; return NAN; }
+    bool use_rn = c[1] != 0;
+    float p1 = use_rn ? nw(g, p, off * g.nrnodes) : p[off];
+    float p2 = 0;
+    if (kind == 4 || kind == 6) p2 = use_rn ? nw(g, p, (off + 1) * g.nrnodes) : p[off + 1];
+    float u;
+    switch (kind) {
+    case 1: return (0 - p1) + rng.next() * ((0 + p1) - (0 - p1));
+    case 2: u = rng.next() * 2 - 1.f; return 0 - p1 * sgn(u) * logf(1 - 2 * fabsf(u));
+    case 3: { float u1 = rng.next(); float u2 = rng.next();
+              return 0 + p1 * sqrtf(-2 * logf(u1)) * cosf(2 * GBK_PI * u2); }
+    case 4: return rejection(4, rng, 5 * p1, p1, p2);
+    case 5: u = rng.next() * 2 - 1.f; return 0 + p1 * tanf(GBK_PI * 0.5f * u);
+    case 6: return rejection(6, rng, 5 * p1, p1, p2);
+    default: u = rng.next() * 2 - 1.f; return 0 + p1 * atanhf(u);
+    }
+}
+
+// gmodels.hpp:325-608 up to the splat: sample one cloud and return its
+// voxel and line.  false if the cloud is discarded.
+__device__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m, int ci, int& xo, int& yo, int& zo,
+                             SpaxelOut& o, int& bad)
+{
+    Philox rng;
+    rng.ci = (unsigned)ci;
+    rng.k0 = (unsigned)m.seed;
+    rng.k1 = (unsigned)(m.seed >> 32);
+    rng.k = 0;
+    const float* rnodes = a.rnodes;
+    const int nrn = a.nrnodes;
+    // cumulative cloud counts -> trait and ring (gmodels.hpp:400-416)
+    int lo = 0, hi = m.csum_len - 1;
+    while (lo < hi) {   // first index with ci < csum[index]
+        int mid = (lo + hi) >> 1;
+        if (ci < m.csum[mid]) hi = mid;
+        else lo = mid + 1;
+    }
+    int rnidx = lo, tidx = 0;
+    const float *rpc = a.rpt.cv, *rpp = a.rpt.pv, *rhc = a.rht.cv, *rhp = a.rht.pv;
+    for (tidx = 0; tidx < a.rpt.n; ++tidx) {
+        int size = m.hasordint[tidx] ? 1 : nrn - 2;
+        if (rnidx < size) break;
+        rnidx -= size;
+        rpc += a.rpt.cc[tidx];
+        rpp += a.rpt.pc[tidx];
+        rhc += a.rht.cc[tidx];
+        rhp += a.rht.pc[tidx];
+    }
+    if (tidx >= a.rpt.n) return false;   // cloud index beyond the budget
+    float rv = m.cflux / a.stz;
+    float sign = 1, rd = 0, theta = 0;
+    // traits.hpp:1333-1435
+    {
+        int uid = a.rpt.uids[tidx];
+        int kind = uid >= 1000 ? uid - 1000 : uid;
+        int rn = rnidx + 1;
+        if (kind == 1) {
+            sample_polar(rd, theta, rng, rnodes[0], rnodes[nrn - 1]);
+        } else if ((kind >= 2 && kind <= 7) || kind == 101 || kind == 102) {
+            float hw = rnodes[1] - rnodes[0];
+            sample_polar(rd, theta, rng, rnodes[rn] - hw, rnodes[rn] + hw);
+            if (kind == 102) {
+                int k = (int)rintf(rpc[0]);
+                float amp = rpp[rn];
+                float ph = rpp[nrn + rn] * GBK_D2R;
+                float vr = amp * (rng.next() * 2 - 1.f);
+                float vf = amp * cosf(k * (theta - ph));
+                sign = vr > vf ? 1.f : -1.f;
+            }
+        } else if (kind >= 51 && kind <= 54) {
+            // not implemented in the reference: position stays at the origin
+        } else if (kind == 103) {
+        } else {
+            bad = 1;
+            return false;
+        }
+    }
+    if (sign < 0) rv = -rv;
+    rv *= a.stz;
+    rv /= a.stx * a.sty;
+    float xd = rd * cosf(theta), yd = rd * sinf(theta);
+    Ring g;
+    g.rnodes = rnodes;
+    g.nrnodes = nrn;
+    g.r = rd;
+    g.theta = theta;
+    if (!disk_info(g.rnidx, rd, nrn, rnodes)) return false;
+    float pt[GBK_TRAIT_NUM_MAX] = {0, 0, 0, 0}, ht[GBK_TRAIT_NUM_MAX] = {0, 0, 0, 0};
+    if (a.spt.uids) {
+        eval_set<K_SP>(pt, a.spt, g, 0, 0, 0, bad);
+        float sv = 0;
+        for (int i = 0; i < a.spt.n; ++i) sv += pt[i];
+        if (!sv) return false;
+    }
+    float zd = rh_trait_rnd(rng, a.rht.uids[tidx], rhc, rhp, g, bad);
+    if (a.zpt.uids) {
+        eval_set<K_ZP>(pt, a.zpt, g, 0, 0, 0, bad);
+        float zv = 0;
+        for (int i = 0; i < a.zpt.n; ++i) zv += pt[i];
+        zd += zv;
+    }
+    float vsysi = a.vsys ? (a.loose ? lerp(rd, g.rnidx, rnodes, a.vsys, 0) : a.vsys[0]) : 0.f;
+    float xposi = a.loose ? lerp(rd, g.rnidx, rnodes, a.xpos, 0) : a.xpos[0];
+    float yposi = a.loose ? lerp(rd, g.rnidx, rnodes, a.ypos, 0) : a.ypos[0];
+    float posai = a.tilted ? lerp(rd, g.rnidx, rnodes, a.posa, 0) : a.posa[0];
+    float incli = a.tilted ? lerp(rd, g.rnidx, rnodes, a.incl, 0) : a.incl[0];
+    posai *= GBK_D2R;
+    incli *= GBK_D2R;
+    // disk -> world (gmodels.hpp:159-165 with negated parameters, :495-496)
+    float xn = xd, yn = yd, zn = zd, s, c;
+    sincosf(-incli, &s, &c);
+    rot_lh_x(yn, zn, s, c);
+    sincosf(-posai, &s, &c);
+    rot_lh_z(xn, yn, s, c);
+    xn -= -xposi;
+    yn -= -yposi;
+    float fx = rintf((xn - a.zx) / a.stx), fy = rintf((yn - a.zy) / a.sty);
+    float fz = rintf((zn - a.zz) / a.stz);
+    if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) return false;
+    if (fx < 0 || fx >= a.sx || fy < 0 || fy >= a.sy || fz < 0 || fz >= a.sz) return false;
+    int x = (int)fx, y = (int)fy, z = (int)fz;
+    float vv = 0, dv = 0, wv = 1;
+    if (a.vpt.uids) eval_set<K_VP>(pt, a.vpt, g, sinf(incli), cosf(incli), 0, bad);
+    if (a.vht.uids) eval_set<K_VH>(ht, a.vht, g, 0, 0, fabsf(zd), bad);
+    for (int i = 0; i < a.vpt.n; ++i) vv += pt[i] * ht[i];
+    vv += vsysi;
+    if (a.dpt.uids) eval_set<K_DP>(pt, a.dpt, g, 0, 0, 0, bad);
+    if (a.dht.uids) eval_set<K_DH>(ht, a.dht, g, 0, 0, fabsf(zd), bad);
+    for (int i = 0; i < a.dpt.n; ++i) dv += pt[i] * ht[i];
+    dv = fabsf(dv);
+    if (a.wpt.uids && a.wdata) {
+        eval_set<K_WP>(pt, a.wpt, g, 0, 0, 0, bad);
+        for (int i = 0; i < a.wpt.n; ++i) wv *= pt[i];
+    }
+    float orv = rv;
+    if (a.opacity) {
+        long long sxy = (long long)a.sx * a.sy;
+        for (int oz = z + 1; oz < a.sz; ++oz)
+            orv -= orv * a.opacity[x + (long long)a.sx * y + sxy * oz];
+    }
+    xo = x;
+    yo = y;
+    zo = z;
+    o.rv = rv;
+    o.vv = vv;
+    o.dv = dv;
+    o.wv = wv;
+    o.orv = orv;
+    return true;
+}
+
+// Fast mode: one thread per cloud; every contribution is a red.global.add.
+__global__ void __launch_bounds__(256) mcdisk_kernel(DiskArgs a, McArgs m, int* status)
+{
+    int bad = 0;
+    for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < m.nclouds;
+         ci += gridDim.x * blockDim.x) {
+        int x, y, z;
+        SpaxelOut o;
+        if (!mcdisk_cloud(a, m, ci, x, y, z, o, bad)) continue;
+        if (a.image) atomicAdd(&a.image[x + (long long)a.sx * y], o.orv);
+        int zlo, zhi;
+        if (a.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
+            float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
+            float inv2c2 = 2 * o.dv * o.dv;
+            float* col = a.scube + (x + (long long)a.sx * y);
+            long long plane = (long long)a.sx * a.sy;
+            for (int zs = zlo; zs <= zhi; ++zs) {
+                float zv = a.spec_zero + zs * a.spec_step;
+                float d = zv - o.vv;
+                atomicAdd(&col[plane * zs], o.orv * (amp * expf(-d * d / inv2c2)));
+            }
+        }
+        long long idx = idx3(x, y, z, a.sx, a.sy);
+        // last-writer-wins assignments, racy as in the reference
+        if (a.wdata) a.wdata[idx] = o.wv;
+        if (a.wdata_cmp) a.wdata_cmp[idx] = o.wv;
+        if (a.rdata) atomicAdd(&a.rdata[idx], o.rv);
+        if (a.rdata_cmp) atomicAdd(&a.rdata_cmp[idx], o.rv);
+        if (a.ordata) atomicAdd(&a.ordata[idx], o.orv);
+        if (a.ordata_cmp) atomicAdd(&a.ordata_cmp[idx], o.orv);
+        if (a.vdata_cmp) a.vdata_cmp[idx] = o.vv;
+        if (a.ddata_cmp) a.ddata_cmp[idx] = o.dv;
+    }
+    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
+}
+
+// ---- wcube (gmodels.hpp:52-82) -----------------------------------------------
+__global__ void wcube_kernel(int sx, int sy, int sz, int spec_z, const float* spat, float* spec)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= sx) return;
+    float sum = 0, mx = 0;
+    for (int z = 0; z < sz; ++z) {
+        float v = spat[idx3(x, y, z, sx, sy)];
+        sum += v;
+        mx = mx < v ? v : mx;
+    }
+    float mean = sum / sz;
+    float w = mx > 0 ? mean / mx : 0.f;
+    for (int z = 0; z < spec_z; ++z) spec[idx3(x, y, z, sx, sy)] = w;
+}
+
+}  // namespace gbk
+
+using namespace gbk;
+
+static void fill_set(TraitSet& s, int n, const int* u, const float* cv, const int* cc,
+                     const float* pv, const int* pc)
+{
+    s.n = n; s.uids = u; s.cv = cv; s.cc = cc; s.pv = pv; s.pc = pc;
+}
+
+#define GBK_FILL_DISK(a)                                                                   \
+    a.loose = loose; a.tilted = tilted; a.nrnodes = nrnodes; a.rnodes = rnodes;          \
+    a.vsys = vsys; a.xpos = xpos; a.ypos = ypos; a.posa = posa; a.incl = incl;            \
+    fill_set(a.rpt, nrt, rpt_uids, rpt_cvalues, rpt_ccounts, rpt_pvalues, rpt_pcounts);    \
+    fill_set(a.rht, nrt, rht_uids, rht_cvalues, rht_ccounts, rht_pvalues, rht_pcounts);    \
+    fill_set(a.vpt, nvt, vpt_uids, vpt_cvalues, vpt_ccounts, vpt_pvalues, vpt_pcounts);    \
+    fill_set(a.vht, nvt, vht_uids, vht_cvalues, vht_ccounts, vht_pvalues, vht_pcounts);    \
+    fill_set(a.dpt, ndt, dpt_uids, dpt_cvalues, dpt_ccounts, dpt_pvalues, dpt_pcounts);    \
+    fill_set(a.dht, ndt, dht_uids, dht_cvalues, dht_ccounts, dht_pvalues, dht_pcounts);    \
+    fill_set(a.zpt, nzt, zpt_uids, zpt_cvalues, zpt_ccounts, zpt_pvalues, zpt_pcounts);    \
+    fill_set(a.spt, nst, spt_uids, spt_cvalues, spt_ccounts, spt_pvalues, spt_pcounts);    \
+    fill_set(a.wpt, nwt, wpt_uids, wpt_cvalues, wpt_ccounts, wpt_pvalues, wpt_pcounts);    \
+    a.opacity = opacity; a.sx = spat_size_x; a.sy = spat_size_y; a.sz = spat_size_z;      \
+    a.stx = spat_step_x; a.sty = spat_step_y; a.stz = spat_step_z;                        \
+    a.zx = spat_zero_x; a.zy = spat_zero_y; a.zz = spat_zero_z;                           \
+    a.spec_size = spec_size; a.spec_step = spec_step; a.spec_zero = spec_zero;            \
+    a.image = image; a.scube = scube; a.wdata = wdata; a.wdata_cmp = wdata_cmp;           \
+    a.rdata = rdata; a.rdata_cmp = rdata_cmp; a.ordata = ordata;                          \
+    a.ordata_cmp = ordata_cmp; a.vdata_cmp = vdata_cmp; a.ddata_cmp = ddata_cmp
+
+static int check_disk(const DiskArgs& a)
+{
+    if (a.nrnodes < 2 || !a.rnodes || !a.xpos || !a.ypos || !a.posa || !a.incl)
+        return GBKB200_ERR_INVALID_ARG;
+    if (a.sx <= 0 || a.sy <= 0 || a.sz <= 0) return GBKB200_ERR_INVALID_ARG;
+    if (a.scube && a.spec_size <= 0) return GBKB200_ERR_INVALID_ARG;
+    const TraitSet* sets[] = {&a.rpt, &a.vpt, &a.dpt, &a.zpt, &a.spt, &a.wpt};
+    for (const TraitSet* s : sets)
+        if (s->n < 0 || s->n > GBK_TRAIT_NUM_MAX) return GBKB200_ERR_INVALID_ARG;
+    return GBKB200_OK;
+}
+
+// Shared launch helper of the smdisk entry point (also used by the batched
+// driver for its per-set fallback).
+int gbk_launch_smdisk(const DiskArgs& a, cudaStream_t stream, int* status)
+{
+    const bool thin = a.rht.uids == nullptr;
+    if (thin && a.sz == 1) {
+        dim3 block(32, 8), grid((a.sx + 31) / 32, (a.sy + 7) / 8);
+        smdisk_thin_kernel<<<grid, block, 0, stream>>>(a, status);
+    } else {
+        dim3 block(32, 8), grid((a.sx + 31) / 32, a.sy);
+        size_t smem = a.scube ? (size_t)a.spec_size * 32 * sizeof(float) : 0;
+        if (smem <= 200 * 1024) {
+            if (smem > 48 * 1024)
+                GBK_CUDA_TRY(cudaFuncSetAttribute(smdisk_thick_kernel<true>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)smem));
+            smdisk_thick_kernel<true><<<grid, block, smem, stream>>>(a, status);
+        } else {
+            smdisk_thick_kernel<false><<<grid, block, 0, stream>>>(a, status);
+        }
+    }
+    GBK_CUDA_TRY(cudaGetLastError());
+    return GBKB200_OK;
+}
+
+extern "C" int gbkb200_gmodel_smdisk_evaluate_f32(gbkb200_ctx* ctx, GBKB200_DISK_ARGS)
+{
+    if (!ctx) return GBKB200_ERR_INVALID_ARG;
+    DiskArgs a;
+    GBK_FILL_DISK(a);
+    int rc = check_disk(a);
+    if (rc) return rc;
+    rc = gbk_launch_smdisk(a, ctx->stream, ctx->d_status);
+    if (rc) return rc;
+    return gbk_finish(ctx);
+}
+
+extern "C" int gbkb200_gmodel_mcdisk_evaluate_f32(gbkb200_ctx* ctx, float cflux, int nclouds,
+                                                  const int* ncloudscsum, int ncloudscsum_len,
+                                                  const unsigned char* hasordint,
+                                                  GBKB200_DISK_ARGS)
+{
+    if (!ctx) return GBKB200_ERR_INVALID_ARG;
+    DiskArgs a;
+    GBK_FILL_DISK(a);
+    int rc = check_disk(a);
+    if (rc) return rc;
+    if (nclouds < 0 || (nclouds > 0 && (!ncloudscsum || ncloudscsum_len <= 0 || !hasordint)))
+        return GBKB200_ERR_INVALID_ARG;
+    if (!a.rpt.uids || !a.rht.uids) return GBKB200_ERR_INVALID_ARG;
+    if (nclouds == 0) return gbk_finish(ctx);
+    McArgs m;
+    m.cflux = cflux;
+    m.nclouds = nclouds;
+    m.csum = ncloudscsum;
+    m.csum_len = ncloudscsum_len;
+    m.hasordint = hasordint;
+    m.seed = ctx->seed;
+    int blocks = (nclouds + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    mcdisk_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, ctx->d_status);
+    GBK_CUDA_TRY(cudaGetLastError());
+    return gbk_finish(ctx);
+}
+
+extern "C" int gbkb200_gmodel_wcube_evaluate_f32(gbkb200_ctx* ctx, int spat_size_x,
+                                                 int spat_size_y, int spat_size_z,
+                                                 int spec_size_z, const float* spat_data,
+                                                 float* spec_data)
+{
+    if (!ctx || !spat_data || !spec_data || spat_size_x <= 0 || spat_size_y <= 0 ||
+        spat_size_z <= 0 || spec_size_z < 0)
+        return GBKB200_ERR_INVALID_ARG;
+    dim3 grid((spat_size_x + 127) / 128, spat_size_y);
+    wcube_kernel<<<grid, 128, 0, ctx->stream>>>(spat_size_x, spat_size_y, spat_size_z,
+                                                spec_size_z, spat_data, spec_data);
+    GBK_CUDA_TRY(cudaGetLastError());
+    return gbk_finish(ctx);
+}

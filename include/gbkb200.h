@@ -1,0 +1,238 @@
+/*
+ * gbkb200.h - C ABI of the B200-native GBKFIT model-evaluation library
+ * (libgbkb200.so, sm_100a).
+ *
+ * The entry points replace the methods of the reference's native modules
+ * (pybind11 classes FFTf32, DModelf32, GModelf32, Objectivef32 of
+ * src/gbkfit/driver/native/gbkfit_{host,cuda}).  Argument lists and argument
+ * meaning follow the reference one to one; each declaration cites the
+ * reference declaration it replaces (paths relative to
+ * src/gbkfit/driver/native/).  The differences are:
+ *
+ *   - every call takes a context (the "module object"): it carries the CUDA
+ *     stream, the synchronous/asynchronous mode and the FFT caches;
+ *   - pointers are typed device pointers instead of std::uintptr_t, and
+ *     std::array<int, 3> / std::array<T, 3> arguments are passed as pointers
+ *     to three host values;
+ *   - every call returns a status (GBKB200_OK or an error code) where the
+ *     reference returns void and checks nothing.
+ *
+ * A null pointer means "absent", as in the reference (_detail/native.py maps
+ * None to 0).  Outputs documented as accumulated (+=) must be zeroed by the
+ * caller, as in the reference.  All device pointers must be on the context's
+ * device.  In synchronous mode (the default, the reference's semantics) a call
+ * returns after its work finished; in asynchronous mode it only enqueues work
+ * on the context's stream.
+ */
+#ifndef GBKB200_H
+#define GBKB200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    GBKB200_OK = 0,
+    GBKB200_ERR_INVALID_ARG = 1,   /* null handle, bad size, bad shape */
+    GBKB200_ERR_UNSUPPORTED = 2,   /* e.g. an FFT length with a prime factor > 61 */
+    GBKB200_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+    GBKB200_ERR_BAD_TRAIT = 4,     /* a kernel met an unknown trait uid */
+    GBKB200_ERR_OOM = 5,           /* device allocation failed */
+    GBKB200_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up */
+    GBKB200_ERR_TOO_LARGE = 7      /* a size exceeds a documented maximum */
+};
+
+typedef struct gbkb200_ctx gbkb200_ctx;
+
+/* ---- context (no reference counterpart: the reference's module objects
+ *      are stateless apart from the FFT caches, fft.hpp:209-210) ---------- */
+
+int gbkb200_ctx_create(gbkb200_ctx** out, int device);
+int gbkb200_ctx_destroy(gbkb200_ctx* ctx);
+/* stream: a cudaStream_t (0 = the legacy default stream) */
+int gbkb200_ctx_set_stream(gbkb200_ctx* ctx, void* stream);
+/* sync = 1: return after the work finished (reference semantics, wrapper.cu
+ * ends every call with cudaDeviceSynchronize); sync = 0: enqueue only */
+int gbkb200_ctx_set_sync(gbkb200_ctx* ctx, int sync);
+/* seed of the counter-based cloud generator of mcdisk_evaluate; mode 0 =
+ * fast (atomics, run-to-run order dependent in the last fp32 bit), mode 1 =
+ * deterministic (bit-identical run to run) */
+int gbkb200_ctx_set_mcdisk(gbkb200_ctx* ctx, unsigned long long seed, int mode);
+/* waits for the context's stream, then returns the status raised by kernels
+ * since the last call (GBKB200_OK, _BAD_TRAIT or _TIMEOUT) and clears it */
+int gbkb200_ctx_synchronize(gbkb200_ctx* ctx);
+const char* gbkb200_error_string(int code);
+/* the CUDA error string of the last GBKB200_ERR_CUDA of this thread */
+const char* gbkb200_last_cuda_error(void);
+
+/* ---- FFTf32: gbkfit_host/include/gbkfit/host/fft.hpp:71-125 ------------ */
+/* size = {nx, ny, nz} (the reference receives shape[::-1], _detail/native.py
+ * :228-250); real data (nz, ny, nx), complex data (nz, ny, nx/2+1) */
+
+/* fft.hpp:71-77  FFT::fft_r2c(size, data_r, data_c) */
+int gbkb200_fft_r2c_f32(gbkb200_ctx* ctx, const int size[3], const float* data_r, void* data_c);
+/* fft.hpp:79-85  FFT::fft_c2r(size, data_c, data_r); data_c is preserved
+ * (unlike FFTW's c2r, which may overwrite its input) */
+int gbkb200_fft_c2r_f32(gbkb200_ctx* ctx, const int size[3], const void* data_c, float* data_r);
+/* fft.hpp:87-96  FFT::fft_convolve(size, data1_r, data1_c, data2_c):
+ * data1_r <- irfft(rfft(data1_r) * data2_c / N); data1_c is work space whose
+ * content afterwards is unspecified (the reference multiplies in it and runs
+ * FFTW's multi-dimensional c2r on it, which destroys it).  data1_r and the
+ * complex buffers must be 8-byte aligned. */
+int gbkb200_fft_convolve_f32(gbkb200_ctx* ctx, const int size[3], float* data1_r, void* data1_c,
+                             const void* data2_c);
+/* fft.hpp:98-125  FFT::fft_convolve_cached(size, data1_r, data2_r): as above
+ * with the spectrum of data2_r computed on first use and cached by
+ * (size, data2_r) */
+int gbkb200_fft_convolve_cached_f32(gbkb200_ctx* ctx, const int size[3], float* data1_r,
+                                    const float* data2_r);
+/* fft.hpp:56-69  FFT::clear_cache() */
+int gbkb200_fft_clear_cache(gbkb200_ctx* ctx);
+
+/* ---- DModelf32: gbkfit_host/include/gbkfit/host/dmodels.hpp:8-34 ------- */
+
+/* dmodels.hpp:11-17  DModel::dcube_downscale(scale, offset, src_size, dst_size, src, dst) */
+int gbkb200_dmodel_dcube_downscale_f32(gbkb200_ctx* ctx, const int scale[3], const int offset[3],
+                                       const int src_size[3], const int dst_size[3],
+                                       const float* src_dcube, float* dst_dcube);
+/* dmodels.hpp:19-23  DModel::dcube_mask(cutoff, apply, size, dcube_d, dcube_m, dcube_w);
+ * size = {nx, ny, nz}; every voxel is processed (the reference CUDA driver
+ * covers only the first plane, gbkfit_cuda/src/wrapper.cu:42-56) */
+int gbkb200_dmodel_dcube_mask_f32(gbkb200_ctx* ctx, float cutoff, int apply, const int size[3],
+                                  float* dcube_d, float* dcube_m, float* dcube_w);
+/* dmodels.hpp:25-33  DModel::mmaps_moments(size, step, zero, dcube_d, dcube_w,
+ * cutoff, norders, orders, mmaps_d, mmaps_m, mmaps_w).  As in the reference
+ * native module, the map passed in the mmaps_m position receives the weight
+ * map and the one in the mmaps_w position the mask map (the reference kernel
+ * swaps them, gbkfit_host/include/gbkfit/host/kernels.hpp:124-131, and its
+ * Python wrapper passes (d, w, m), _detail/native.py:280-289).  orders is a
+ * device array of norders ascending ints; maps are (norders, ny, nx). */
+int gbkb200_dmodel_mmaps_moments_f32(gbkb200_ctx* ctx, const int size[3], const float step[3],
+                                     const float zero[3], const float* dcube_d,
+                                     const float* dcube_w, float cutoff, int norders,
+                                     const int* orders, float* mmaps_d, float* mmaps_m,
+                                     float* mmaps_w);
+
+/* ---- GModelf32: gbkfit_host/include/gbkfit/host/gmodels.hpp:8-137 ------ */
+
+/* gmodels.hpp:21-27  GModel::wcube_evaluate(spat_size_x, y, z, spec_size_z, spat, spec) */
+int gbkb200_gmodel_wcube_evaluate_f32(gbkb200_ctx* ctx, int spat_size_x, int spat_size_y,
+                                      int spat_size_z, int spec_size_z, const float* spat_data,
+                                      float* spec_data);
+
+/* The trait-table group of one trait kind, as in the reference:
+ * uids, cvalues, ccounts, pvalues, pcounts. */
+#define GBKB200_TRAIT_ARGS(p) \
+    const int* p##_uids, const float* p##_cvalues, const int* p##_ccounts, \
+    const float* p##_pvalues, const int* p##_pcounts
+
+#define GBKB200_DISK_ARGS \
+    int loose, int tilted, int nrnodes, const float* rnodes, const float* vsys, \
+    const float* xpos, const float* ypos, const float* posa, const float* incl, \
+    int nrt, GBKB200_TRAIT_ARGS(rpt), GBKB200_TRAIT_ARGS(rht), \
+    int nvt, GBKB200_TRAIT_ARGS(vpt), GBKB200_TRAIT_ARGS(vht), \
+    int ndt, GBKB200_TRAIT_ARGS(dpt), GBKB200_TRAIT_ARGS(dht), \
+    int nzt, GBKB200_TRAIT_ARGS(zpt), \
+    int nst, GBKB200_TRAIT_ARGS(spt), \
+    int nwt, GBKB200_TRAIT_ARGS(wpt), \
+    const float* opacity, \
+    int spat_size_x, int spat_size_y, int spat_size_z, \
+    float spat_step_x, float spat_step_y, float spat_step_z, \
+    float spat_zero_x, float spat_zero_y, float spat_zero_z, \
+    int spec_size, float spec_step, float spec_zero, \
+    float* image, float* scube, float* wdata, float* wdata_cmp, \
+    float* rdata, float* rdata_cmp, float* ordata, float* ordata_cmp, \
+    float* vdata_cmp, float* ddata_cmp
+
+/* gmodels.hpp:82-135  GModel::smdisk_evaluate(loose, tilted, nrnodes, rnodes, ...).
+ * image, scube, wdata, rdata, ordata are accumulated into. */
+int gbkb200_gmodel_smdisk_evaluate_f32(gbkb200_ctx* ctx, GBKB200_DISK_ARGS);
+
+/* gmodels.hpp:26-79  GModel::mcdisk_evaluate(cflux, nclouds, ncloudscsum,
+ * ncloudscsum_len, hasordint, loose, tilted, ...).  hasordint is a device
+ * array of one byte per density trait.  Clouds draw from a counter-based
+ * Philox-4x32-10 stream keyed by (seed, cloud index), see
+ * gbkb200_ctx_set_mcdisk; the reference draws from per-thread mt19937
+ * generators that all start from seed 42. */
+int gbkb200_gmodel_mcdisk_evaluate_f32(gbkb200_ctx* ctx, float cflux, int nclouds,
+                                       const int* ncloudscsum, int ncloudscsum_len,
+                                       const unsigned char* hasordint, GBKB200_DISK_ARGS);
+
+/* ---- Objectivef32: gbkfit_host/include/gbkfit/host/objective.hpp:8-21 -- */
+
+/* objective.hpp:15-18  Objective::residual(obs_d, obs_e, obs_m, mdl_d, mdl_w,
+ * mdl_m, size, weight, residual) */
+int gbkb200_objective_residual_f32(gbkb200_ctx* ctx, const float* obs_d, const float* obs_e,
+                                   const float* obs_m, const float* mdl_d, const float* mdl_w,
+                                   const float* mdl_m, int size, float weight, float* residual);
+/* objective.hpp:20  Objective::residual_sum(residual, size, squared, sum);
+ * sum is a device pointer to one float (overwritten).  The reduction is
+ * deterministic (fixed tree order, fp32 pairwise + fp64 final), unlike the
+ * reference's OpenMP reduction. */
+int gbkb200_objective_residual_sum_f32(gbkb200_ctx* ctx, const float* residual, int size,
+                                       int squared, float* sum);
+
+/* ---- batched evaluation (no reference counterpart as one call) ---------
+ *
+ * Evaluates many parameter sets of one thin smooth disk against one data
+ * cube: per set, what the reference computes with GModel::smdisk_evaluate on
+ * the padded DCube grid, FFT::fft_convolve_cached with the PSF x LSF cube,
+ * DModel::dcube_downscale (crop), Objective::residual and
+ * Objective::residual_sum(squared) (objective/objective.py:187-226).  The
+ * model is only evaluated on the window that the crop reads (size +
+ * kernel_size - 1 per axis) and the FFT grid is chosen freely (factors 2, 3,
+ * 5, 7), which leaves the cropped result unchanged.  Kernel truncation:
+ * only the kernel_size box of the PSF x LSF cube is used (the reference's
+ * one-sided LSF truncation keeps a negative tail beyond it, below 1e-14 of the
+ * peak for a Gaussian LSF). */
+
+typedef struct gbkb200_batch gbkb200_batch;
+
+/* trait-kind order of the arrays below: rpt, rht, vpt, vht, dpt, dht, zpt,
+ * spt, wpt (rht must be absent: thin disks) */
+typedef struct {
+    int size[3];            /* data cube (nx, ny, nz) */
+    int kernel_size[3];     /* PSF box (x, y) and LSF box (z), odd */
+    int fft_size[3];        /* FFT grid >= size + kernel_size - 1; 0 = automatic */
+    float spat_step[2];     /* evaluation grid step (x, y) */
+    float spat_zero[2];     /* evaluation grid zero (DCube scratch zero, x, y) */
+    float spec_step;
+    float spec_zero;        /* DCube scratch zero along the spectral axis */
+    int loose, tilted, nrnodes;
+    const float* rnodes;    /* device: sub-nodes */
+    int ntraits[9];
+    const int* uids[9];     /* device */
+    const float* cvalues[9];
+    const int* ccounts[9];
+    const int* pcounts[9];
+    int npvalues[9];        /* parameter values per set, per kind */
+    const double* psf;      /* host: (kernel_size[1], kernel_size[0]) PSF image, centred */
+    const double* lsf;      /* host: kernel_size[2] LSF, centred */
+    const float* obs_d;     /* device: data (nz, ny, nx) */
+    const float* obs_e;     /* device: errors, or NULL */
+    const float* obs_m;     /* device: mask, or NULL */
+    float weight;
+    int max_sets;           /* largest nsets of an evaluate call */
+    int chunk;              /* sets per pipeline wave (0 = 8) */
+    int rows_k1;            /* spectral rows per shared-memory group of the model kernel (0 = 16) */
+    int rows_k5;            /* rows per block of the residual kernel (0 = 8) */
+} gbkb200_batch_desc;
+
+int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);
+/* chi2[s] = sum over voxels of residual^2 for set s (device, nsets floats).
+ * Per-set inputs are device arrays of nsets rows: vsys, xpos, ypos, posa,
+ * incl (1 or nrnodes values per set) and pvalues[k] (npvalues[k] per set).
+ * model: optional device (nsets, nz, ny, nx) output of the cropped model. */
+int gbkb200_batch_evaluate(gbkb200_batch* b, int nsets, const float* vsys, const float* xpos,
+                           const float* ypos, const float* posa, const float* incl,
+                           const float* const pvalues[9], float* chi2, float* model);
+int gbkb200_batch_info(const gbkb200_batch* b, int fft_size[3], int* chunk, size_t* work_bytes);
+int gbkb200_batch_destroy(gbkb200_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GBKB200_H */

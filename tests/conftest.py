@@ -1,0 +1,31 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+@pytest.fixture(scope='session')
+def oracle_built():
+    """Builds oracle/_build/liboracle.so (and oracle/_ref where possible)."""
+    from oracle import oracle
+    if not os.path.exists(oracle.ORACLE_LIB):
+        oracle.build()
+    return oracle
+
+
+@pytest.fixture(scope='session')
+def gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from gbkfit_b200 import build
+    build.build()
+    return torch.device('cuda', 0)

@@ -1,0 +1,87 @@
+"""Batched evaluator (gbkb200_batch_*) against the oracle's DModelSCube +
+Objective chain and against the drop-in per-call GPU path."""
+
+import numpy as np
+import pytest
+
+from tests.helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_batch_workload(nsets):
+    from gbkfit_b200 import workloads
+    return workloads.smdisk_batch128(nsets=nsets, size=(64, 60, 48), nnodes=16)
+
+
+def test_batched_chi2_vs_oracle(gpu, oracle_built):
+    import torch
+    from oracle.oracle import chi2, scube_pipeline
+    from gbkfit_b200 import workloads
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    w = _small_batch_workload(6)
+    data, err, truth_model = synthetic_data(w)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=6, chunk=4)
+    bufs = ev.alloc_inputs(6)
+    ev.upload(ev.pack(w.params, 6), bufs, 6)
+    model = torch.zeros((6,) + tuple(w.geom.size[::-1]), device='cuda')
+    got = ev.evaluate_device(bufs, 6, model=model).cpu().numpy()
+    model = model.cpu().numpy()
+    for i in range(6):
+        p = w.disk.pack(workloads.set_params(w, i))
+        ref64 = scube_pipeline(p, w.geom, precision='f64')
+        ref32 = scube_pipeline(p, w.geom, precision='f32')
+        cpu = rel_err(ref32, ref64)
+        e = rel_err(model[i], ref64)
+        assert e <= max(1e-5, 1.5 * cpu), (i, e, cpu)
+        c_ref = chi2(ref64, data, err)
+        assert abs(got[i] - c_ref) / c_ref < 1e-4, (i, got[i], c_ref)
+    # the truth parameters give chi^2 ~ number of voxels (noise only)
+    truth = {k: np.asarray(v)[None] for k, v in w.extra['truth'].items()}
+    ev.upload(ev.pack(truth, 1), bufs, 1)
+    c = ev.evaluate_device(bufs, 1).cpu().numpy()[0]
+    n = np.prod(w.geom.size)
+    assert 0.9 * n < c < 1.1 * n
+
+
+def test_batched_matches_dropin_path(gpu):
+    """Batched chi^2 == the per-call drop-in path (DModelSCube + Objective)."""
+    from gbkfit_b200 import workloads
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    from gbkfit_b200.driver import DriverB200
+    from gbkfit_b200 import model as M
+    w = _small_batch_workload(3)
+    data, err, _ = synthetic_data(w)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=3)
+    got = ev.evaluate(w.params, 3)
+    drv = DriverB200(0)
+    comp = M.SpectralSMDisk2D(False, False, w.disk.traits['rpt'], w.disk.traits['vpt'],
+                              w.disk.traits['dpt'], rnodes=w.disk.rnodes)
+    gm = M.GModelKinematics2D([comp])
+    g = w.geom
+    dm = M.DModelSCube(g.size, g.step, rpix=(0, 0, (g.size[2] - 1) / 2), rval=(0, 0, 0),
+                       psf=g.psf, lsf=g.lsf)
+    obj = M.Objective(M.Model(drv, dm, gm), data, err)
+    for i in range(3):
+        ref = -2 * obj.log_likelihood(workloads.set_params(w, i))
+        assert abs(got[i] - ref) / ref < 1e-4, (i, got[i], ref)
+
+
+def test_batched_chunks_and_graph(gpu):
+    """Results do not depend on the chunk size; a captured graph replays them."""
+    import torch
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    w = _small_batch_workload(10)
+    data, err, _ = synthetic_data(w)
+    outs = []
+    for chunk in (1, 3, 10):
+        ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=10, chunk=chunk)
+        bufs = ev.alloc_inputs(10)
+        ev.upload(ev.pack(w.params, 10), bufs, 10)
+        outs.append(ev.evaluate_device(bufs, 10).cpu().numpy().copy())
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    ev.capture(bufs, 10)
+    ev.chi2.zero_()
+    ev.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(ev.chi2[:10].cpu().numpy(), outs[0])
