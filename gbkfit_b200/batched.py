@@ -55,6 +55,14 @@ BATCH_EXPORTED = ['gbkb200_batch_create', 'gbkb200_batch_evaluate', 'gbkb200_bat
                   'gbkb200_batch_destroy']
 
 
+def shard_sets(nsets, rank, world):
+    """Contiguous [lo, hi) share of nsets parameter sets for one rank (the
+    multi-GPU path evaluates independent sets per GPU, no data exchange)."""
+    base, extra = divmod(int(nsets), int(world))
+    lo = rank * base + min(rank, extra)
+    return lo, lo + base + (1 if rank < extra else 0)
+
+
 def kernel_boxes(geom):
     """PSF image (Ky, Kx) and LSF (Kz) on their own odd-sized boxes, with the
     reference's sampling, truncation and normalisation (psfs.py, lsfs.py)."""

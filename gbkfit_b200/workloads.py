@@ -45,6 +45,25 @@ def fft_optimal_shape(shape, threshold=32):
     return tuple(out)
 
 
+def dcube_geometry(size, step, rpix, rval, scale, psf, lsf, pad=None):
+    """_dcube.py:128-179: (zero_lo, size_hi, step_hi, zero_hi, edge_hi,
+    kernel_size) of a DCube."""
+    zero = tuple(rval[i] - rpix[i] * step[i] for i in range(3))
+    size_hi = tuple(int(size[i]) * int(scale[i]) for i in range(3))
+    step_hi = tuple(step[i] / scale[i] for i in range(3))
+    edge = (0, 0, 0)
+    ksize = (1, 1, 1)
+    if psf is not None or lsf is not None:
+        ps = psf.size(step_hi[:2]) if psf else (1, 1)
+        ls = lsf.size(step_hi[2]) if lsf else 1
+        ksize = (ps[0], ps[1], ls)
+        need = tuple(size_hi[i] + ksize[i] - 1 for i in range(3))
+        size_hi = fft_optimal_shape(need) if pad is None else pad(need)
+        edge = tuple(k // 2 for k in ksize)
+    zero_hi = tuple(zero[i] - step[i] / 2 - (edge[i] - 0.5) * step_hi[i] for i in range(3))
+    return zero, size_hi, step_hi, zero_hi, edge, ksize
+
+
 class Geometry:
     """Low-res cube and its padded ("hi") evaluation grid (_dcube.py:128-243),
     for scale (1, 1, 1)."""
@@ -52,21 +71,10 @@ class Geometry:
     def __init__(self, size, step, rpix, rval, psf, lsf, pad=None):
         self.size = tuple(int(v) for v in size)
         self.step = tuple(float(v) for v in step)
-        self.zero = tuple(rval[i] - rpix[i] * step[i] for i in range(3))
         self.psf, self.lsf = psf, lsf
-        if psf is not None or lsf is not None:
-            ps = psf.size(self.step[:2]) if psf else (1, 1)
-            ls = lsf.size(self.step[2]) if lsf else 1
-            self.kernel_size = (ps[0], ps[1], ls)
-            need = tuple(self.size[i] + self.kernel_size[i] - 1 for i in range(3))
-            self.size_hi = fft_optimal_shape(need) if pad is None else pad(need)
-            self.edge = tuple(k // 2 for k in self.kernel_size)
-        else:
-            self.kernel_size = (1, 1, 1)
-            self.size_hi = self.size
-            self.edge = (0, 0, 0)
-        self.zero_hi = tuple(self.zero[i] - self.step[i] / 2 - (self.edge[i] - 0.5) * self.step[i]
-                             for i in range(3))
+        (self.zero, self.size_hi, _, self.zero_hi, self.edge,
+         self.kernel_size) = dcube_geometry(self.size, self.step, rpix, rval, (1, 1, 1), psf, lsf,
+                                            pad)
 
     def pcube(self, dtype=np.float32):
         """_dcube.py:189-207: PSF x LSF on the padded grid, rolled to (0,0,0)."""

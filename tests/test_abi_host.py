@@ -1,0 +1,118 @@
+"""CPU tests of the boundary and the host logic: the C ABI library loads and
+exports every function declared in include/gbkb200.h; DCube geometry, padding
+and packing rules; parameter validation."""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    with open(os.path.join(ROOT, 'include', 'gbkb200.h')) as f:
+        text = f.read()
+    text = re.sub(r'/\*.*?\*/', '', text, flags=re.S)
+    return sorted(set(re.findall(r'\b(gbkb200_\w+)\s*\(', text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from gbkfit_b200 import build
+    build.build()
+    import ctypes
+    lib = ctypes.CDLL(build.OUT)
+    names = _declared()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_native_binding_loads_and_binds():
+    from gbkfit_b200 import _native
+    for n in _native.EXPORTED:
+        assert hasattr(_native.lib(), n)
+    assert _native.lib().gbkb200_error_string(4) == b'unknown trait uid'
+
+
+def test_fft_optimal_shape_matches_reference_rule():
+    """driver/backend.py:51-59: po2 up to 32, else the next multiple of 32."""
+    from gbkfit_b200.workloads import fft_optimal_shape
+    assert fft_optimal_shape([1, 2, 3, 17, 32, 33, 80, 96, 148, 290]) == \
+        (1, 2, 4, 32, 32, 64, 96, 96, 160, 320)
+
+
+def test_dcube_geometry_reference_pins():
+    """tests/unit/test_dmodel.py:102-170 of the reference: scratch size, step
+    and zero of a DCube without PSF/LSF."""
+    from gbkfit_b200.workloads import dcube_geometry
+    size, step = (21, 30, 41), (0.5, 1.5, 2.0)
+    rpix, rval, scale = (5.0, 6.5, 7.5), (1.0, 1.5, 2.0), (1, 2, 3)
+    zero, size_hi, step_hi, zero_hi, edge, _ = dcube_geometry(size, step, rpix, rval, scale,
+                                                              None, None)
+    assert zero == tuple(rval[i] - rpix[i] * step[i] for i in range(3))
+    assert size_hi == (21, 60, 123)
+    assert step_hi == (0.5, 0.75, 2.0 / 3)
+    assert edge == (0, 0, 0)
+    assert zero_hi == tuple(zero[i] - step[i] / 2 - (0 - 0.5) * step_hi[i] for i in range(3))
+
+
+def test_dcube_geometry_with_psf_lsf():
+    """_dcube.py:158-179 for the 64^3 workload: kernel (17, 17, 15), padded
+    grid 96^3, edge (8, 8, 7)."""
+    from gbkfit_b200 import workloads
+    g = workloads.smdisk_cube64().geom
+    assert g.kernel_size == (17, 17, 15)
+    assert g.size_hi == (96, 96, 96)
+    assert g.edge == (8, 8, 7)
+    assert np.allclose(g.zero_hi, (-8.0, -8.0, -385.0))
+    pc = g.pcube()
+    assert pc.shape == (96, 96, 96)
+    assert abs(pc.sum() - 1) < 1e-5
+    assert np.unravel_index(np.argmax(pc), pc.shape) == (0, 0, 0)
+
+
+def test_subrnodes_rule():
+    """_disk.py:151-154."""
+    from gbkfit_b200.disk import make_subrnodes, default_rstep
+    rn = np.linspace(0, 30, 20)
+    h = default_rstep(rn)
+    s = make_subrnodes(rn, h)
+    assert s[0] == 0 and np.isclose(s[1], h / 2) and np.isclose(s[-1], s[-2] + h / 2)
+    assert np.allclose(np.diff(s[1:-1]), h)
+
+
+def test_disk_validation():
+    from gbkfit_b200 import traits as T
+    from gbkfit_b200.disk import Disk
+    with pytest.raises(RuntimeError):
+        Disk(False, False, [0.0])
+    with pytest.raises(RuntimeError):
+        Disk(False, False, [0.0, 2.0, 1.0])
+    with pytest.raises(RuntimeError):
+        Disk(False, False, [0.0, 1.0], rstep=0.8)
+    with pytest.raises(RuntimeError):
+        Disk(False, False, [0.0, 1.0, 2.0], traits=dict(rpt=[T.bpt('exponential')] * 5))
+
+
+def test_pack_batch_equals_pack():
+    """Disk.pack_batch row i == Disk.pack of parameter set i."""
+    from gbkfit_b200 import workloads
+    w = workloads.smdisk_batch128(nsets=5)
+    pb = w.disk.pack_batch(w.params, 5)
+    for i in range(5):
+        p = w.disk.pack(workloads.set_params(w, i))
+        for n in ('xpos', 'ypos', 'posa', 'incl', 'vsys'):
+            assert np.allclose(pb[n][i], p[n]), n
+        for k in ('rpt', 'vpt', 'dpt'):
+            assert np.allclose(pb[k]['pvalues'][i], p[k]['pvalues'], rtol=1e-6), k
+
+
+def test_shard_sets_partition():
+    from gbkfit_b200.batched import shard_sets
+    for n in (0, 1, 7, 512, 513):
+        for world in (1, 2, 3, 8):
+            parts = [shard_sets(n, r, world) for r in range(world)]
+            idx = np.concatenate([np.arange(a, b) for a, b in parts])
+            assert np.array_equal(idx, np.arange(n))
