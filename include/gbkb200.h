@@ -174,6 +174,22 @@ int gbkb200_objective_residual_f32(gbkb200_ctx* ctx, const float* obs_d, const f
 int gbkb200_objective_residual_sum_f32(gbkb200_ctx* ctx, const float* residual, int size,
                                        int squared, float* sum);
 
+/* No counterpart in the reference.  The residual sum of
+ * gbkb200_objective_residual_sum_f32 for callers that cannot allocate device
+ * memory (a host framework that owns every device byte through its own pool,
+ * or a loop that must not allocate after start-up): it needs no context and
+ * allocates nothing.  Its block partials live in a fixed 64 KiB device array
+ * inside the library, held by every GPU that loads the library until exit.
+ * size is limited to 268,435,456 residuals (GBKB200_ERR_TOO_LARGE beyond).
+ * The call only enqueues work on `stream` (a cudaStream_t, 0 = legacy
+ * default stream) on the current device; sum (one device float) is ready
+ * when the stream reaches that point.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race and must be ordered by the caller. */
+int gbkb200_objective_residual_sum_noalloc_f32(const float* residual, int size, int squared,
+                                               float* sum, void* stream);
+
 /* ---- batched evaluation (no reference counterpart as one call) ---------
  *
  * Evaluates many parameter sets of one thin smooth disk against one data
