@@ -213,6 +213,7 @@ def run_b200(args):
         b_eval = staged_bytes_per_eval(w.geom)
         achieved = b_eval * nsets / (ms_step / 1e3) / 1e9
         n_chunks = (nsets + ev.chunk - 1) // ev.chunk
+        per_chunk = 2 if ev.conv_mode == 'direct' else 5
         plain = plain_per_call(w, data, err) if args.plain else None
         cpu = cpu_baseline(w, data, err) if args.cpu_baseline else None
         out = dict(
@@ -221,7 +222,8 @@ def run_b200(args):
             scaling='weak', vs_baseline=None, dtype='f32', data='synthetic',
             config=dict(workload='smdisk_batch128: 512 sets x 128x128x96 cube, 30 rings, '
                                  'Gaussian PSF FWHM 3 px x Gaussian LSF FWHM 1.5 ch, chi^2',
-                        nsets_per_gpu=nsets, fft_grid=list(ev.fft_size), chunk=ev.chunk,
+                        nsets_per_gpu=nsets, conv=ev.conv_mode, psf_rank=ev.psf_rank,
+                        fft_grid=list(ev.fft_size), chunk=ev.chunk,
                         tuned=cfg, cuda_graph=use_graph, l2='flushed between steps (256 MB write)',
                         parallelism=f'dp{world} (independent parameter sets per GPU)'),
             e2e=e2e,
@@ -233,7 +235,7 @@ def run_b200(args):
                           fp32_tflops=round(fft_flops_per_eval(w.geom) * nsets
                                             / (ms_step / 1e3) / 1e12, 2)),
             clocks=clocks,
-            gpu_launches=args.steps * (5 * n_chunks + 1),
+            gpu_launches=args.steps * (per_chunk * n_chunks + 1),
             plain_per_call=plain,
             cpu_baseline=cpu,
         )

@@ -1,6 +1,7 @@
 """Autotuner of the batched pipeline's shape parameters.
 
 Knobs (all change speed only, never results beyond fp32 rounding):
+* ``conv``: direct separable FIR (low-rank PSFs) or FFT convolution;
 * ``fft_size``: FFT grid per axis, any 2/3/5/7-smooth size >= the window
   (x even);
 * ``chunk``: parameter sets per pipeline wave (the wave's intermediates
@@ -37,8 +38,10 @@ def smooth_sizes(w, even=False, count=3):
 
 def _key(w, nsets):
     import torch
+    from .batched import kernel_boxes, separable_factors
     g = w.geom
-    return json.dumps(dict(size=g.size, kernel=g.kernel_size, nsets=nsets,
+    rank = separable_factors(kernel_boxes(g)[0])[0]
+    return json.dumps(dict(size=g.size, kernel=g.kernel_size, nsets=nsets, psf_rank=rank,
                            nsub=w.disk.nsub, device=torch.cuda.get_device_name()))
 
 
@@ -89,13 +92,21 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
     if use_cache:
         c = _load().get(key)
         if c:
-            return dict(fft_size=tuple(c['fft_size']), chunk=c['chunk'], rows_k1=c['rows_k1'])
+            return dict(fft_size=tuple(c['fft_size']), chunk=c['chunk'], rows_k1=c['rows_k1'],
+                        conv=c['conv'])
     g = w.geom
+    t_end = time.time() + budget_s
+    # direct separable convolution (when the PSF is low rank): chunk only
+    best_d, best_dt = None, float('inf')
+    for chunk in (4, 8, 16, 32, 64):
+        cfg = dict(fft_size=(0, 0, 0), chunk=chunk, rows_k1=16, conv='direct')
+        t = time_config(w, data, err, nsets, cfg)
+        if t < best_dt:
+            best_d, best_dt = cfg, t
     win = [g.size[i] + g.kernel_size[i] - 1 for i in range(3)]
     cand = [smooth_sizes(win[0], even=True), smooth_sizes(win[1]), smooth_sizes(win[2])]
-    best = dict(fft_size=(cand[0][0], cand[1][0], cand[2][0]), chunk=8, rows_k1=16)
+    best = dict(fft_size=(cand[0][0], cand[1][0], cand[2][0]), chunk=8, rows_k1=16, conv='fft')
     best_t = time_config(w, data, err, nsets, best)
-    t_end = time.time() + budget_s
     trials = []
     for knob, values in (('chunk', (2, 4, 8, 16, 32)), ('rows_k1', (8, 16, 32)),
                          ('fft_x', cand[0]), ('fft_y', cand[1]), ('fft_z', cand[2]),
@@ -116,6 +127,8 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
             trials.append((knob, v, t))
             if t < best_t:
                 best, best_t = cfg, t
+    if best_dt < best_t:
+        best, best_t = best_d, best_dt
     out = dict(best)
     out['fft_size'] = tuple(out['fft_size'])
     if use_cache:

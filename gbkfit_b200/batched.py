@@ -36,7 +36,11 @@ class BatchDesc(ctypes.Structure):
         ('psf', ctypes.POINTER(ctypes.c_double)), ('lsf', ctypes.POINTER(ctypes.c_double)),
         ('obs_d', c_void_p), ('obs_e', c_void_p), ('obs_m', c_void_p), ('weight', c_float),
         ('max_sets', c_int), ('chunk', c_int), ('rows_k1', c_int), ('rows_k5', c_int),
+        ('conv_mode', c_int), ('psf_rank', c_int),
+        ('psf_u', ctypes.POINTER(ctypes.c_double)), ('psf_v', ctypes.POINTER(ctypes.c_double)),
     ]
+
+CONV_MODES = dict(auto=0, fft=1, direct=2)
 
 
 _lib.gbkb200_batch_create.argtypes = [c_void_p, ctypes.POINTER(BatchDesc),
@@ -46,7 +50,7 @@ _lib.gbkb200_batch_evaluate.argtypes = [c_void_p, c_int] + [c_void_p] * 5 + [
     c_void_p * 9, c_void_p, c_void_p]
 _lib.gbkb200_batch_evaluate.restype = c_int
 _lib.gbkb200_batch_info.argtypes = [c_void_p, c_int * 3, ctypes.POINTER(c_int),
-                                    ctypes.POINTER(ctypes.c_size_t)]
+                                    ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(c_int)]
 _lib.gbkb200_batch_info.restype = c_int
 _lib.gbkb200_batch_destroy.argtypes = [c_void_p]
 _lib.gbkb200_batch_destroy.restype = c_int
@@ -73,6 +77,20 @@ def kernel_boxes(geom):
     return np.ascontiguousarray(psf, np.float64), np.ascontiguousarray(lsf, np.float64)
 
 
+def separable_factors(psf, tol=1e-9, max_rank=8):
+    """PSF image (Ky, Kx) = sum_r u_r[y] v_r[x], from its SVD, with the
+    smallest rank whose reconstruction is within tol x max|psf|; (0, None,
+    None) when no rank up to max_rank reaches it."""
+    u, s, vt = np.linalg.svd(psf)
+    peak = np.max(np.abs(psf))
+    for r in range(1, min(max_rank, len(s)) + 1):
+        uu = u[:, :r] * np.sqrt(s[:r])
+        vv = vt[:r].T * np.sqrt(s[:r])
+        if np.max(np.abs(psf - uu @ vv.T)) <= tol * peak:
+            return r, np.ascontiguousarray(uu.T), np.ascontiguousarray(vv.T)
+    return 0, None, None
+
+
 class BatchedSMDisk:
     """One thin disk, one data cube, up to max_sets parameter sets per call.
 
@@ -80,7 +98,8 @@ class BatchedSMDisk:
     data/error/mask: (nz, ny, nx) arrays (host or device) or None."""
 
     def __init__(self, disk, geom, data, error=None, mask=None, weight=1.0, max_sets=512,
-                 chunk=0, fft_size=(0, 0, 0), rows_k1=0, rows_k5=0, device=0, stream=None):
+                 chunk=0, fft_size=(0, 0, 0), rows_k1=0, rows_k5=0, conv='auto', device=0,
+                 stream=None):
         if disk.traits['rht']:
             raise ValueError("the batched evaluator takes thin disks only")
         self.disk = disk
@@ -132,6 +151,13 @@ class BatchedSMDisk:
         d.obs_m = self.msk.data_ptr() if self.msk is not None else None
         d.weight = float(weight)
         d.max_sets, d.chunk, d.rows_k1, d.rows_k5 = self.max_sets, chunk, rows_k1, rows_k5
+        d.conv_mode = CONV_MODES[conv]
+        rank, fu, fv = separable_factors(psf) if conv != 'fft' else (0, None, None)
+        self._fu, self._fv = fu, fv
+        d.psf_rank = rank
+        if rank:
+            d.psf_u = fu.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            d.psf_v = fv.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         h = c_void_p()
         check(_lib.gbkb200_batch_create(self.ctx.handle, ctypes.byref(d), ctypes.byref(h)),
               'gbkb200_batch_create')
@@ -139,8 +165,12 @@ class BatchedSMDisk:
         fs = (c_int * 3)()
         ch = c_int()
         wb = ctypes.c_size_t()
-        check(_lib.gbkb200_batch_info(h, fs, ctypes.byref(ch), ctypes.byref(wb)), 'batch_info')
+        cm = c_int()
+        check(_lib.gbkb200_batch_info(h, fs, ctypes.byref(ch), ctypes.byref(wb),
+                                      ctypes.byref(cm)), 'batch_info')
         self.fft_size, self.chunk, self.work_bytes = tuple(fs), ch.value, wb.value
+        self.conv_mode = {1: 'fft', 2: 'direct'}[cm.value]
+        self.psf_rank = rank
         self.chi2 = torch.zeros(self.max_sets, device=dev)
         self._graph = None
         self._inputs = None

@@ -53,7 +53,229 @@ struct BatchKernelArgs {
     int set0;
     // element counts of the buffers (bounds of the checked build)
     long long lim_work, lim_model, lim_part, lim_obs, lim_smem1, lim_smem5;
+    // direct (separable) convolution
+    int Kx, Ky, Kz;       // PSF (x, y) and LSF box sizes
+    int rank;             // PSF = sum over rank of u_r[y] v_r[x]
+    int pitch;            // row pitch of the LSF-convolved planes (floats, % 4 == 0)
+    int Nxp;              // Nx rounded up to 4
+    const float* vr;      // (rank, Kx): v_r reversed
+    const float* ur;      // (rank, Ky): u_r reversed
+    const float* lsfr;    // (Kz): LSF reversed
+    float* mplanes;       // (chunk, Nz, Wy, pitch)
 };
+
+// ---- direct convolution: LSF FIR per column, separable PSF FIR per plane ----
+//
+// Crop output (zo, yo, xo) of the reference's FFT convolution equals
+//   sum_t sum_sy sum_sx  lsf[Kz-1-t] psf[Ky-1-sy][Kx-1-sx] model(zo+t, yo+sy, xo+sx)
+// in window coordinates (the padded grid's first W indices): the kernel is
+// PSF(x, y) x LSF(z), and PSF = sum_r u_r(y) v_r(x) (rank 1 for a circular
+// Gaussian: its 8-sigma truncation corners are ~1e-14 of the peak).
+
+__device__ __forceinline__ DiskArgs set_disk(const BatchKernelArgs& P, int b);
+
+// KA: one block per (set, window row y): the row's spaxel lines, each spectral
+// column convolved with the LSF (a warp per spaxel), written as rows of the
+// planes (zo, y, x).
+constexpr int KA_THREADS = 256;
+
+__global__ void __launch_bounds__(KA_THREADS) ka_lines_lsf(BatchKernelArgs P, int* status)
+{
+    extern __shared__ float4 sm4[];
+    float* tile = reinterpret_cast<float*>(sm4);          // (Nz, pitch)
+    float* lbuf = tile + (long long)P.Nz * P.pitch;        // (nwarps, Wz)
+    float* s_v = lbuf + (KA_THREADS / 32) * P.Wz;
+    float* s_amp = s_v + P.Wx;
+    float* s_i2 = s_amp + P.Wx;
+    float* s_orv = s_i2 + P.Wx;
+    float* s_lsf = s_orv + P.Wx;
+    int* s_lo = reinterpret_cast<int*>(s_lsf + P.Kz);
+    int* s_hi = s_lo + P.Wx;
+    const int y = blockIdx.x, c = blockIdx.y, b = P.set0 + c;
+    const DiskArgs a = set_disk(P, b);
+    int bad = 0;
+    for (int i = threadIdx.x; i < P.Kz; i += blockDim.x) s_lsf[i] = P.lsfr[i];
+    const DiskConst kc = disk_const(a);
+    for (int x = threadIdx.x; x < P.Wx; x += blockDim.x) {
+        SpaxelOut o;
+        int lo = INT_MAX, hi = -1;
+        float amp = 0, i2 = 1;
+        if (smdisk_spaxel(a, kc, x, y, 0, o, bad) &&
+            line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo, hi)) {
+            amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
+            i2 = 2 * o.dv * o.dv;
+        } else {
+            lo = INT_MAX;
+            hi = -1;
+        }
+        s_v[x] = o.vv;
+        s_amp[x] = amp;
+        s_i2[x] = i2;
+        s_orv[x] = o.orv;
+        s_lo[x] = lo;
+        s_hi[x] = hi;
+    }
+    float4* t4 = reinterpret_cast<float4*>(tile);
+    for (int i = threadIdx.x; i < P.Nz * (P.pitch / 4); i += blockDim.x)
+        t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    float* L = lbuf + warp * P.Wz;
+    for (int x = warp; x < P.Wx; x += nwarps) {
+        const int lo = s_lo[x], hi = s_hi[x];
+        if (lo > hi) continue;
+        const float v = s_v[x], amp = s_amp[x], i2 = s_i2[x], orv = s_orv[x];
+        // gmodels.hpp:109-115: the line, channel by channel (window coordinates)
+        for (int z = lo + lane; z <= hi; z += 32) {
+            float zv = a.spec_zero + z * a.spec_step;
+            float d = zv - v;
+            L[z - lo] = orv * (amp * expf(-d * d / i2));
+        }
+        __syncwarp();
+        const int zo0 = max(0, lo - P.Kz + 1), zo1 = min(P.Nz - 1, hi);
+        for (int zo = zo0 + lane; zo <= zo1; zo += 32) {
+            float acc = 0.f;
+            const int t0 = max(0, lo - zo), t1 = min(P.Kz - 1, hi - zo);
+            for (int t = t0; t <= t1; ++t) acc += s_lsf[t] * L[zo + t - lo];
+            tile[zo * P.pitch + x] = acc;
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    float4* dst = reinterpret_cast<float4*>(P.mplanes) +
+                  ((long long)c * P.Nz * P.Wy + y) * (P.pitch / 4);
+    const long long zstride = (long long)P.Wy * (P.pitch / 4);
+    for (int i = threadIdx.x; i < P.Nz * (P.pitch / 4); i += blockDim.x) {
+        int zo = i / (P.pitch / 4), q = i % (P.pitch / 4);
+        dst[zo * zstride + q] = t4[i];
+    }
+    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
+}
+
+// KB: one block per (set, output plane zo): the plane's separable PSF FIR
+// (x then y, register-blocked: 4 outputs per x strip, 4x4 per y item, with
+// the reversed coefficients held in registers), the crop, the residual and
+// the plane's sum of r^2.  KX/KY bound the kernel sizes (Kx + 3 <= KX + 3).
+constexpr int KB_THREADS = 512;
+constexpr int KB_ITEMS = 4;     // 4x4 output items per thread
+
+template<int KX, int KY>
+__global__ void __launch_bounds__(KB_THREADS) kb_psf_residual(BatchKernelArgs P)
+{
+    extern __shared__ float4 sm4[];
+    float* Mp = reinterpret_cast<float*>(sm4);              // (Wy, pitch)
+    float* P1 = Mp + (long long)P.Wy * P.pitch;             // (Wy, Nxp)
+    __shared__ float warp_part[KB_THREADS / 32];
+    const int zo = blockIdx.x, c = blockIdx.y, b = P.set0 + c;
+    const int Kx = P.Kx, Ky = P.Ky;
+    const float4* src = reinterpret_cast<const float4*>(P.mplanes) +
+                        ((long long)c * P.Nz + zo) * P.Wy * (P.pitch / 4);
+    float4* M4 = reinterpret_cast<float4*>(Mp);
+    for (int i = threadIdx.x; i < P.Wy * (P.pitch / 4); i += blockDim.x) M4[i] = src[i];
+    const int gx = P.Nxp / 4, gy = (P.Ny + 3) / 4;
+    const int nitems = gx * gy;
+    float acc[KB_ITEMS][4][4];
+#pragma unroll
+    for (int it = 0; it < KB_ITEMS; ++it)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[it][q][k] = 0.f;
+    __syncthreads();
+    for (int r = 0; r < P.rank; ++r) {
+        // x FIR: P1[y][xo] = sum_s vr[s] * Mp[y][xo + s]
+        {
+            float vr[KX];
+#pragma unroll
+            for (int s = 0; s < KX; ++s) vr[s] = s < Kx ? P.vr[r * Kx + s] : 0.f;
+            const int nstrips = P.Wy * gx;
+            for (int st = threadIdx.x; st < nstrips; st += blockDim.x) {
+                const int y = st / gx, xg = st % gx;
+                const float4* row = reinterpret_cast<const float4*>(Mp + (long long)y * P.pitch) + xg;
+                float w[KX + 4];
+#pragma unroll
+                for (int m = 0; m < (KX + 4) / 4; ++m) {
+                    float4 f = row[m];
+                    w[4 * m] = f.x; w[4 * m + 1] = f.y; w[4 * m + 2] = f.z; w[4 * m + 3] = f.w;
+                }
+                float o[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int s = 0; s < KX; ++s) o[q] += vr[s] * w[q + s];
+                reinterpret_cast<float4*>(P1 + (long long)y * P.Nxp)[xg] =
+                    make_float4(o[0], o[1], o[2], o[3]);
+            }
+        }
+        __syncthreads();
+        // y FIR, accumulated over the rank: out[yo][xo] += sum_t ur[t] * P1[yo + t][xo]
+        {
+            float ur[KY];
+#pragma unroll
+            for (int t = 0; t < KY; ++t) ur[t] = t < Ky ? P.ur[r * Ky + t] : 0.f;
+#pragma unroll
+            for (int it = 0; it < KB_ITEMS; ++it) {
+                const int item = threadIdx.x + it * blockDim.x;
+                if (item >= nitems) break;
+                const int yg = item / gx, xg = item % gx;
+#pragma unroll
+                for (int m = 0; m < KY + 3; ++m) {
+                    const int row = 4 * yg + m;
+                    float4 p = row < P.Wy
+                        ? reinterpret_cast<const float4*>(P1 + (long long)row * P.Nxp)[xg]
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int t = m - q;
+                        if (t >= 0 && t < KY) {
+                            acc[it][q][0] += ur[t] * p.x;
+                            acc[it][q][1] += ur[t] * p.y;
+                            acc[it][q][2] += ur[t] * p.z;
+                            acc[it][q][3] += ur[t] * p.w;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // crop, residual (objective.hpp:7-31) and r^2
+    float sum = 0.f;
+    const long long plane = (long long)P.Ny * P.Nx;
+#pragma unroll
+    for (int it = 0; it < KB_ITEMS; ++it) {
+        const int item = threadIdx.x + it * blockDim.x;
+        if (item >= nitems) break;
+        const int yg = item / gx, xg = item % gx;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int yo = 4 * yg + q;
+            if (yo >= P.Ny) break;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int xo = 4 * xg + k;
+                if (xo >= P.Nx) break;
+                const float m = acc[it][q][k];
+                const long long vi = (long long)zo * plane + (long long)yo * P.Nx + xo;
+                if (P.model) P.model[(long long)b * P.Nz * plane + vi] = m;
+                float rr = m - P.obs[vi];
+                if (P.err) rr /= P.err[vi];
+                if (P.msk) rr *= P.msk[vi];
+                rr *= P.weight;
+                sum += rr * rr;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (int w = 0; w < KB_THREADS / 32; ++w) s += warp_part[w];
+        P.partials[(long long)b * P.Nz + zo] = (double)s;
+    }
+}
 
 __device__ __forceinline__ DiskArgs set_disk(const BatchKernelArgs& P, int b)
 {
@@ -148,8 +370,8 @@ __global__ void __launch_bounds__(512) k1_model_xfft(BatchKernelArgs P, int* sta
             float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
             float2 od = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
             float2 t = cmul(s_post[k], make_float2(od.y, -od.x));
-            const long long oi = (out - P.work) + l * zs + k;
-            if (GBK_OK_IDX(oi, P.lim_work, 2)) out[l * zs + k] = cadd(ev, t);
+            if (GBK_OK_IDX((out - P.work) + l * zs + k, P.lim_work, 2))
+                out[l * zs + k] = cadd(ev, t);
         }
         __syncthreads();
     }
@@ -319,7 +541,68 @@ struct gbkb200_batch {
     float2* work = nullptr;
     double* partials = nullptr;
     int nper = 0;
+    int direct = 0;
+    size_t smemA = 0, smemB = 0;
+    float *vr = nullptr, *ur = nullptr, *lsfr = nullptr, *mplanes = nullptr;
 };
+
+constexpr int KB_KMAX = 24;   // largest PSF box side of the direct path
+
+// Direct-mode setup: reversed FIR coefficients, plane buffers and shared
+// memory sizes.  Returns GBKB200_ERR_UNSUPPORTED when the direct path does
+// not apply (PSF rank or size, cube size, shared memory).
+static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
+{
+    BatchKernelArgs& P = bt->P;
+    P.Kx = d->kernel_size[0];
+    P.Ky = d->kernel_size[1];
+    P.Kz = d->kernel_size[2];
+    P.rank = d->psf_rank;
+    if (P.rank < 1 || P.rank > 8 || !d->psf_u || !d->psf_v) return GBKB200_ERR_UNSUPPORTED;
+    if (P.Kx > KB_KMAX || P.Ky > KB_KMAX) return GBKB200_ERR_UNSUPPORTED;
+    P.Nxp = (P.Nx + 3) / 4 * 4;
+    const int items = (P.Nxp / 4) * ((P.Ny + 3) / 4);
+    if (items > KB_THREADS * KB_ITEMS) return GBKB200_ERR_UNSUPPORTED;
+    P.pitch = (std::max(P.Wx, P.Nxp + KB_KMAX) + 3) / 4 * 4;
+    bt->smemA = (size_t)P.Nz * P.pitch * sizeof(float) +
+                (size_t)(KA_THREADS / 32) * P.Wz * sizeof(float) +
+                (size_t)P.Wx * (4 * sizeof(float) + 2 * sizeof(int)) + P.Kz * sizeof(float) + 16;
+    bt->smemB = ((size_t)P.Wy * P.pitch + (size_t)P.Wy * P.Nxp) * sizeof(float);
+    const size_t lim = 227 * 1024;
+    if (bt->smemA > lim || bt->smemB > lim) return GBKB200_ERR_UNSUPPORTED;
+    std::vector<float> vr((size_t)P.rank * P.Kx), ur((size_t)P.rank * P.Ky), lr(P.Kz);
+    for (int r = 0; r < P.rank; ++r) {
+        for (int s = 0; s < P.Kx; ++s) vr[r * P.Kx + s] = (float)d->psf_v[r * P.Kx + P.Kx - 1 - s];
+        for (int t = 0; t < P.Ky; ++t) ur[r * P.Ky + t] = (float)d->psf_u[r * P.Ky + P.Ky - 1 - t];
+    }
+    for (int t = 0; t < P.Kz; ++t) lr[t] = (float)d->lsf[P.Kz - 1 - t];
+    if (cudaMalloc(&bt->vr, vr.size() * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&bt->ur, ur.size() * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&bt->lsfr, lr.size() * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&bt->mplanes, (size_t)bt->chunk * P.Nz * P.Wy * P.pitch * sizeof(float)) !=
+            cudaSuccess)
+        return GBKB200_ERR_OOM;
+    GBK_CUDA_TRY(cudaMemcpy(bt->vr, vr.data(), vr.size() * sizeof(float), cudaMemcpyHostToDevice));
+    GBK_CUDA_TRY(cudaMemcpy(bt->ur, ur.data(), ur.size() * sizeof(float), cudaMemcpyHostToDevice));
+    GBK_CUDA_TRY(cudaMemcpy(bt->lsfr, lr.data(), lr.size() * sizeof(float), cudaMemcpyHostToDevice));
+    P.vr = bt->vr;
+    P.ur = bt->ur;
+    P.lsfr = bt->lsfr;
+    P.mplanes = bt->mplanes;
+    GBK_CUDA_TRY(cudaFuncSetAttribute(ka_lines_lsf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)bt->smemA));
+    GBK_CUDA_TRY(cudaFuncSetAttribute(kb_psf_residual<KB_KMAX, KB_KMAX>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)bt->smemB));
+    bt->nper = P.Nz;
+    if (cudaMalloc(&bt->partials, (size_t)bt->max_sets * bt->nper * sizeof(double)) != cudaSuccess)
+        return GBKB200_ERR_OOM;
+    P.partials = bt->partials;
+    P.lim_part = (long long)bt->max_sets * bt->nper;
+    P.lim_obs = (long long)P.Nx * P.Ny * P.Nz;
+    bt->direct = 1;
+    return GBKB200_OK;
+}
 
 static bool fft_factor_ok(int n)
 {
@@ -367,6 +650,10 @@ extern "C" int gbkb200_batch_destroy(gbkb200_batch* bt)
     cudaFree(bt->kspec);
     cudaFree(bt->work);
     cudaFree(bt->partials);
+    cudaFree(bt->vr);
+    cudaFree(bt->ur);
+    cudaFree(bt->lsfr);
+    cudaFree(bt->mplanes);
     delete bt;
     return GBKB200_OK;
 }
@@ -437,6 +724,19 @@ extern "C" int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* 
     P.vstride[0] = nv; P.vstride[1] = nv; P.vstride[2] = nv; P.vstride[3] = nt; P.vstride[4] = nt;
     P.obs = d->obs_d; P.err = d->obs_e; P.msk = d->obs_m; P.weight = d->weight;
     P.scale = 1.0f / (float)((long long)P.Px * P.Py * P.Pz);
+    // direct separable convolution when requested or (automatic) when it applies
+    if (d->conv_mode != 1) {
+        rc = setup_direct(bt, d);
+        if (rc == GBKB200_OK) {
+            GBK_CUDA_TRY(cudaGetLastError());
+            *out = bt;
+            return GBKB200_OK;
+        }
+        if (d->conv_mode == 2 || rc != GBKB200_ERR_UNSUPPORTED) {
+            gbkb200_batch_destroy(bt);
+            return rc;
+        }
+    }
     // post twiddles of the x axis
     {
         std::vector<float2> h(P.hx);
@@ -523,9 +823,10 @@ extern "C" int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* 
 }
 
 extern "C" int gbkb200_batch_info(const gbkb200_batch* bt, int fft_size[3], int* chunk,
-                                  size_t* work_bytes)
+                                  size_t* work_bytes, int* conv_mode)
 {
     if (!bt) return GBKB200_ERR_INVALID_ARG;
+    if (conv_mode) *conv_mode = bt->direct ? 2 : 1;
     if (fft_size) {
         fft_size[0] = bt->P.Px; fft_size[1] = bt->P.Py; fft_size[2] = bt->P.Pz;
     }
@@ -558,6 +859,17 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
     const long long set_stride = (long long)P.Wz * P.Py * P.hx;
     const long long lim_spec = (long long)P.Pz * P.Py * P.hx;
     const int tiles = (P.hx + BLT - 1) / BLT;
+    if (bt->direct) {
+        for (int s0 = 0; s0 < nsets; s0 += bt->chunk) {
+            const int cn = std::min(bt->chunk, nsets - s0);
+            P.set0 = s0;
+            ka_lines_lsf<<<dim3(P.Wy, cn), KA_THREADS, bt->smemA, st>>>(P, bt->ctx->d_status);
+            kb_psf_residual<KB_KMAX, KB_KMAX><<<dim3(P.Nz, cn), KB_THREADS, bt->smemB, st>>>(P);
+        }
+        if (nsets > 0) k6_sum<<<nsets, 256, 0, st>>>(P.partials, bt->nper, 0, chi2);
+        GBK_CUDA_TRY(cudaGetLastError());
+        return gbk_finish(bt->ctx);
+    }
     for (int s0 = 0; s0 < nsets; s0 += bt->chunk) {
         const int cn = std::min(bt->chunk, nsets - s0);
         P.set0 = s0;

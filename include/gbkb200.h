@@ -234,6 +234,10 @@ typedef struct {
     int chunk;              /* sets per pipeline wave (0 = 8) */
     int rows_k1;            /* spectral rows per shared-memory group of the model kernel (0 = 16) */
     int rows_k5;            /* rows per block of the residual kernel (0 = 8) */
+    int conv_mode;          /* 0 = automatic, 1 = FFT, 2 = direct separable FIR */
+    int psf_rank;           /* direct mode: PSF = sum_r u_r(y) v_r(x), rank <= 8 */
+    const double* psf_u;    /* host: (psf_rank, kernel_size[1]) */
+    const double* psf_v;    /* host: (psf_rank, kernel_size[0]) */
 } gbkb200_batch_desc;
 
 int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);
@@ -244,7 +248,10 @@ int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb2
 int gbkb200_batch_evaluate(gbkb200_batch* b, int nsets, const float* vsys, const float* xpos,
                            const float* ypos, const float* posa, const float* incl,
                            const float* const pvalues[9], float* chi2, float* model);
-int gbkb200_batch_info(const gbkb200_batch* b, int fft_size[3], int* chunk, size_t* work_bytes);
+/* the chosen FFT grid, chunk, work-space bytes and convolution mode (1 = FFT,
+ * 2 = direct) */
+int gbkb200_batch_info(const gbkb200_batch* b, int fft_size[3], int* chunk, size_t* work_bytes,
+                       int* conv_mode);
 int gbkb200_batch_destroy(gbkb200_batch* b);
 
 #ifdef __cplusplus

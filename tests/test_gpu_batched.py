@@ -14,14 +14,16 @@ def _small_batch_workload(nsets):
     return workloads.smdisk_batch128(nsets=nsets, size=(64, 60, 48), nnodes=16)
 
 
-def test_batched_chi2_vs_oracle(gpu, oracle_built):
+@pytest.mark.parametrize('conv', ['fft', 'direct'])
+def test_batched_chi2_vs_oracle(gpu, oracle_built, conv):
     import torch
     from oracle.oracle import chi2, scube_pipeline
     from gbkfit_b200 import workloads
     from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
     w = _small_batch_workload(6)
     data, err, truth_model = synthetic_data(w)
-    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=6, chunk=4)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=6, chunk=4, conv=conv)
+    assert ev.conv_mode == conv
     bufs = ev.alloc_inputs(6)
     ev.upload(ev.pack(w.params, 6), bufs, 6)
     model = torch.zeros((6,) + tuple(w.geom.size[::-1]), device='cuda')
@@ -44,7 +46,8 @@ def test_batched_chi2_vs_oracle(gpu, oracle_built):
     assert 0.9 * n < c < 1.1 * n
 
 
-def test_batched_matches_dropin_path(gpu):
+@pytest.mark.parametrize('conv', ['fft', 'direct'])
+def test_batched_matches_dropin_path(gpu, conv):
     """Batched chi^2 == the per-call drop-in path (DModelSCube + Objective)."""
     from gbkfit_b200 import workloads
     from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
@@ -52,7 +55,7 @@ def test_batched_matches_dropin_path(gpu):
     from gbkfit_b200 import model as M
     w = _small_batch_workload(3)
     data, err, _ = synthetic_data(w)
-    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=3)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=3, conv=conv)
     got = ev.evaluate(w.params, 3)
     drv = DriverB200(0)
     comp = M.SpectralSMDisk2D(False, False, w.disk.traits['rpt'], w.disk.traits['vpt'],
@@ -67,7 +70,8 @@ def test_batched_matches_dropin_path(gpu):
         assert abs(got[i] - ref) / ref < 1e-4, (i, got[i], ref)
 
 
-def test_batched_chunks_and_graph(gpu):
+@pytest.mark.parametrize('conv', ['fft', 'direct'])
+def test_batched_chunks_and_graph(gpu, conv):
     """Results do not depend on the chunk size; a captured graph replays them."""
     import torch
     from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
@@ -75,7 +79,7 @@ def test_batched_chunks_and_graph(gpu):
     data, err, _ = synthetic_data(w)
     outs = []
     for chunk in (1, 3, 10):
-        ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=10, chunk=chunk)
+        ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=10, chunk=chunk, conv=conv)
         bufs = ev.alloc_inputs(10)
         ev.upload(ev.pack(w.params, 10), bufs, 10)
         outs.append(ev.evaluate_device(bufs, 10).cpu().numpy().copy())
@@ -85,3 +89,26 @@ def test_batched_chunks_and_graph(gpu):
     ev.replay()
     torch.cuda.synchronize()
     assert np.array_equal(ev.chi2[:10].cpu().numpy(), outs[0])
+
+
+def test_batched_direct_mode_selection(gpu):
+    """Automatic mode: direct for a (rank-1) circular Gaussian PSF, FFT for a
+    high-rank Moffat PSF; both agree with the oracle."""
+    from oracle.oracle import scube_pipeline
+    from gbkfit_b200 import psflsf, workloads
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    import torch
+    w = _small_batch_workload(2)
+    data, err, _ = synthetic_data(w)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=2)
+    assert ev.conv_mode == 'direct' and ev.psf_rank == 1
+    w.geom = workloads.Geometry(w.geom.size, w.geom.step, (0, 0, (w.geom.size[2] - 1) / 2),
+                                (0, 0, 0), psflsf.PSFMoffat(1.2, 2.5), w.geom.lsf)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=2)
+    assert ev.conv_mode == 'fft'
+    bufs = ev.alloc_inputs(2)
+    ev.upload(ev.pack(w.params, 2), bufs, 2)
+    model = torch.zeros((2,) + tuple(w.geom.size[::-1]), device='cuda')
+    ev.evaluate_device(bufs, 2, model=model)
+    ref = scube_pipeline(w.disk.pack(workloads.set_params(w, 1)), w.geom)
+    assert rel_err(model[1].cpu().numpy(), ref) < 2e-5
