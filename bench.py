@@ -155,6 +155,12 @@ def run_b200(args):
     w = workloads.smdisk_batch128(nsets=nsets, seed=1234 + rank)
     data, err, _ = synthetic_data(w, device=local)
     cfg = autotune(w, data, err, nsets, budget_s=args.tune_budget) if args.tune else {}
+    if args.conv:
+        cfg['conv'] = args.conv
+        if args.conv == 'direct':
+            cfg['fft_size'] = (0, 0, 0)
+    if args.chunk:
+        cfg['chunk'] = args.chunk
     ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
     bufs = ev.alloc_inputs(nsets)
     ev.upload(ev.pack(w.params, nsets), bufs, nsets)
@@ -189,6 +195,21 @@ def run_b200(args):
     value = world * nsets / (ms_step / 1e3)
     chi2 = ev.chi2[:nsets].cpu().numpy()
     assert np.all(np.isfinite(chi2)) and np.all(chi2 > 0)
+
+    # per-kernel device time: the same evaluation launched without the graph,
+    # with a CUDA event pair around every launch on the evaluator's stream
+    ev.set_timing(True)
+    ev.stage_times()
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        ev.evaluate_device(bufs, nsets)
+    stages = ev.stage_times()
+    ev.set_timing(False)
+    total = sum(t for t, _ in stages.values())
+    kernels = {k: dict(launches_per_step=n / args.steps, ms_per_step=round(t / args.steps, 4),
+                       ms_per_launch=round(t / n, 5), share=round(t / total, 4))
+               for k, (t, n) in stages.items()}
+    dominant = max(kernels, key=lambda k: kernels[k]['share'])
 
     # end to end through the public API: host dicts -> pinned H2D -> chi^2 D2H
     ev_api = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
@@ -231,7 +252,9 @@ def run_b200(args):
                           unit='GB/s', frac=round(achieved / hbm, 3), traffic=None,
                           peak_kind=peak_kind,
                           basis=f'staged algorithmic bytes per evaluation ({b_eval} B, '
-                                f'reference padding {list(w.geom.size_hi)}) x 512 / step time',
+                                f'reference padding {list(w.geom.size_hi)}) x {nsets} / step time '
+                                '(all kernels of the step)',
+                          kernels=kernels, dominant=dominant,
                           fp32_tflops=round(fft_flops_per_eval(w.geom) * nsets
                                             / (ms_step / 1e3) / 1e12, 2)),
             clocks=clocks,
@@ -368,6 +391,9 @@ def main():
     ap.add_argument('--tune-budget', type=float, default=40.0)
     ap.add_argument('--no-plain', dest='plain', action='store_false')
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
+    ap.add_argument('--conv', choices=['fft', 'direct'], default=None,
+                    help='force the convolution mode (default: tuned)')
+    ap.add_argument('--chunk', type=int, default=0, help='force the sets per wave (default: tuned)')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

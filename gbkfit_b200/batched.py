@@ -54,9 +54,20 @@ _lib.gbkb200_batch_info.argtypes = [c_void_p, c_int * 3, ctypes.POINTER(c_int),
 _lib.gbkb200_batch_info.restype = c_int
 _lib.gbkb200_batch_destroy.argtypes = [c_void_p]
 _lib.gbkb200_batch_destroy.restype = c_int
+_lib.gbkb200_batch_set_timing.argtypes = [c_void_p, c_int]
+_lib.gbkb200_batch_set_timing.restype = c_int
+_lib.gbkb200_batch_timing.argtypes = [c_void_p, ctypes.c_double * 6, c_int * 6]
+_lib.gbkb200_batch_timing.restype = c_int
 
 BATCH_EXPORTED = ['gbkb200_batch_create', 'gbkb200_batch_evaluate', 'gbkb200_batch_info',
-                  'gbkb200_batch_destroy']
+                  'gbkb200_batch_destroy', 'gbkb200_batch_set_timing', 'gbkb200_batch_timing']
+
+# per-stage kernel names of gbkb200_batch_timing, by convolution mode
+STAGE_KERNELS = {
+    'direct': {0: 'ka_lines_lsf', 4: 'kb_psf_residual', 5: 'k6_sum'},
+    'fft': {0: 'k1_model_xfft', 1: 'k_lines (y forward)', 2: 'k_lines (z convolution)',
+            3: 'k_lines (y inverse)', 4: 'k5_c2r_residual', 5: 'k6_sum'},
+}
 
 
 def shard_sets(nsets, rank, world):
@@ -243,6 +254,18 @@ class BatchedSMDisk:
     def replay(self):
         self._graph.replay()
         return self.chi2
+
+    def set_timing(self, enable):
+        """Per-stage CUDA-event timing of subsequent (uncaptured) evaluations."""
+        check(_lib.gbkb200_batch_set_timing(self.handle, int(bool(enable))), 'batch_set_timing')
+
+    def stage_times(self):
+        """{kernel name: (summed ms, launches)} since the last call (synchronises)."""
+        ms = (ctypes.c_double * 6)()
+        n = (c_int * 6)()
+        check(_lib.gbkb200_batch_timing(self.handle, ms, n), 'batch_timing')
+        names = STAGE_KERNELS[self.conv_mode]
+        return {names[i]: (ms[i], n[i]) for i in range(6) if n[i]}
 
     def close(self):
         if getattr(self, 'handle', None):

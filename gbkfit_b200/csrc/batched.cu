@@ -55,13 +55,18 @@ struct BatchKernelArgs {
     long long lim_work, lim_model, lim_part, lim_obs, lim_smem1, lim_smem5;
     // direct (separable) convolution
     int Kx, Ky, Kz;       // PSF (x, y) and LSF box sizes
-    int rank;             // PSF = sum over rank of u_r[y] v_r[x]
-    int pitch;            // row pitch of the LSF-convolved planes (floats, % 4 == 0)
-    int Nxp;              // Nx rounded up to 4
-    const float* vr;      // (rank, Kx): v_r reversed
-    const float* ur;      // (rank, Ky): u_r reversed
+    int K;                // FIR length of the PSF kernel (odd, >= Kx, Ky; zero-padded taps)
+    int pitch;            // row pitch of the LSF-convolved planes in HBM (floats, % 4 == 0)
+    int tpitch;           // row pitch of the model kernel's shared tile (odd: no bank conflicts)
+    int tile_floats;      // Nz * tpitch rounded up to 4
+    int sp;               // row pitch of the PSF kernel's shared rows (floats, % 32 == 4)
+    int band, nbands;     // output rows per PSF block, bands per plane
+    const float* vr;      // (K): PSF x factor, reversed
+    const float* ur;      // (K): PSF y factor, reversed
     const float* lsfr;    // (Kz): LSF reversed
-    float* mplanes;       // (chunk, Nz, Wy, pitch)
+    float* mplanes;       // (chunk, Nz, Wy, pitch): only the xr segments are written
+    int* xr;              // (chunk, Nz, Wy): nonzero x range of each plane row, or -1
+    const double* sat;    // (Nz, Ny + 1, Nx + 1): summed-area table of the zero-model r^2
 };
 
 // ---- direct convolution: LSF FIR per column, separable PSF FIR per plane ----
@@ -69,21 +74,30 @@ struct BatchKernelArgs {
 // Crop output (zo, yo, xo) of the reference's FFT convolution equals
 //   sum_t sum_sy sum_sx  lsf[Kz-1-t] psf[Ky-1-sy][Kx-1-sx] model(zo+t, yo+sy, xo+sx)
 // in window coordinates (the padded grid's first W indices): the kernel is
-// PSF(x, y) x LSF(z), and PSF = sum_r u_r(y) v_r(x) (rank 1 for a circular
-// Gaussian: its 8-sigma truncation corners are ~1e-14 of the peak).
+// PSF(x, y) x LSF(z), and PSF = u(y) v(x) (rank 1: a circular Gaussian's
+// 8-sigma truncation corners are ~1e-14 of the peak).
+//
+// Sparsity: a line is exactly zero outside its +-5 sigma channel window and
+// off the disk, so each LSF-convolved plane is nonzero only in a band of
+// rows and columns.  The model kernel records each plane row's nonzero x
+// range; the PSF kernel convolves only the bounding box of its plane (sums
+// of exact zeros are exact zeros, so results do not change) and takes the
+// residual outside the box, where the model is exactly 0, from a summed-area
+// table of ((0 - data) / error * mask * weight)^2 built once per data cube.
 
 __device__ __forceinline__ DiskArgs set_disk(const BatchKernelArgs& P, int b);
 
 // KA: one block per (set, window row y): the row's spaxel lines, each spectral
-// column convolved with the LSF (a warp per spaxel), written as rows of the
-// planes (zo, y, x).
+// column convolved with the LSF (a warp per spaxel), then per output plane the
+// nonzero x segment of the row (aligned to 4) and its range.
 constexpr int KA_THREADS = 256;
 
-__global__ void __launch_bounds__(KA_THREADS) ka_lines_lsf(BatchKernelArgs P, int* status)
+__global__ void __launch_bounds__(KA_THREADS, 3) ka_lines_lsf(BatchKernelArgs P, int* status)
 {
     extern __shared__ float4 sm4[];
-    float* tile = reinterpret_cast<float*>(sm4);          // (Nz, pitch)
-    float* lbuf = tile + (long long)P.Nz * P.pitch;        // (nwarps, Wz)
+    const int tp = P.tpitch;
+    float* tile = reinterpret_cast<float*>(sm4);          // (Nz, tp)
+    float* lbuf = tile + P.tile_floats;                    // (nwarps, Wz)
     float* s_v = lbuf + (KA_THREADS / 32) * P.Wz;
     float* s_amp = s_v + P.Wx;
     float* s_i2 = s_amp + P.Wx;
@@ -116,7 +130,7 @@ __global__ void __launch_bounds__(KA_THREADS) ka_lines_lsf(BatchKernelArgs P, in
         s_hi[x] = hi;
     }
     float4* t4 = reinterpret_cast<float4*>(tile);
-    for (int i = threadIdx.x; i < P.Nz * (P.pitch / 4); i += blockDim.x)
+    for (int i = threadIdx.x; i < P.tile_floats / 4; i += blockDim.x)
         t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
@@ -137,133 +151,236 @@ __global__ void __launch_bounds__(KA_THREADS) ka_lines_lsf(BatchKernelArgs P, in
             float acc = 0.f;
             const int t0 = max(0, lo - zo), t1 = min(P.Kz - 1, hi - zo);
             for (int t = t0; t <= t1; ++t) acc += s_lsf[t] * L[zo + t - lo];
-            tile[zo * P.pitch + x] = acc;
+            tile[zo * tp + x] = acc;
         }
         __syncwarp();
     }
     __syncthreads();
-    float4* dst = reinterpret_cast<float4*>(P.mplanes) +
-                  ((long long)c * P.Nz * P.Wy + y) * (P.pitch / 4);
-    const long long zstride = (long long)P.Wy * (P.pitch / 4);
-    for (int i = threadIdx.x; i < P.Nz * (P.pitch / 4); i += blockDim.x) {
-        int zo = i / (P.pitch / 4), q = i % (P.pitch / 4);
-        dst[zo * zstride + q] = t4[i];
+    // per output plane: the row's nonzero x range (ballots over the spaxels
+    // whose convolved line reaches zo), then its 4-aligned segment
+    for (int zo = warp; zo < P.Nz; zo += nwarps) {
+        int xmin = INT_MAX, xmax = -1;
+        for (int x0 = 0; x0 < P.Wx; x0 += 32) {
+            const int x = x0 + lane;
+            bool on = false;
+            if (x < P.Wx) {
+                const int lo = s_lo[x], hi = s_hi[x];
+                on = lo <= hi && zo >= lo - P.Kz + 1 && zo <= hi;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, on);
+            if (m) {
+                xmin = min(xmin, x0 + __ffs(m) - 1);
+                xmax = max(xmax, x0 + 31 - __clz(m));
+            }
+        }
+        const long long row = ((long long)c * P.Nz + zo) * P.Wy + y;
+        if (xmax < 0) {
+            if (lane == 0) P.xr[row] = -1;
+            continue;
+        }
+        if (lane == 0) P.xr[row] = xmin | (xmax << 16);
+        float* dst = P.mplanes + row * P.pitch;
+        const float* srow = tile + zo * tp;
+        for (int x = (xmin & ~3) + lane; x <= (xmax | 3); x += 32) dst[x] = srow[x];
     }
     if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
 }
 
-// KB: one block per (set, output plane zo): the plane's separable PSF FIR
-// (x then y, register-blocked: 4 outputs per x strip, 4x4 per y item, with
-// the reversed coefficients held in registers), the crop, the residual and
-// the plane's sum of r^2.  KX/KY bound the kernel sizes (Kx + 3 <= KX + 3).
-constexpr int KB_THREADS = 512;
-constexpr int KB_ITEMS = 4;     // 4x4 output items per thread
-
-template<int KX, int KY>
-__global__ void __launch_bounds__(KB_THREADS) kb_psf_residual(BatchKernelArgs P)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
 {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// sum of the summed-area table over rows [y0, y1) and columns [x0, x1)
+__device__ __forceinline__ double sat_box(const double* T, int ld, int y0, int y1, int x0, int x1)
+{
+    return T[(long long)y1 * ld + x1] - T[(long long)y0 * ld + x1] - T[(long long)y1 * ld + x0] +
+           T[(long long)y0 * ld + x0];
+}
+
+// KB: one block per (set, output plane zo, band of output rows): the bounding
+// box of the band's nonzero input rows is loaded (cp.async), convolved in x in
+// place (8 outputs per thread and window, whole rows per round), then in y
+// (8 x 4 outputs per item) with the crop, residual (objective.hpp:7-31) and
+// r^2 fused; the zero-model residual outside the box comes from the table.
+constexpr int KB_THREADS = 256;
+
+template<int K>
+__global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs P)
+{
+    constexpr int NW = (K + 7 + 3) / 4;     // float4 slots of one 8-output x window
     extern __shared__ float4 sm4[];
-    float* Mp = reinterpret_cast<float*>(sm4);              // (Wy, pitch)
-    float* P1 = Mp + (long long)P.Wy * P.pitch;             // (Wy, Nxp)
+    float* S = reinterpret_cast<float*>(sm4);                   // (band + K - 1, sp)
+    const int rows_in = P.band + K - 1;
+    int* s_xr = reinterpret_cast<int*>(S + (long long)rows_in * P.sp);
+    __shared__ int s_box[4];
     __shared__ float warp_part[KB_THREADS / 32];
-    const int zo = blockIdx.x, c = blockIdx.y, b = P.set0 + c;
-    const int Kx = P.Kx, Ky = P.Ky;
-    const float4* src = reinterpret_cast<const float4*>(P.mplanes) +
-                        ((long long)c * P.Nz + zo) * P.Wy * (P.pitch / 4);
-    float4* M4 = reinterpret_cast<float4*>(Mp);
-    for (int i = threadIdx.x; i < P.Wy * (P.pitch / 4); i += blockDim.x) M4[i] = src[i];
-    const int gx = P.Nxp / 4, gy = (P.Ny + 3) / 4;
-    const int nitems = gx * gy;
-    float acc[KB_ITEMS][4][4];
+    const int zo = blockIdx.x / P.nbands, band = blockIdx.x % P.nbands;
+    const int c = blockIdx.y, b = P.set0 + c;
+    const int ob0 = band * P.band, ob1 = min(P.Ny, ob0 + P.band);  // output rows [ob0, ob1)
+    const int in1 = min(P.Wy, ob1 + K - 1);                        // input rows [ob0, in1)
+    const long long prow = ((long long)c * P.Nz + zo) * P.Wy;
+    const int ld = P.Nx + 1;
+    const double* T = P.sat + (long long)zo * (P.Ny + 1) * ld;
+    if (threadIdx.x < 32) {
+        int y0 = INT_MAX, y1 = -1, x0 = INT_MAX, x1 = -1;
+        for (int y = ob0 + threadIdx.x; y < in1; y += 32) {
+            const int v = P.xr[prow + y];
+            s_xr[y - ob0] = v;
+            if (v >= 0) {
+                y0 = min(y0, y);
+                y1 = max(y1, y);
+                x0 = min(x0, v & 0xffff);
+                x1 = max(x1, v >> 16);
+            }
+        }
 #pragma unroll
-    for (int it = 0; it < KB_ITEMS; ++it)
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int k = 0; k < 4; ++k) acc[it][q][k] = 0.f;
+        for (int o = 16; o > 0; o >>= 1) {
+            y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+            y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+            x0 = min(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+            x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+        }
+        if (threadIdx.x == 0) {
+            s_box[0] = y0; s_box[1] = y1; s_box[2] = x0; s_box[3] = x1;
+        }
+    }
     __syncthreads();
-    for (int r = 0; r < P.rank; ++r) {
-        // x FIR: P1[y][xo] = sum_s vr[s] * Mp[y][xo + s]
-        {
-            float vr[KX];
+    const int y0 = s_box[0], y1 = s_box[1], x0 = s_box[2], x1 = s_box[3];
+    const long long plane = (long long)P.Ny * P.Nx;
+    float* model = P.model ? P.model + ((long long)b * P.Nz + zo) * plane : nullptr;
+    const long long part = ((long long)b * P.Nz + zo) * P.nbands + band;
+    if (y1 < 0) {   // nothing reaches this band: the model is 0 on it
+        if (model)
+            for (long long i = (long long)ob0 * P.Nx + threadIdx.x; i < (long long)ob1 * P.Nx;
+                 i += blockDim.x)
+                model[i] = 0.f;
+        if (threadIdx.x == 0) P.partials[part] = sat_box(T, ld, ob0, ob1, 0, P.Nx);
+        return;
+    }
+    // output box: x in 8-column strips [g_lo, g_hi], y rows [yo_lo, yo_hi]
+    const int g_lo = max(0, x0 - K + 1) >> 3, g_hi = min(P.Nx - 1, x1) >> 3;
+    const int ns8 = g_hi - g_lo + 1;
+    const int yo_lo = max(ob0, y0 - K + 1), yo_hi = min(ob1 - 1, y1);
+    // load rows [y0, y1], float4 slots [2 g_lo, 2 g_hi + NW): the row's
+    // segment from HBM, zeros elsewhere
+    {
+        const int nsl = 2 * (ns8 - 1) + NW, sl0 = 2 * g_lo;
+        const int nrows = y1 - y0 + 1;
+        const float4* src = reinterpret_cast<const float4*>(P.mplanes + prow * P.pitch);
+        for (int i = threadIdx.x; i < nrows * nsl; i += blockDim.x) {
+            const int y = y0 + i / nsl, sl = sl0 + i % nsl;
+            const int v = s_xr[y - ob0];
+            float4* d = reinterpret_cast<float4*>(S + (long long)(y - ob0) * P.sp) + sl;
+            if (v >= 0 && sl >= (v & 0xffff) >> 2 && sl <= (v >> 16) >> 2)
+                cp_async16(d, src + (long long)y * (P.pitch / 4) + sl);
+            else
+                *d = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        cp_async_wait_all();
+    }
+    __syncthreads();
+    // x FIR in place: S[y][xo] = sum_s vr[s] S[y][xo + s] for xo in the strips;
+    // a round covers whole rows, loads before the barrier, stores after it
+    {
+        float vr[K];
 #pragma unroll
-            for (int s = 0; s < KX; ++s) vr[s] = s < Kx ? P.vr[r * Kx + s] : 0.f;
-            const int nstrips = P.Wy * gx;
-            for (int st = threadIdx.x; st < nstrips; st += blockDim.x) {
-                const int y = st / gx, xg = st % gx;
-                const float4* row = reinterpret_cast<const float4*>(Mp + (long long)y * P.pitch) + xg;
-                float w[KX + 4];
+        for (int s = 0; s < K; ++s) vr[s] = P.vr[s];
+        const int rpr = max(1, (int)blockDim.x / ns8);
+        const int rr = threadIdx.x % rpr, g = g_lo + threadIdx.x / rpr;
+        for (int r0 = y0; r0 <= y1; r0 += rpr) {
+            const int y = r0 + rr;
+            const bool act = g <= g_hi && y <= y1;
+            float w[4 * NW];
+            float4* row = reinterpret_cast<float4*>(S + (long long)(y - ob0) * P.sp) + 2 * g;
+            if (act) {
 #pragma unroll
-                for (int m = 0; m < (KX + 4) / 4; ++m) {
-                    float4 f = row[m];
+                for (int m = 0; m < NW; ++m) {
+                    const float4 f = row[m];
                     w[4 * m] = f.x; w[4 * m + 1] = f.y; w[4 * m + 2] = f.z; w[4 * m + 3] = f.w;
                 }
-                float o[4] = {0.f, 0.f, 0.f, 0.f};
+            }
+            __syncthreads();
+            if (act) {
+                float o[8];
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
+                for (int q = 0; q < 8; ++q) {
+                    float acc = 0.f;
 #pragma unroll
-                    for (int s = 0; s < KX; ++s) o[q] += vr[s] * w[q + s];
-                reinterpret_cast<float4*>(P1 + (long long)y * P.Nxp)[xg] =
-                    make_float4(o[0], o[1], o[2], o[3]);
+                    for (int s = 0; s < K; ++s) acc += vr[s] * w[q + s];
+                    o[q] = acc;
+                }
+                row[0] = make_float4(o[0], o[1], o[2], o[3]);
+                row[1] = make_float4(o[4], o[5], o[6], o[7]);
             }
         }
-        __syncthreads();
-        // y FIR, accumulated over the rank: out[yo][xo] += sum_t ur[t] * P1[yo + t][xo]
-        {
-            float ur[KY];
+    }
+    __syncthreads();
+    // y FIR + crop + residual: items of 8 output rows x 4 columns
+    float ur[K];
 #pragma unroll
-            for (int t = 0; t < KY; ++t) ur[t] = t < Ky ? P.ur[r * Ky + t] : 0.f;
+    for (int t = 0; t < K; ++t) ur[t] = P.ur[t];
+    const int ngy = (yo_hi - yo_lo + 8) / 8, s4_lo = 2 * g_lo, ns4 = 2 * ns8;
+    const int items = ngy * ns4;
+    float sum = 0.f;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int gy = it / ns4, s4 = s4_lo + it % ns4;
+        const int yb = yo_lo + 8 * gy;
+        float acc[8][4];
 #pragma unroll
-            for (int it = 0; it < KB_ITEMS; ++it) {
-                const int item = threadIdx.x + it * blockDim.x;
-                if (item >= nitems) break;
-                const int yg = item / gx, xg = item % gx;
+        for (int q = 0; q < 8; ++q)
 #pragma unroll
-                for (int m = 0; m < KY + 3; ++m) {
-                    const int row = 4 * yg + m;
-                    float4 p = row < P.Wy
-                        ? reinterpret_cast<const float4*>(P1 + (long long)row * P.Nxp)[xg]
-                        : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int k = 0; k < 4; ++k) acc[q][k] = 0.f;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int t = m - q;
-                        if (t >= 0 && t < KY) {
-                            acc[it][q][0] += ur[t] * p.x;
-                            acc[it][q][1] += ur[t] * p.y;
-                            acc[it][q][2] += ur[t] * p.z;
-                            acc[it][q][3] += ur[t] * p.w;
-                        }
-                    }
+        for (int m = 0; m < K + 7; ++m) {
+            const int y = yb + m;
+            const float4 p = (y >= y0 && y <= y1)
+                ? reinterpret_cast<const float4*>(S + (long long)(y - ob0) * P.sp)[s4]
+                : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int t = m - q;
+                if (t >= 0 && t < K) {
+                    acc[q][0] += ur[t] * p.x;
+                    acc[q][1] += ur[t] * p.y;
+                    acc[q][2] += ur[t] * p.z;
+                    acc[q][3] += ur[t] * p.w;
                 }
             }
         }
-        __syncthreads();
-    }
-    // crop, residual (objective.hpp:7-31) and r^2
-    float sum = 0.f;
-    const long long plane = (long long)P.Ny * P.Nx;
 #pragma unroll
-    for (int it = 0; it < KB_ITEMS; ++it) {
-        const int item = threadIdx.x + it * blockDim.x;
-        if (item >= nitems) break;
-        const int yg = item / gx, xg = item % gx;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int yo = 4 * yg + q;
-            if (yo >= P.Ny) break;
+        for (int q = 0; q < 8; ++q) {
+            const int yo = yb + q;
+            if (yo >= ob1) break;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const int xo = 4 * xg + k;
+                const int xo = 4 * s4 + k;
                 if (xo >= P.Nx) break;
-                const float m = acc[it][q][k];
+                const float m = acc[q][k];
                 const long long vi = (long long)zo * plane + (long long)yo * P.Nx + xo;
-                if (P.model) P.model[(long long)b * P.Nz * plane + vi] = m;
+                if (model) model[(long long)yo * P.Nx + xo] = m;
                 float rr = m - P.obs[vi];
                 if (P.err) rr /= P.err[vi];
                 if (P.msk) rr *= P.msk[vi];
                 rr *= P.weight;
                 sum += rr * rr;
             }
+        }
+    }
+    // the computed box: rows [yo_lo, yb_end), columns [8 g_lo, xb_end)
+    const int yb_end = min(ob1, yo_lo + 8 * ngy), xb_end = min(P.Nx, 8 * g_hi + 8);
+    if (model) {
+        const int bw = P.Nx;
+        for (long long i = (long long)ob0 * bw + threadIdx.x; i < (long long)ob1 * bw;
+             i += blockDim.x) {
+            const int yo = (int)(i / bw), xo = (int)(i % bw);
+            if (yo < yo_lo || yo >= yb_end || xo < 8 * g_lo || xo >= xb_end) model[i] = 0.f;
         }
     }
 #pragma unroll
@@ -273,7 +390,41 @@ __global__ void __launch_bounds__(KB_THREADS) kb_psf_residual(BatchKernelArgs P)
     if (threadIdx.x == 0) {
         float s = 0.f;
         for (int w = 0; w < KB_THREADS / 32; ++w) s += warp_part[w];
-        P.partials[(long long)b * P.Nz + zo] = (double)s;
+        const double outside = sat_box(T, ld, ob0, ob1, 0, P.Nx) -
+                               sat_box(T, ld, yo_lo, yb_end, 8 * g_lo, xb_end);
+        P.partials[part] = (double)s + outside;
+    }
+}
+
+// summed-area table of the zero-model residual^2 of each data plane, in fp64:
+// T[y][x] = sum over y' < y, x' < x of ((0 - d) / e * m * weight)^2 (fp32 terms,
+// as the residual kernels compute them)
+__global__ void k_sat(BatchKernelArgs P, double* T)
+{
+    const int zo = blockIdx.x, ld = P.Nx + 1;
+    double* t = T + (long long)zo * (P.Ny + 1) * ld;
+    const long long base = (long long)zo * P.Ny * P.Nx;
+    for (int x = threadIdx.x; x <= P.Nx; x += blockDim.x) t[x] = 0.0;
+    for (int y = threadIdx.x; y < P.Ny; y += blockDim.x) {
+        double s = 0.0;
+        t[(long long)(y + 1) * ld] = 0.0;
+        for (int x = 0; x < P.Nx; ++x) {
+            const long long vi = base + (long long)y * P.Nx + x;
+            float rr = 0.f - P.obs[vi];
+            if (P.err) rr /= P.err[vi];
+            if (P.msk) rr *= P.msk[vi];
+            rr *= P.weight;
+            s += (double)(rr * rr);
+            t[(long long)(y + 1) * ld + x + 1] = s;
+        }
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < P.Nx; x += blockDim.x) {
+        double s = 0.0;
+        for (int y = 0; y < P.Ny; ++y) {
+            s += t[(long long)(y + 1) * ld + x + 1];
+            t[(long long)(y + 1) * ld + x + 1] = s;
+        }
     }
 }
 
@@ -544,42 +695,100 @@ struct gbkb200_batch {
     int direct = 0;
     size_t smemA = 0, smemB = 0;
     float *vr = nullptr, *ur = nullptr, *lsfr = nullptr, *mplanes = nullptr;
+    int* xr = nullptr;
+    double* sat = nullptr;
+    void (*kb)(BatchKernelArgs) = nullptr;
+    // per-stage timing: event pairs recorded around launches while enabled
+    int timing = 0;
+    std::vector<cudaEvent_t> ev;      // 2 per record
+    std::vector<int> ev_stage;
+    size_t ev_used = 0;
+    int ev_error = 0;
 };
 
-constexpr int KB_KMAX = 24;   // largest PSF box side of the direct path
+// records an event before (begin) or after (end) a launch of `stage`
+static void stage_mark(gbkb200_batch* bt, int stage, bool begin)
+{
+    if (!bt->timing || bt->ev_error) return;
+    const size_t i = begin ? 2 * bt->ev_used : 2 * bt->ev_used + 1;
+    if (i >= bt->ev.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            bt->ev_error = 1;
+            return;
+        }
+        bt->ev.push_back(e);
+    }
+    cudaEventRecord(bt->ev[i], bt->ctx->stream);
+    if (begin) {
+        if (bt->ev_stage.size() <= bt->ev_used) bt->ev_stage.resize(bt->ev_used + 1);
+        bt->ev_stage[bt->ev_used] = stage;
+    } else {
+        ++bt->ev_used;
+    }
+}
 
-// Direct-mode setup: reversed FIR coefficients, plane buffers and shared
-// memory sizes.  Returns GBKB200_ERR_UNSUPPORTED when the direct path does
-// not apply (PSF rank or size, cube size, shared memory).
+// the PSF kernel instantiated per odd FIR length
+typedef void (*KbFn)(BatchKernelArgs);
+constexpr int KB_KMIN = 5, KB_KMAX = 33;
+template<int K>
+static void kb_table(KbFn* t)
+{
+    t[(K - KB_KMIN) / 2] = kb_psf_residual<K>;
+    if constexpr (K + 2 <= KB_KMAX) kb_table<K + 2>(t);
+}
+static KbFn kb_fn(int K)
+{
+    static KbFn t[(KB_KMAX - KB_KMIN) / 2 + 1] = {};
+    if (!t[0]) kb_table<KB_KMIN>(t);
+    return t[(K - KB_KMIN) / 2];
+}
+
+// Direct-mode setup: reversed FIR coefficients, plane buffers, the data's
+// summed-area table and shared memory sizes.  Returns
+// GBKB200_ERR_UNSUPPORTED when the direct path does not apply (PSF rank or
+// size, cube size, shared memory).
 static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
 {
     BatchKernelArgs& P = bt->P;
     P.Kx = d->kernel_size[0];
     P.Ky = d->kernel_size[1];
     P.Kz = d->kernel_size[2];
-    P.rank = d->psf_rank;
-    if (P.rank < 1 || P.rank > 8 || !d->psf_u || !d->psf_v) return GBKB200_ERR_UNSUPPORTED;
-    if (P.Kx > KB_KMAX || P.Ky > KB_KMAX) return GBKB200_ERR_UNSUPPORTED;
-    P.Nxp = (P.Nx + 3) / 4 * 4;
-    const int items = (P.Nxp / 4) * ((P.Ny + 3) / 4);
-    if (items > KB_THREADS * KB_ITEMS) return GBKB200_ERR_UNSUPPORTED;
-    P.pitch = (std::max(P.Wx, P.Nxp + KB_KMAX) + 3) / 4 * 4;
-    bt->smemA = (size_t)P.Nz * P.pitch * sizeof(float) +
+    if (d->psf_rank != 1 || !d->psf_u || !d->psf_v) return GBKB200_ERR_UNSUPPORTED;
+    P.K = std::max(KB_KMIN, std::max(P.Kx, P.Ky) | 1);
+    if (P.K > KB_KMAX || P.Nx > 8 * KB_THREADS || P.Wx > 32767) return GBKB200_ERR_UNSUPPORTED;
+    const int NW = (P.K + 7 + 3) / 4;
+    P.pitch = (P.Wx + 3) / 4 * 4;
+    P.tpitch = P.pitch + 1;
+    P.tile_floats = (P.Nz * P.tpitch + 3) / 4 * 4;
+    P.sp = 8 * ((P.Nx - 1) / 8) + 4 * NW;
+    P.sp += ((4 - P.sp % 32) + 32) % 32;
+    bt->smemA = (size_t)P.tile_floats * sizeof(float) +
                 (size_t)(KA_THREADS / 32) * P.Wz * sizeof(float) +
                 (size_t)P.Wx * (4 * sizeof(float) + 2 * sizeof(int)) + P.Kz * sizeof(float) + 16;
-    bt->smemB = ((size_t)P.Wy * P.pitch + (size_t)P.Wy * P.Nxp) * sizeof(float);
-    const size_t lim = 227 * 1024;
-    if (bt->smemA > lim || bt->smemB > lim) return GBKB200_ERR_UNSUPPORTED;
-    std::vector<float> vr((size_t)P.rank * P.Kx), ur((size_t)P.rank * P.Ky), lr(P.Kz);
-    for (int r = 0; r < P.rank; ++r) {
-        for (int s = 0; s < P.Kx; ++s) vr[r * P.Kx + s] = (float)d->psf_v[r * P.Kx + P.Kx - 1 - s];
-        for (int t = 0; t < P.Ky; ++t) ur[r * P.Ky + t] = (float)d->psf_u[r * P.Ky + P.Ky - 1 - t];
-    }
+    // bands of output rows: two PSF blocks per SM when they fit
+    const size_t lim = 227 * 1024, two = 113 * 1024;
+    auto smem_b = [&](int band) {
+        return (size_t)(band + P.K - 1) * (P.sp + 1) * sizeof(float);
+    };
+    int band = P.Ny;
+    while (band > 8 && smem_b(band) > two) band = (band + 1) / 2;
+    if (smem_b(band) > lim) return GBKB200_ERR_UNSUPPORTED;
+    P.nbands = (P.Ny + band - 1) / band;
+    P.band = (P.Ny + P.nbands - 1) / P.nbands;
+    bt->smemB = smem_b(P.band);
+    if (bt->smemA > lim) return GBKB200_ERR_UNSUPPORTED;
+    std::vector<float> vr(P.K, 0.f), ur(P.K, 0.f), lr(P.Kz);
+    for (int s = 0; s < P.Kx; ++s) vr[s] = (float)d->psf_v[P.Kx - 1 - s];
+    for (int t = 0; t < P.Ky; ++t) ur[t] = (float)d->psf_u[P.Ky - 1 - t];
     for (int t = 0; t < P.Kz; ++t) lr[t] = (float)d->lsf[P.Kz - 1 - t];
+    const size_t nrows = (size_t)bt->chunk * P.Nz * P.Wy;
     if (cudaMalloc(&bt->vr, vr.size() * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&bt->ur, ur.size() * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&bt->lsfr, lr.size() * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&bt->mplanes, (size_t)bt->chunk * P.Nz * P.Wy * P.pitch * sizeof(float)) !=
+        cudaMalloc(&bt->mplanes, nrows * P.pitch * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&bt->xr, nrows * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&bt->sat, (size_t)P.Nz * (P.Ny + 1) * (P.Nx + 1) * sizeof(double)) !=
             cudaSuccess)
         return GBKB200_ERR_OOM;
     GBK_CUDA_TRY(cudaMemcpy(bt->vr, vr.data(), vr.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -589,12 +798,17 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.ur = bt->ur;
     P.lsfr = bt->lsfr;
     P.mplanes = bt->mplanes;
+    P.xr = bt->xr;
+    P.sat = bt->sat;
+    k_sat<<<P.Nz, 128, 0, bt->ctx->stream>>>(P, bt->sat);
+    GBK_CUDA_TRY(cudaGetLastError());
+    GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
     GBK_CUDA_TRY(cudaFuncSetAttribute(ka_lines_lsf, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)bt->smemA));
-    GBK_CUDA_TRY(cudaFuncSetAttribute(kb_psf_residual<KB_KMAX, KB_KMAX>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+    bt->kb = kb_fn(P.K);
+    GBK_CUDA_TRY(cudaFuncSetAttribute(bt->kb, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)bt->smemB));
-    bt->nper = P.Nz;
+    bt->nper = P.Nz * P.nbands;
     if (cudaMalloc(&bt->partials, (size_t)bt->max_sets * bt->nper * sizeof(double)) != cudaSuccess)
         return GBKB200_ERR_OOM;
     P.partials = bt->partials;
@@ -654,6 +868,9 @@ extern "C" int gbkb200_batch_destroy(gbkb200_batch* bt)
     cudaFree(bt->ur);
     cudaFree(bt->lsfr);
     cudaFree(bt->mplanes);
+    cudaFree(bt->xr);
+    cudaFree(bt->sat);
+    for (cudaEvent_t e : bt->ev) cudaEventDestroy(e);
     delete bt;
     return GBKB200_OK;
 }
@@ -863,33 +1080,81 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
         for (int s0 = 0; s0 < nsets; s0 += bt->chunk) {
             const int cn = std::min(bt->chunk, nsets - s0);
             P.set0 = s0;
+            stage_mark(bt, 0, true);
             ka_lines_lsf<<<dim3(P.Wy, cn), KA_THREADS, bt->smemA, st>>>(P, bt->ctx->d_status);
-            kb_psf_residual<KB_KMAX, KB_KMAX><<<dim3(P.Nz, cn), KB_THREADS, bt->smemB, st>>>(P);
+            stage_mark(bt, 0, false);
+            stage_mark(bt, 4, true);
+            bt->kb<<<dim3(P.Nz * P.nbands, cn), KB_THREADS, bt->smemB, st>>>(P);
+            stage_mark(bt, 4, false);
         }
+        stage_mark(bt, 5, true);
         if (nsets > 0) k6_sum<<<nsets, 256, 0, st>>>(P.partials, bt->nper, 0, chi2);
+        stage_mark(bt, 5, false);
         GBK_CUDA_TRY(cudaGetLastError());
         return gbk_finish(bt->ctx);
     }
     for (int s0 = 0; s0 < nsets; s0 += bt->chunk) {
         const int cn = std::min(bt->chunk, nsets - s0);
         P.set0 = s0;
+        stage_mark(bt, 0, true);
         k1_model_xfft<<<dim3(P.Wy, cn), 512, bt->smem1, st>>>(P, bt->ctx->d_status);
+        stage_mark(bt, 0, false);
+        stage_mark(bt, 1, true);
         // K2: y forward over (z < Wz, kx); columns stride hx, outer stride Py * hx
         k_lines<<<dim3(tiles * P.Wz, cn), 256, bt->smem_y, st>>>(
             P.work, set_stride, P.hx, (long long)P.Py * P.hx, P.hx, P.ay, 0, 0, nullptr, 0, 0,
             1.f, P.Wy, 0, P.Py, P.lim_work, lim_spec);
+        stage_mark(bt, 1, false);
+        stage_mark(bt, 2, true);
         // K3: z conv over (y < Py, kx); element stride Py * hx
         k_lines<<<dim3(tiles * P.Py, cn), 256, bt->smem_z, st>>>(
             P.work, set_stride, P.hx, P.hx, (long long)P.Py * P.hx, P.az, 0, 1, P.kspec, P.hx,
             (long long)P.Py * P.hx, P.scale, P.Wz, P.ez, P.Nz, P.lim_work, lim_spec);
+        stage_mark(bt, 2, false);
+        stage_mark(bt, 3, true);
         // K4: y inverse over (z < Nz, kx)
         k_lines<<<dim3(tiles * P.Nz, cn), 256, bt->smem_y, st>>>(
             P.work, set_stride, P.hx, (long long)P.Py * P.hx, P.hx, P.ay, 1, 0, nullptr, 0, 0,
             1.f, P.Py, P.ey, P.Ny, P.lim_work, lim_spec);
+        stage_mark(bt, 3, false);
+        stage_mark(bt, 4, true);
         k5_c2r_residual<<<dim3((P.Ny + P.rows_k5 - 1) / P.rows_k5, P.Nz, cn), 256, bt->smem5,
                           st>>>(P);
+        stage_mark(bt, 4, false);
     }
+    stage_mark(bt, 5, true);
     if (nsets > 0) k6_sum<<<nsets, 256, 0, st>>>(P.partials, bt->nper, 0, chi2);
+    stage_mark(bt, 5, false);
     GBK_CUDA_TRY(cudaGetLastError());
     return gbk_finish(bt->ctx);
+}
+
+extern "C" int gbkb200_batch_set_timing(gbkb200_batch* bt, int enable)
+{
+    if (!bt) return GBKB200_ERR_INVALID_ARG;
+    bt->timing = enable ? 1 : 0;
+    bt->ev_used = 0;
+    bt->ev_error = 0;
+    return GBKB200_OK;
+}
+
+extern "C" int gbkb200_batch_timing(gbkb200_batch* bt, double ms[GBKB200_BATCH_STAGES],
+                                    int launches[GBKB200_BATCH_STAGES])
+{
+    if (!bt || !ms || !launches) return GBKB200_ERR_INVALID_ARG;
+    for (int s = 0; s < GBKB200_BATCH_STAGES; ++s) {
+        ms[s] = 0.0;
+        launches[s] = 0;
+    }
+    GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
+    const int failed = bt->ev_error;
+    for (size_t i = 0; i < bt->ev_used && !failed; ++i) {
+        float t = 0.f;
+        GBK_CUDA_TRY(cudaEventElapsedTime(&t, bt->ev[2 * i], bt->ev[2 * i + 1]));
+        ms[bt->ev_stage[i]] += t;
+        launches[bt->ev_stage[i]] += 1;
+    }
+    bt->ev_used = 0;
+    bt->ev_error = 0;
+    return failed ? GBKB200_ERR_OOM : GBKB200_OK;
 }

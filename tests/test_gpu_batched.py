@@ -112,3 +112,53 @@ def test_batched_direct_mode_selection(gpu):
     ev.evaluate_device(bufs, 2, model=model)
     ref = scube_pipeline(w.disk.pack(workloads.set_params(w, 1)), w.geom)
     assert rel_err(model[1].cpu().numpy(), ref) < 2e-5
+
+
+def test_batched_direct_bands_wide_psf(gpu, oracle_built):
+    """Direct mode on a wide cube whose planes are split into bands of rows
+    (shared memory) with a large PSF box (FWHM 4 px): cube, chi^2 and the
+    zero model outside each plane's nonzero box agree with the oracle."""
+    import torch
+    from oracle.oracle import chi2, scube_pipeline
+    from gbkfit_b200 import psflsf, workloads
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    w = workloads.smdisk_batch128(nsets=3, size=(200, 180, 24), nnodes=12)
+    w.geom = workloads.Geometry(w.geom.size, w.geom.step, (0, 0, (w.geom.size[2] - 1) / 2),
+                                (0, 0, 0), psflsf.PSFGauss(psflsf.gauss_fwhm_to_sigma(4.0)),
+                                w.geom.lsf)
+    w.params['xpos'] = np.array([100.0, 60.0, 150.0])
+    w.params['ypos'] = np.array([90.0, 40.0, 120.0])
+    w.extra['truth']['xpos'], w.extra['truth']['ypos'] = 100.0, 90.0
+    assert w.geom.kernel_size[0] > 25
+    data, err, _ = synthetic_data(w)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=3, chunk=2, conv='direct')
+    bufs = ev.alloc_inputs(3)
+    ev.upload(ev.pack(w.params, 3), bufs, 3)
+    model = torch.full((3,) + tuple(w.geom.size[::-1]), 7.0, device='cuda')
+    got = ev.evaluate_device(bufs, 3, model=model).cpu().numpy()
+    model = model.cpu().numpy()
+    for i in range(3):
+        ref = scube_pipeline(w.disk.pack(workloads.set_params(w, i)), w.geom)
+        ref32 = scube_pipeline(w.disk.pack(workloads.set_params(w, i)), w.geom, precision='f32')
+        assert rel_err(model[i], ref) <= max(1e-5, 1.5 * rel_err(ref32, ref)), i
+        assert not np.any(model[i] == 7.0), i     # every voxel written
+        c_ref = chi2(ref, data, err)
+        assert abs(got[i] - c_ref) / c_ref < 1e-4, (i, got[i], c_ref)
+
+
+def test_batched_direct_empty_planes(gpu, oracle_built):
+    """A disk whose lines fall outside most channels (large vsys): the empty
+    planes' chi^2 comes from the data table alone and matches the oracle."""
+    from oracle.oracle import chi2, scube_pipeline
+    from gbkfit_b200 import workloads
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    w = _small_batch_workload(2)
+    data, err, _ = synthetic_data(w)
+    w.params['vsys'] = np.array([-300.0, 2000.0])
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=2, conv='direct')
+    got = ev.evaluate(w.params, 2)
+    for i in range(2):
+        ref = scube_pipeline(w.disk.pack(workloads.set_params(w, i)), w.geom)
+        c_ref = chi2(ref, data, err)
+        assert abs(got[i] - c_ref) / c_ref < 1e-4, (i, got[i], c_ref)
+    assert abs(got[1] - chi2(0 * data, data, err)) / got[1] < 1e-6
