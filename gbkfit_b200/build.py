@@ -2,8 +2,11 @@
 
 import glob
 import os
+import shutil
 import subprocess
 import sys
+import tempfile
+from concurrent.futures import ThreadPoolExecutor
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(_HERE)
@@ -11,7 +14,7 @@ CSRC = os.path.join(_HERE, 'csrc')
 OUT = os.path.join(_HERE, 'libgbkb200.so')
 
 NVCC_FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-O3', '-lineinfo', '-std=c++17',
-              '-Xcompiler', '-fPIC', '-shared', '-diag-suppress', '39']
+              '-Xcompiler', '-fPIC', '-diag-suppress', '39']
 
 
 def sources():
@@ -28,17 +31,38 @@ def _stale():
 
 
 def build(force=False, verbose=False, checked=False):
-    """Compile every .cu under csrc/ into gbkfit_b200/libgbkb200.so, or with
-    checked=True into the bounds-checked debug build libgbkb200_checked.so."""
+    """Compile every .cu under csrc/ (one object per file, in parallel) and
+    link gbkfit_b200/libgbkb200.so, or with checked=True the bounds-checked
+    debug build libgbkb200_checked.so."""
     out = OUT.replace('.so', '_checked.so') if checked else OUT
     if not force and not checked and not _stale():
         return out
     nvcc = os.environ.get('NVCC', 'nvcc')
-    cmd = [nvcc] + NVCC_FLAGS + (['-DGBK_CHECKED'] if checked else []) + \
-        ['-o', out + '.tmp'] + sources()
-    if verbose:
-        print(' '.join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True, cwd=ROOT)
+    flags = NVCC_FLAGS + (['-DGBK_CHECKED'] if checked else [])
+    tmp = tempfile.mkdtemp(prefix='gbkb200_build_')
+    try:
+        objs = [os.path.join(tmp, os.path.basename(src)[:-3] + '.o') for src in sources()]
+
+        def compile_one(src_obj):
+            cmd = [nvcc] + flags + ['-c', '-o', src_obj[1], src_obj[0]]
+            if verbose:
+                print(' '.join(cmd), file=sys.stderr)
+            return subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True)
+
+        with ThreadPoolExecutor(max_workers=max(1, min(len(objs), os.cpu_count() or 1))) as ex:
+            results = list(ex.map(compile_one, zip(sources(), objs)))
+        for src, r in zip(sources(), results):
+            if r.stderr.strip() and (verbose or r.returncode):
+                print(r.stderr, file=sys.stderr)
+            if r.returncode:
+                raise subprocess.CalledProcessError(r.returncode, 'nvcc ' + src)
+        cmd = [nvcc, '-gencode', 'arch=compute_100a,code=sm_100a', '-shared', '-o',
+               out + '.tmp'] + objs
+        if verbose:
+            print(' '.join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True, cwd=ROOT)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
     os.replace(out + '.tmp', out)
     return out
 

@@ -25,7 +25,7 @@
 //   K6  per set, the partials summed in a fixed order in fp64.
 // Sets run in chunks whose intermediates (Wz x Py x hx complex each) stay in
 // the 126 MB L2 between stages.
-#include "gbk_disk.cuh"
+#include "gbk_batched.cuh"
 #include "gbk_fft.cuh"
 
 #include <climits>
@@ -34,365 +34,15 @@
 
 namespace gbk {
 
-struct BatchKernelArgs {
-    int Nx, Ny, Nz, Wx, Wy, Wz, Px, Py, Pz, hx, ex, ey, ez;
-    int rows_k1;     // z rows per shared-memory group in K1
-    int rows_k5;     // y rows per block in K5
-    DiskArgs disk;   // per-set pointers are offset from set 0 by the strides
-    int vstride[5];  // vsys, xpos, ypos, posa, incl values per set
-    int pstride[9];  // trait parameter values per set, per kind
-    AxisDev ax, ay, az;
-    const float2* post;   // exp(-2 pi i k / Px), k in [0, Px/2]
-    const float2* kspec;  // PSF x LSF spectrum (Pz, Py, hx)
-    float scale;          // 1 / (Px Py Pz)
-    const float *obs, *err, *msk;
-    float weight;
-    float2* work;         // (chunk, Wz, Py, hx)
-    float* model;         // optional (nsets, Nz, Ny, Nx)
-    double* partials;     // (nsets, Nz, ceil(Ny / rows_k5))
-    int set0;
-    // element counts of the buffers (bounds of the checked build)
-    long long lim_work, lim_model, lim_part, lim_obs, lim_smem1, lim_smem5;
-    // direct (separable) convolution
-    int Kx, Ky, Kz;       // PSF (x, y) and LSF box sizes
-    int K;                // FIR length of the PSF kernel (odd, >= Kx, Ky; zero-padded taps)
-    int pitch;            // row pitch of the LSF-convolved planes in HBM (floats, % 4 == 0)
-    int tpitch;           // row pitch of the model kernel's shared tile (odd: no bank conflicts)
-    int tile_floats;      // Nz * tpitch rounded up to 4
-    int sp;               // row pitch of the PSF kernel's shared rows (floats, % 32 == 4)
-    int band, nbands;     // output rows per PSF block, bands per plane
-    const float* vr;      // (K): PSF x factor, reversed
-    const float* ur;      // (K): PSF y factor, reversed
-    const float* lsfr;    // (Kz): LSF reversed
-    float* mplanes;       // (chunk, Nz, Wy, pitch): only the xr segments are written
-    int* xr;              // (chunk, Nz, Wy): nonzero x range of each plane row, or -1
-    const double* sat;    // (Nz, Ny + 1, Nx + 1): summed-area table of the zero-model r^2
-};
-
-// ---- direct convolution: LSF FIR per column, separable PSF FIR per plane ----
-//
-// Crop output (zo, yo, xo) of the reference's FFT convolution equals
-//   sum_t sum_sy sum_sx  lsf[Kz-1-t] psf[Ky-1-sy][Kx-1-sx] model(zo+t, yo+sy, xo+sx)
-// in window coordinates (the padded grid's first W indices): the kernel is
-// PSF(x, y) x LSF(z), and PSF = u(y) v(x) (rank 1: a circular Gaussian's
-// 8-sigma truncation corners are ~1e-14 of the peak).
-//
-// Sparsity: a line is exactly zero outside its +-5 sigma channel window and
-// off the disk, so each LSF-convolved plane is nonzero only in a band of
-// rows and columns.  The model kernel records each plane row's nonzero x
-// range; the PSF kernel convolves only the bounding box of its plane (sums
-// of exact zeros are exact zeros, so results do not change) and takes the
-// residual outside the box, where the model is exactly 0, from a summed-area
-// table of ((0 - data) / error * mask * weight)^2 built once per data cube.
-
-__device__ __forceinline__ DiskArgs set_disk(const BatchKernelArgs& P, int b);
-
-// KA: one block per (set, window row y): the row's spaxel lines, each spectral
-// column convolved with the LSF (a warp per spaxel), then per output plane the
-// nonzero x segment of the row (aligned to 4) and its range.
-constexpr int KA_THREADS = 256;
-
-__global__ void __launch_bounds__(KA_THREADS, 3) ka_lines_lsf(BatchKernelArgs P, int* status)
+// per-voxel residual factor of the direct path: mask * weight / error
+__global__ void k_iw(BatchKernelArgs P, float* iw, long long n)
 {
-    extern __shared__ float4 sm4[];
-    const int tp = P.tpitch;
-    float* tile = reinterpret_cast<float*>(sm4);          // (Nz, tp)
-    float* lbuf = tile + P.tile_floats;                    // (nwarps, Wz)
-    float* s_v = lbuf + (KA_THREADS / 32) * P.Wz;
-    float* s_amp = s_v + P.Wx;
-    float* s_i2 = s_amp + P.Wx;
-    float* s_orv = s_i2 + P.Wx;
-    float* s_lsf = s_orv + P.Wx;
-    int* s_lo = reinterpret_cast<int*>(s_lsf + P.Kz);
-    int* s_hi = s_lo + P.Wx;
-    const int y = blockIdx.x, c = blockIdx.y, b = P.set0 + c;
-    const DiskArgs a = set_disk(P, b);
-    int bad = 0;
-    for (int i = threadIdx.x; i < P.Kz; i += blockDim.x) s_lsf[i] = P.lsfr[i];
-    const DiskConst kc = disk_const(a);
-    for (int x = threadIdx.x; x < P.Wx; x += blockDim.x) {
-        SpaxelOut o;
-        int lo = INT_MAX, hi = -1;
-        float amp = 0, i2 = 1;
-        if (smdisk_spaxel(a, kc, x, y, 0, o, bad) &&
-            line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo, hi)) {
-            amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
-            i2 = 2 * o.dv * o.dv;
-        } else {
-            lo = INT_MAX;
-            hi = -1;
-        }
-        s_v[x] = o.vv;
-        s_amp[x] = amp;
-        s_i2[x] = i2;
-        s_orv[x] = o.orv;
-        s_lo[x] = lo;
-        s_hi[x] = hi;
-    }
-    float4* t4 = reinterpret_cast<float4*>(tile);
-    for (int i = threadIdx.x; i < P.tile_floats / 4; i += blockDim.x)
-        t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    float* L = lbuf + warp * P.Wz;
-    for (int x = warp; x < P.Wx; x += nwarps) {
-        const int lo = s_lo[x], hi = s_hi[x];
-        if (lo > hi) continue;
-        const float v = s_v[x], amp = s_amp[x], i2 = s_i2[x], orv = s_orv[x];
-        // gmodels.hpp:109-115: the line, channel by channel (window coordinates)
-        for (int z = lo + lane; z <= hi; z += 32) {
-            float zv = a.spec_zero + z * a.spec_step;
-            float d = zv - v;
-            L[z - lo] = orv * (amp * expf(-d * d / i2));
-        }
-        __syncwarp();
-        const int zo0 = max(0, lo - P.Kz + 1), zo1 = min(P.Nz - 1, hi);
-        for (int zo = zo0 + lane; zo <= zo1; zo += 32) {
-            float acc = 0.f;
-            const int t0 = max(0, lo - zo), t1 = min(P.Kz - 1, hi - zo);
-            for (int t = t0; t <= t1; ++t) acc += s_lsf[t] * L[zo + t - lo];
-            tile[zo * tp + x] = acc;
-        }
-        __syncwarp();
-    }
-    __syncthreads();
-    // per output plane: the row's nonzero x range (ballots over the spaxels
-    // whose convolved line reaches zo), then its 4-aligned segment
-    for (int zo = warp; zo < P.Nz; zo += nwarps) {
-        int xmin = INT_MAX, xmax = -1;
-        for (int x0 = 0; x0 < P.Wx; x0 += 32) {
-            const int x = x0 + lane;
-            bool on = false;
-            if (x < P.Wx) {
-                const int lo = s_lo[x], hi = s_hi[x];
-                on = lo <= hi && zo >= lo - P.Kz + 1 && zo <= hi;
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, on);
-            if (m) {
-                xmin = min(xmin, x0 + __ffs(m) - 1);
-                xmax = max(xmax, x0 + 31 - __clz(m));
-            }
-        }
-        const long long row = ((long long)c * P.Nz + zo) * P.Wy + y;
-        if (xmax < 0) {
-            if (lane == 0) P.xr[row] = -1;
-            continue;
-        }
-        if (lane == 0) P.xr[row] = xmin | (xmax << 16);
-        float* dst = P.mplanes + row * P.pitch;
-        const float* srow = tile + zo * tp;
-        for (int x = (xmin & ~3) + lane; x <= (xmax | 3); x += 32) dst[x] = srow[x];
-    }
-    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
-}
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_wait_all()
-{
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-}
-
-// sum of the summed-area table over rows [y0, y1) and columns [x0, x1)
-__device__ __forceinline__ double sat_box(const double* T, int ld, int y0, int y1, int x0, int x1)
-{
-    return T[(long long)y1 * ld + x1] - T[(long long)y0 * ld + x1] - T[(long long)y1 * ld + x0] +
-           T[(long long)y0 * ld + x0];
-}
-
-// KB: one block per (set, output plane zo, band of output rows): the bounding
-// box of the band's nonzero input rows is loaded (cp.async), convolved in x in
-// place (8 outputs per thread and window, whole rows per round), then in y
-// (8 x 4 outputs per item) with the crop, residual (objective.hpp:7-31) and
-// r^2 fused; the zero-model residual outside the box comes from the table.
-constexpr int KB_THREADS = 256;
-
-template<int K>
-__global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs P)
-{
-    constexpr int NW = (K + 7 + 3) / 4;     // float4 slots of one 8-output x window
-    extern __shared__ float4 sm4[];
-    float* S = reinterpret_cast<float*>(sm4);                   // (band + K - 1, sp)
-    const int rows_in = P.band + K - 1;
-    int* s_xr = reinterpret_cast<int*>(S + (long long)rows_in * P.sp);
-    __shared__ int s_box[4];
-    __shared__ float warp_part[KB_THREADS / 32];
-    const int zo = blockIdx.x / P.nbands, band = blockIdx.x % P.nbands;
-    const int c = blockIdx.y, b = P.set0 + c;
-    const int ob0 = band * P.band, ob1 = min(P.Ny, ob0 + P.band);  // output rows [ob0, ob1)
-    const int in1 = min(P.Wy, ob1 + K - 1);                        // input rows [ob0, in1)
-    const long long prow = ((long long)c * P.Nz + zo) * P.Wy;
-    const int ld = P.Nx + 1;
-    const double* T = P.sat + (long long)zo * (P.Ny + 1) * ld;
-    if (threadIdx.x < 32) {
-        int y0 = INT_MAX, y1 = -1, x0 = INT_MAX, x1 = -1;
-        for (int y = ob0 + threadIdx.x; y < in1; y += 32) {
-            const int v = P.xr[prow + y];
-            s_xr[y - ob0] = v;
-            if (v >= 0) {
-                y0 = min(y0, y);
-                y1 = max(y1, y);
-                x0 = min(x0, v & 0xffff);
-                x1 = max(x1, v >> 16);
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
-            y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
-            x0 = min(x0, __shfl_xor_sync(0xffffffffu, x0, o));
-            x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, o));
-        }
-        if (threadIdx.x == 0) {
-            s_box[0] = y0; s_box[1] = y1; s_box[2] = x0; s_box[3] = x1;
-        }
-    }
-    __syncthreads();
-    const int y0 = s_box[0], y1 = s_box[1], x0 = s_box[2], x1 = s_box[3];
-    const long long plane = (long long)P.Ny * P.Nx;
-    float* model = P.model ? P.model + ((long long)b * P.Nz + zo) * plane : nullptr;
-    const long long part = ((long long)b * P.Nz + zo) * P.nbands + band;
-    if (y1 < 0) {   // nothing reaches this band: the model is 0 on it
-        if (model)
-            for (long long i = (long long)ob0 * P.Nx + threadIdx.x; i < (long long)ob1 * P.Nx;
-                 i += blockDim.x)
-                model[i] = 0.f;
-        if (threadIdx.x == 0) P.partials[part] = sat_box(T, ld, ob0, ob1, 0, P.Nx);
-        return;
-    }
-    // output box: x in 8-column strips [g_lo, g_hi], y rows [yo_lo, yo_hi]
-    const int g_lo = max(0, x0 - K + 1) >> 3, g_hi = min(P.Nx - 1, x1) >> 3;
-    const int ns8 = g_hi - g_lo + 1;
-    const int yo_lo = max(ob0, y0 - K + 1), yo_hi = min(ob1 - 1, y1);
-    // load rows [y0, y1], float4 slots [2 g_lo, 2 g_hi + NW): the row's
-    // segment from HBM, zeros elsewhere
-    {
-        const int nsl = 2 * (ns8 - 1) + NW, sl0 = 2 * g_lo;
-        const int nrows = y1 - y0 + 1;
-        const float4* src = reinterpret_cast<const float4*>(P.mplanes + prow * P.pitch);
-        for (int i = threadIdx.x; i < nrows * nsl; i += blockDim.x) {
-            const int y = y0 + i / nsl, sl = sl0 + i % nsl;
-            const int v = s_xr[y - ob0];
-            float4* d = reinterpret_cast<float4*>(S + (long long)(y - ob0) * P.sp) + sl;
-            if (v >= 0 && sl >= (v & 0xffff) >> 2 && sl <= (v >> 16) >> 2)
-                cp_async16(d, src + (long long)y * (P.pitch / 4) + sl);
-            else
-                *d = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        cp_async_wait_all();
-    }
-    __syncthreads();
-    // x FIR in place: S[y][xo] = sum_s vr[s] S[y][xo + s] for xo in the strips;
-    // a round covers whole rows, loads before the barrier, stores after it
-    {
-        float vr[K];
-#pragma unroll
-        for (int s = 0; s < K; ++s) vr[s] = P.vr[s];
-        const int rpr = max(1, (int)blockDim.x / ns8);
-        const int rr = threadIdx.x % rpr, g = g_lo + threadIdx.x / rpr;
-        for (int r0 = y0; r0 <= y1; r0 += rpr) {
-            const int y = r0 + rr;
-            const bool act = g <= g_hi && y <= y1;
-            float w[4 * NW];
-            float4* row = reinterpret_cast<float4*>(S + (long long)(y - ob0) * P.sp) + 2 * g;
-            if (act) {
-#pragma unroll
-                for (int m = 0; m < NW; ++m) {
-                    const float4 f = row[m];
-                    w[4 * m] = f.x; w[4 * m + 1] = f.y; w[4 * m + 2] = f.z; w[4 * m + 3] = f.w;
-                }
-            }
-            __syncthreads();
-            if (act) {
-                float o[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    float acc = 0.f;
-#pragma unroll
-                    for (int s = 0; s < K; ++s) acc += vr[s] * w[q + s];
-                    o[q] = acc;
-                }
-                row[0] = make_float4(o[0], o[1], o[2], o[3]);
-                row[1] = make_float4(o[4], o[5], o[6], o[7]);
-            }
-        }
-    }
-    __syncthreads();
-    // y FIR + crop + residual: items of 8 output rows x 4 columns
-    float ur[K];
-#pragma unroll
-    for (int t = 0; t < K; ++t) ur[t] = P.ur[t];
-    const int ngy = (yo_hi - yo_lo + 8) / 8, s4_lo = 2 * g_lo, ns4 = 2 * ns8;
-    const int items = ngy * ns4;
-    float sum = 0.f;
-    for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int gy = it / ns4, s4 = s4_lo + it % ns4;
-        const int yb = yo_lo + 8 * gy;
-        float acc[8][4];
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-#pragma unroll
-            for (int k = 0; k < 4; ++k) acc[q][k] = 0.f;
-#pragma unroll
-        for (int m = 0; m < K + 7; ++m) {
-            const int y = yb + m;
-            const float4 p = (y >= y0 && y <= y1)
-                ? reinterpret_cast<const float4*>(S + (long long)(y - ob0) * P.sp)[s4]
-                : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int t = m - q;
-                if (t >= 0 && t < K) {
-                    acc[q][0] += ur[t] * p.x;
-                    acc[q][1] += ur[t] * p.y;
-                    acc[q][2] += ur[t] * p.z;
-                    acc[q][3] += ur[t] * p.w;
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int yo = yb + q;
-            if (yo >= ob1) break;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int xo = 4 * s4 + k;
-                if (xo >= P.Nx) break;
-                const float m = acc[q][k];
-                const long long vi = (long long)zo * plane + (long long)yo * P.Nx + xo;
-                if (model) model[(long long)yo * P.Nx + xo] = m;
-                float rr = m - P.obs[vi];
-                if (P.err) rr /= P.err[vi];
-                if (P.msk) rr *= P.msk[vi];
-                rr *= P.weight;
-                sum += rr * rr;
-            }
-        }
-    }
-    // the computed box: rows [yo_lo, yb_end), columns [8 g_lo, xb_end)
-    const int yb_end = min(ob1, yo_lo + 8 * ngy), xb_end = min(P.Nx, 8 * g_hi + 8);
-    if (model) {
-        const int bw = P.Nx;
-        for (long long i = (long long)ob0 * bw + threadIdx.x; i < (long long)ob1 * bw;
-             i += blockDim.x) {
-            const int yo = (int)(i / bw), xo = (int)(i % bw);
-            if (yo < yo_lo || yo >= yb_end || xo < 8 * g_lo || xo >= xb_end) model[i] = 0.f;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = sum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float s = 0.f;
-        for (int w = 0; w < KB_THREADS / 32; ++w) s += warp_part[w];
-        const double outside = sat_box(T, ld, ob0, ob1, 0, P.Nx) -
-                               sat_box(T, ld, yo_lo, yb_end, 8 * g_lo, xb_end);
-        P.partials[part] = (double)s + outside;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        float w = P.weight;
+        if (P.msk) w *= P.msk[i];
+        if (P.err) w /= P.err[i];
+        iw[i] = w;
     }
 }
 
@@ -428,20 +78,6 @@ __global__ void k_sat(BatchKernelArgs P, double* T)
     }
 }
 
-__device__ __forceinline__ DiskArgs set_disk(const BatchKernelArgs& P, int b)
-{
-    DiskArgs a = P.disk;
-    if (a.vsys) a.vsys += (long long)b * P.vstride[0];
-    a.xpos += (long long)b * P.vstride[1];
-    a.ypos += (long long)b * P.vstride[2];
-    a.posa += (long long)b * P.vstride[3];
-    a.incl += (long long)b * P.vstride[4];
-    TraitSet* ts[9] = {&a.rpt, &a.rht, &a.vpt, &a.vht, &a.dpt, &a.dht, &a.zpt, &a.spt, &a.wpt};
-#pragma unroll
-    for (int k = 0; k < 9; ++k)
-        if (ts[k]->pv) ts[k]->pv += (long long)b * P.pstride[k];
-    return a;
-}
 
 // K1: model row + x-axis r2c.  Shared memory: two (rows_k1 x Px/2) complex
 // buffers, the x twiddles, the post twiddles and 5 floats + 2 ints per spaxel.
@@ -697,7 +333,9 @@ struct gbkb200_batch {
     float *vr = nullptr, *ur = nullptr, *lsfr = nullptr, *mplanes = nullptr;
     int* xr = nullptr;
     double* sat = nullptr;
+    float* iw = nullptr;
     void (*kb)(BatchKernelArgs) = nullptr;
+    void (*ka)(BatchKernelArgs, int*) = nullptr;
     // per-stage timing: event pairs recorded around launches while enabled
     int timing = 0;
     std::vector<cudaEvent_t> ev;      // 2 per record
@@ -728,19 +366,20 @@ static void stage_mark(gbkb200_batch* bt, int stage, bool begin)
     }
 }
 
-// the PSF kernel instantiated per odd FIR length
-typedef void (*KbFn)(BatchKernelArgs);
-constexpr int KB_KMIN = 5, KB_KMAX = 33;
-template<int K>
-static void kb_table(KbFn* t)
+static KaFn ka_fn(int Kz)
 {
-    t[(K - KB_KMIN) / 2] = kb_psf_residual<K>;
-    if constexpr (K + 2 <= KB_KMAX) kb_table<K + 2>(t);
+    static KaFn t[KA_KMAX / 2 + 1] = {};
+    if (!t[0]) {
+        ka_register_short(t);
+        ka_register_long(t);
+    }
+    return t[Kz / 2];
 }
+
 static KbFn kb_fn(int K)
 {
     static KbFn t[(KB_KMAX - KB_KMIN) / 2 + 1] = {};
-    if (!t[0]) kb_table<KB_KMIN>(t);
+    if (!t[0]) kb_register(t);
     return t[(K - KB_KMIN) / 2];
 }
 
@@ -756,7 +395,8 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.Kz = d->kernel_size[2];
     if (d->psf_rank != 1 || !d->psf_u || !d->psf_v) return GBKB200_ERR_UNSUPPORTED;
     P.K = std::max(KB_KMIN, std::max(P.Kx, P.Ky) | 1);
-    if (P.K > KB_KMAX || P.Nx > 8 * KB_THREADS || P.Wx > 32767) return GBKB200_ERR_UNSUPPORTED;
+    if (P.K > KB_KMAX || P.Kz > KA_KMAX || P.Nx > 8 * KB_THREADS || P.Wx > 32767)
+        return GBKB200_ERR_UNSUPPORTED;
     const int NW = (P.K + 7 + 3) / 4;
     P.pitch = (P.Wx + 3) / 4 * 4;
     P.tpitch = P.pitch + 1;
@@ -764,8 +404,8 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.sp = 8 * ((P.Nx - 1) / 8) + 4 * NW;
     P.sp += ((4 - P.sp % 32) + 32) % 32;
     bt->smemA = (size_t)P.tile_floats * sizeof(float) +
-                (size_t)(KA_THREADS / 32) * P.Wz * sizeof(float) +
-                (size_t)P.Wx * (4 * sizeof(float) + 2 * sizeof(int)) + P.Kz * sizeof(float) + 16;
+                (size_t)(KA_THREADS / 32) * (P.Wz + 2 * (P.Kz - 1)) * sizeof(float) +
+                (size_t)P.Wx * (4 * sizeof(float) + 2 * sizeof(int)) + 2 * P.Nz * sizeof(int);
     // bands of output rows: two PSF blocks per SM when they fit
     const size_t lim = 227 * 1024, two = 113 * 1024;
     auto smem_b = [&](int band) {
@@ -789,7 +429,8 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
         cudaMalloc(&bt->mplanes, nrows * P.pitch * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&bt->xr, nrows * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&bt->sat, (size_t)P.Nz * (P.Ny + 1) * (P.Nx + 1) * sizeof(double)) !=
-            cudaSuccess)
+            cudaSuccess ||
+        cudaMalloc(&bt->iw, (size_t)P.Nz * P.Ny * P.Nx * sizeof(float)) != cudaSuccess)
         return GBKB200_ERR_OOM;
     GBK_CUDA_TRY(cudaMemcpy(bt->vr, vr.data(), vr.size() * sizeof(float), cudaMemcpyHostToDevice));
     GBK_CUDA_TRY(cudaMemcpy(bt->ur, ur.data(), ur.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -800,10 +441,13 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.mplanes = bt->mplanes;
     P.xr = bt->xr;
     P.sat = bt->sat;
+    P.iw = bt->iw;
     k_sat<<<P.Nz, 128, 0, bt->ctx->stream>>>(P, bt->sat);
+    k_iw<<<592, 256, 0, bt->ctx->stream>>>(P, bt->iw, (long long)P.Nz * P.Ny * P.Nx);
     GBK_CUDA_TRY(cudaGetLastError());
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
-    GBK_CUDA_TRY(cudaFuncSetAttribute(ka_lines_lsf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    bt->ka = ka_fn(P.Kz);
+    GBK_CUDA_TRY(cudaFuncSetAttribute(bt->ka, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)bt->smemA));
     bt->kb = kb_fn(P.K);
     GBK_CUDA_TRY(cudaFuncSetAttribute(bt->kb, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -870,6 +514,7 @@ extern "C" int gbkb200_batch_destroy(gbkb200_batch* bt)
     cudaFree(bt->mplanes);
     cudaFree(bt->xr);
     cudaFree(bt->sat);
+    cudaFree(bt->iw);
     for (cudaEvent_t e : bt->ev) cudaEventDestroy(e);
     delete bt;
     return GBKB200_OK;
@@ -1081,7 +726,7 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
             const int cn = std::min(bt->chunk, nsets - s0);
             P.set0 = s0;
             stage_mark(bt, 0, true);
-            ka_lines_lsf<<<dim3(P.Wy, cn), KA_THREADS, bt->smemA, st>>>(P, bt->ctx->d_status);
+            bt->ka<<<dim3(P.Wy, cn), KA_THREADS, bt->smemA, st>>>(P, bt->ctx->d_status);
             stage_mark(bt, 0, false);
             stage_mark(bt, 4, true);
             bt->kb<<<dim3(P.Nz * P.nbands, cn), KB_THREADS, bt->smemB, st>>>(P);
