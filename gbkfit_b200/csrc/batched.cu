@@ -329,7 +329,7 @@ struct gbkb200_batch {
     double* partials = nullptr;
     int nper = 0;
     int direct = 0;
-    size_t smemA = 0, smemB = 0;
+    size_t smemB = 0;
     float *vr = nullptr, *ur = nullptr, *lsfr = nullptr, *mplanes = nullptr;
     int* xr = nullptr;
     double* sat = nullptr;
@@ -395,21 +395,17 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.Kz = d->kernel_size[2];
     if (d->psf_rank != 1 || !d->psf_u || !d->psf_v) return GBKB200_ERR_UNSUPPORTED;
     P.K = std::max(KB_KMIN, std::max(P.Kx, P.Ky) | 1);
-    if (P.K > KB_KMAX || P.Kz > KA_KMAX || P.Nx > 8 * KB_THREADS || P.Wx > 32767)
+    if (P.K > KB_KMAX || P.Kz > KA_KMAX || P.Nx > 8 * KB_THREADS || P.Wx > 1024)
         return GBKB200_ERR_UNSUPPORTED;
     const int NW = (P.K + 7 + 3) / 4;
-    P.pitch = (P.Wx + 3) / 4 * 4;
-    P.tpitch = P.pitch + 1;
-    P.tile_floats = (P.Nz * P.tpitch + 3) / 4 * 4;
+    P.pitch = (P.Wx + 31) / 32 * 32;
     P.sp = 8 * ((P.Nx - 1) / 8) + 4 * NW;
     P.sp += ((4 - P.sp % 32) + 32) % 32;
-    bt->smemA = (size_t)P.tile_floats * sizeof(float) +
-                (size_t)(KA_THREADS / 32) * (P.Wz + 2 * (P.Kz - 1)) * sizeof(float) +
-                (size_t)P.Wx * (4 * sizeof(float) + 2 * sizeof(int)) + 2 * P.Nz * sizeof(int);
+    P.nch = (P.Wx + 31) / 32;
     // bands of output rows: two PSF blocks per SM when they fit
     const size_t lim = 227 * 1024, two = 113 * 1024;
     auto smem_b = [&](int band) {
-        return (size_t)(band + P.K - 1) * (P.sp + 1) * sizeof(float);
+        return (size_t)(band + P.K + 7) * (P.sp + P.nch) * sizeof(float);
     };
     int band = P.Ny;
     while (band > 8 && smem_b(band) > two) band = (band + 1) / 2;
@@ -417,7 +413,6 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.nbands = (P.Ny + band - 1) / band;
     P.band = (P.Ny + P.nbands - 1) / P.nbands;
     bt->smemB = smem_b(P.band);
-    if (bt->smemA > lim) return GBKB200_ERR_UNSUPPORTED;
     std::vector<float> vr(P.K, 0.f), ur(P.K, 0.f), lr(P.Kz);
     for (int s = 0; s < P.Kx; ++s) vr[s] = (float)d->psf_v[P.Kx - 1 - s];
     for (int t = 0; t < P.Ky; ++t) ur[t] = (float)d->psf_u[P.Ky - 1 - t];
@@ -427,7 +422,7 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
         cudaMalloc(&bt->ur, ur.size() * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&bt->lsfr, lr.size() * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&bt->mplanes, nrows * P.pitch * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&bt->xr, nrows * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&bt->xr, nrows * P.nch * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&bt->sat, (size_t)P.Nz * (P.Ny + 1) * (P.Nx + 1) * sizeof(double)) !=
             cudaSuccess ||
         cudaMalloc(&bt->iw, (size_t)P.Nz * P.Ny * P.Nx * sizeof(float)) != cudaSuccess)
@@ -447,8 +442,6 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     GBK_CUDA_TRY(cudaGetLastError());
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
     bt->ka = ka_fn(P.Kz);
-    GBK_CUDA_TRY(cudaFuncSetAttribute(bt->ka, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)bt->smemA));
     bt->kb = kb_fn(P.K);
     GBK_CUDA_TRY(cudaFuncSetAttribute(bt->kb, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)bt->smemB));
@@ -726,7 +719,8 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
             const int cn = std::min(bt->chunk, nsets - s0);
             P.set0 = s0;
             stage_mark(bt, 0, true);
-            bt->ka<<<dim3(P.Wy, cn), KA_THREADS, bt->smemA, st>>>(P, bt->ctx->d_status);
+            bt->ka<<<dim3((P.Wy * P.nch + KA_THREADS / 32 - 1) / (KA_THREADS / 32), cn), KA_THREADS,
+                     0, st>>>(P, bt->ctx->d_status);
             stage_mark(bt, 0, false);
             stage_mark(bt, 4, true);
             bt->kb<<<dim3(P.Nz * P.nbands, cn), KB_THREADS, bt->smemB, st>>>(P);

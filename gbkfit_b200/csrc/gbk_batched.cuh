@@ -33,16 +33,16 @@ struct BatchKernelArgs {
     // direct (separable) convolution
     int Kx, Ky, Kz;       // PSF (x, y) and LSF box sizes
     int K;                // FIR length of the PSF kernel (odd, >= Kx, Ky; zero-padded taps)
-    int pitch;            // row pitch of the LSF-convolved planes in HBM (floats, % 4 == 0)
-    int tpitch;           // row pitch of the model kernel's shared tile (odd: no bank conflicts)
-    int tile_floats;      // Nz * tpitch rounded up to 4
+    int pitch;            // row pitch of the LSF-convolved planes in HBM (floats, % 32 == 0)
     int sp;               // row pitch of the PSF kernel's shared rows (floats, % 32 == 4)
     int band, nbands;     // output rows per PSF block, bands per plane
     const float* vr;      // (K): PSF x factor, reversed
     const float* ur;      // (K): PSF y factor, reversed
     const float* lsfr;    // (Kz): LSF reversed
-    float* mplanes;       // (chunk, Nz, Wy, pitch): only the xr segments are written
-    int* xr;              // (chunk, Nz, Wy): nonzero x range of each plane row, or -1
+    float* mplanes;       // (chunk, Nz, Wy, pitch): written where xr is not empty
+    int nch;              // 32-column chunks per window row, ceil(Wx / 32)
+    int* xr;              // (chunk, Wy, nch, Nz): nonzero x range (xmin | xmax << 16) of
+                          // each plane row chunk (4-aligned around it is written), or -1
     const double* sat;    // (Nz, Ny + 1, Nx + 1): summed-area table of the zero-model r^2
 };
 
@@ -62,6 +62,8 @@ __device__ __forceinline__ DiskArgs set_disk(const BatchKernelArgs& P, int b)
     return a;
 }
 
+constexpr int KA_THREADS = 128;        // 4 independent (row, chunk) warps per block
+
 // ---- direct convolution: LSF FIR per column, separable PSF FIR per plane ----
 //
 // Crop output (zo, yo, xo) of the reference's FFT convolution equals
@@ -78,105 +80,87 @@ __device__ __forceinline__ DiskArgs set_disk(const BatchKernelArgs& P, int b)
 // residual outside the box, where the model is exactly 0, from a summed-area
 // table of ((0 - data) / error * mask * weight)^2 built once per data cube.
 
-// KA: one block per (set, window row y): the row's spaxel lines, each spectral
-// column convolved with the LSF (a warp per spaxel, KZ taps unrolled with the
-// coefficients in registers), then per output plane the nonzero x segment of
-// the row (aligned to 4) and its range.
-constexpr int KA_THREADS = 256;
-
+// KA: a warp per (set, window row y, 32-spaxel chunk of the row), no block
+// synchronisation.  A lane evaluates its spaxel and then streams its
+// LSF-convolved spectral column over the warp's output channel range: a
+// sliding window of KZ line values in registers (compile-time rotation, KZ
+// taps per output), each output plane row chunk stored as one coalesced
+// 128-byte segment.  Per plane the chunk's nonzero x range is stored.
 template<int KZ>
-__global__ void __launch_bounds__(KA_THREADS, 3) ka_lines_lsf(BatchKernelArgs P, int* status)
+__global__ void __launch_bounds__(KA_THREADS, 4) ka_lines_lsf(BatchKernelArgs P, int* status)
 {
-    extern __shared__ float4 sm4[];
-    const int tp = P.tpitch, lb = P.Wz + 2 * (KZ - 1);
-    float* tile = reinterpret_cast<float*>(sm4);          // (Nz, tp)
-    float* lbuf = tile + P.tile_floats;                    // (nwarps, lb)
-    float* s_v = lbuf + (KA_THREADS / 32) * lb;
-    float* s_amp = s_v + P.Wx;
-    float* s_i2 = s_amp + P.Wx;
-    float* s_orv = s_i2 + P.Wx;
-    int* s_lo = reinterpret_cast<int*>(s_orv + P.Wx);
-    int* s_hi = s_lo + P.Wx;
-    int* s_xmin = s_hi + P.Wx;                             // (Nz)
-    int* s_xmax = s_xmin + P.Nz;
-    const int y = blockIdx.x, c = blockIdx.y, b = P.set0 + c;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int item = blockIdx.x * (KA_THREADS / 32) + warp;
+    if (item >= P.Wy * P.nch) return;                    // whole warp
+    const int y = item / P.nch, chunk = item % P.nch;
+    const int c = blockIdx.y, b = P.set0 + c;
     const DiskArgs a = set_disk(P, b);
-    int bad = 0;
     const DiskConst kc = disk_const(a);
-    for (int x = threadIdx.x; x < P.Wx; x += blockDim.x) {
-        SpaxelOut o;
-        int lo = INT_MAX, hi = -1;
-        float amp = 0, i2 = 1;
-        if (smdisk_spaxel(a, kc, x, y, 0, o, bad) &&
-            line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo, hi)) {
-            amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
-            i2 = 2 * o.dv * o.dv;
-        } else {
-            lo = INT_MAX;
-            hi = -1;
-        }
-        s_v[x] = o.vv;
-        s_amp[x] = amp;
-        s_i2[x] = i2;
-        s_orv[x] = o.orv;
-        s_lo[x] = lo;
-        s_hi[x] = hi;
+    int bad = 0;
+    const int x = chunk * 32 + lane;
+    SpaxelOut o{};
+    int lo = INT_MAX, hi = -1;
+    float amp = 0.f, rinv = 0.f;
+    if (x < P.Wx && smdisk_spaxel(a, kc, x, y, 0, o, bad) &&
+        line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo, hi)) {
+        amp = o.orv * (1 / (o.dv * sqrtf(2 * GBK_PI)));
+        rinv = 1 / (2 * o.dv * o.dv);
+    } else {
+        lo = INT_MAX;
+        hi = -1;
     }
-    float4* t4 = reinterpret_cast<float4*>(tile);
-    for (int i = threadIdx.x; i < P.tile_floats / 4; i += blockDim.x)
-        t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = threadIdx.x; i < P.Nz; i += blockDim.x) {
-        s_xmin[i] = INT_MAX;
-        s_xmax[i] = -1;
-    }
-    float lz[KZ];
+    const float v = o.vv, z0 = a.spec_zero, dz = a.spec_step;
+    // gmodels.hpp:109-115: the line at window channel z (0 outside [lo, hi])
+    auto line = [&](int z) {
+        const float d = (z0 + z * dz) - v;
+        return (z >= lo && z <= hi) ? amp * expf(-(d * d) * rinv) : 0.f;
+    };
+    // the lane's and the warp's output channel ranges
+    const bool on = lo <= hi;
+    const int olo = on ? max(0, lo - KZ + 1) : INT_MAX, ohi = on ? min(P.Nz - 1, hi) : -1;
+    int zlo = olo, zhi = ohi;
 #pragma unroll
-    for (int t = 0; t < KZ; ++t) lz[t] = P.lsfr[t];
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    // L[j], j = z - lo + KZ - 1: the line with KZ - 1 zeros on both sides
-    float* L = lbuf + warp * lb;
-    for (int x = warp; x < P.Wx; x += nwarps) {
-        const int lo = s_lo[x], hi = s_hi[x];
-        if (lo > hi) continue;
-        const float v = s_v[x], amp = s_amp[x], i2 = s_i2[x], orv = s_orv[x];
-        const int n = hi - lo + 1;
-        for (int j = lane; j < KZ - 1; j += 32) {
-            L[j] = 0.f;
-            L[n + KZ - 1 + j] = 0.f;
-        }
-        // gmodels.hpp:109-115: the line, channel by channel (window coordinates)
-        for (int z = lo + lane; z <= hi; z += 32) {
-            float zv = a.spec_zero + z * a.spec_step;
-            float d = zv - v;
-            L[z - lo + KZ - 1] = orv * (amp * expf(-d * d / i2));
-        }
-        __syncwarp();
-        const int zo0 = max(0, lo - KZ + 1), zo1 = min(P.Nz - 1, hi);
-        for (int zo = zo0 + lane; zo <= zo1; zo += 32) {
-            const float* l = L + (zo - lo + KZ - 1);
-            float acc = 0.f;
-#pragma unroll
-            for (int t = 0; t < KZ; ++t) acc += lz[t] * l[t];
-            tile[zo * tp + x] = acc;
-            atomicMin(&s_xmin[zo], x);
-            atomicMax(&s_xmax[zo], x);
-        }
-        __syncwarp();
+    for (int s = 16; s > 0; s >>= 1) {
+        zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, s));
+        zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, s));
     }
-    __syncthreads();
-    // per output plane: the row's nonzero x range and its 4-aligned segment
-    for (int zo = warp; zo < P.Nz; zo += nwarps) {
-        const int xmin = s_xmin[zo], xmax = s_xmax[zo];
-        const long long row = ((long long)c * P.Nz + zo) * P.Wy + y;
-        if (xmax < 0) {
-            if (lane == 0) P.xr[row] = -1;
-            continue;
+    int* xr = P.xr + (((long long)c * P.Wy + y) * P.nch + chunk) * P.Nz;
+    // planes outside [zlo, zhi] are empty for this chunk
+    for (int zo = lane; zo < P.Nz; zo += 32)
+        if (zo < zlo || zo > zhi) xr[zo] = -1;
+    if (zlo <= zhi) {
+        float lz[KZ];
+#pragma unroll
+        for (int t = 0; t < KZ; ++t) lz[t] = P.lsfr[t];
+        float w[KZ];
+#pragma unroll
+        for (int t = 0; t < KZ - 1; ++t) w[t] = line(zlo + t);
+        float* dst = P.mplanes + ((long long)c * P.Nz * P.Wy + y) * P.pitch + x;
+        const long long zstride = (long long)P.Wy * P.pitch;
+        int mlo = 0, mhi = -1, mz = zlo;     // range of the 32 planes zo in [mz, mz + 32)
+        for (int zb = zlo; zb <= zhi; zb += KZ) {
+#pragma unroll
+            for (int k = 0; k < KZ; ++k) {
+                const int zo = zb + k;
+                if (zo > zhi) break;
+                w[(k + KZ - 1) % KZ] = line(zo + KZ - 1);
+                float acc = 0.f;
+#pragma unroll
+                for (int t = 0; t < KZ; ++t) acc += lz[t] * w[(k + t) % KZ];
+                dst[zo * zstride] = acc;
+                const unsigned m = __ballot_sync(0xffffffffu, zo >= olo && zo <= ohi);
+                // lane (zo - mz) keeps plane zo's range; flushed every 32 planes
+                if (lane == zo - mz) {
+                    mlo = m ? chunk * 32 + __ffs(m) - 1 : 0;
+                    mhi = m ? chunk * 32 + 31 - __clz(m) : -1;
+                }
+                if (zo - mz == 31 || zo == zhi) {
+                    const int zz = mz + lane;
+                    if (zz <= zo) xr[zz] = mhi >= 0 ? (mlo | (mhi << 16)) : -1;
+                    mz = zo + 1;
+                }
+            }
         }
-        if (lane == 0) P.xr[row] = xmin | (xmax << 16);
-        float* dst = P.mplanes + row * P.pitch;
-        const float* srow = tile + zo * tp;
-        for (int x = (xmin & ~3) + lane; x <= (xmax | 3); x += 32) dst[x] = srow[x];
     }
     if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
 }
@@ -215,7 +199,7 @@ __global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs
 {
     constexpr int NW = (K + 7 + 3) / 4;     // float4 slots of one 8-output x window
     extern __shared__ float4 sm4[];
-    float* S = reinterpret_cast<float*>(sm4);                   // (band + K - 1, sp)
+    float* S = reinterpret_cast<float*>(sm4);                   // (band + K + 7, sp), then s_xr
     __shared__ float warp_part[KB_THREADS / 32];
     const int zo = blockIdx.x / P.nbands, band = blockIdx.x % P.nbands;
     const int c = blockIdx.y, b = P.set0 + c;
@@ -223,27 +207,47 @@ __global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs
     const int ob0 = band * P.band, ob1 = min(P.Ny, ob0 + P.band);  // output rows [ob0, ob1)
     const int in1 = min(P.Wy, ob1 + K - 1);                        // input rows [ob0, in1)
     const long long prow = ((long long)c * P.Nz + zo) * P.Wy;
-    const int* xr = P.xr + prow;
+    const int* xr = P.xr + (long long)c * P.Wy * P.nch * P.Nz + zo;   // (y, chunk) at [(y nch + chunk) Nz]
     const int ld = P.Nx + 1;
     const double* T = P.sat + (long long)zo * (P.Ny + 1) * ld;
-    // bounding box of the nonzero input rows (every warp, no barrier)
-    int y0 = INT_MAX, y1 = -1, x0 = INT_MAX, x1 = -1;
-    for (int y = ob0 + lane; y < in1; y += 32) {
-        const int v = xr[y];
-        if (v >= 0) {
-            y0 = min(y0, y);
-            y1 = max(y1, y);
-            x0 = min(x0, v & 0xffff);
-            x1 = max(x1, v >> 16);
+    const int rows_s = P.band + K + 7;
+    int* s_xr = reinterpret_cast<int*>(S + (long long)rows_s * P.sp);   // (in1 - ob0, nch)
+    __shared__ int s_box[4];
+    if (threadIdx.x == 0) {
+        s_box[0] = INT_MAX; s_box[1] = -1; s_box[2] = INT_MAX; s_box[3] = -1;
+    }
+    __syncthreads();
+    // bounding box of the nonzero input row chunks
+    {
+        int y0 = INT_MAX, y1 = -1, x0 = INT_MAX, x1 = -1;
+        const int n = (in1 - ob0) * P.nch;
+        for (int i = threadIdx.x; i < n; i += KB_THREADS) {
+            const int v = xr[(long long)(ob0 * P.nch + i) * P.Nz];
+            s_xr[i] = v;
+            if (v >= 0) {
+                const int y = ob0 + i / P.nch;
+                y0 = min(y0, y);
+                y1 = max(y1, y);
+                x0 = min(x0, v & 0xffff);
+                x1 = max(x1, v >> 16);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+            y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+            x0 = min(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+            x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+        }
+        if (lane == 0 && y1 >= 0) {
+            atomicMin(&s_box[0], y0);
+            atomicMax(&s_box[1], y1);
+            atomicMin(&s_box[2], x0);
+            atomicMax(&s_box[3], x1);
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
-        y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
-        x0 = min(x0, __shfl_xor_sync(0xffffffffu, x0, o));
-        x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, o));
-    }
+    __syncthreads();
+    const int y0 = s_box[0], y1 = s_box[1], x0 = s_box[2], x1 = s_box[3];
     const long long plane = (long long)P.Ny * P.Nx;
     float* model = P.model ? P.model + ((long long)b * P.Nz + zo) * plane : nullptr;
     const long long part = ((long long)b * P.Nz + zo) * P.nbands + band;
@@ -259,20 +263,40 @@ __global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs
     const int g_lo = max(0, x0 - K + 1) >> 3, g_hi = min(P.Nx - 1, x1) >> 3;
     const int ns8 = g_hi - g_lo + 1;
     const int yo_lo = max(ob0, y0 - K + 1), yo_hi = min(ob1 - 1, y1);
-    // load rows [y0, y1], float4 slots [2 g_lo, 2 g_hi + NW): the row's
-    // segment from HBM, zeros elsewhere
+    const int ngy = (yo_hi - yo_lo + 8) / 8, s4_lo = 2 * g_lo, ns4 = 2 * ns8;
+    // rows [y0, y1], float4 slots [2 g_lo, 2 g_hi + NW): each row chunk's
+    // nonzero range from HBM, zeros elsewhere; the other rows that
+    // the y FIR reads, [yo_lo, y0) and (y1, yo_lo + 8 ngy + K - 2], are zeroed
     {
         const int nsl = 2 * (ns8 - 1) + NW, sl0 = 2 * g_lo;
-        const int nrows = y1 - y0 + 1;
+        const int tc = min(nsl, (int)blockDim.x), tr = blockDim.x / tc;
+        const int ti = threadIdx.x % tc, ty = threadIdx.x / tc;
         const float4* src = reinterpret_cast<const float4*>(P.mplanes + prow * P.pitch);
-        for (int i = threadIdx.x; i < nrows * nsl; i += blockDim.x) {
-            const int y = y0 + i / nsl, sl = sl0 + i % nsl;
-            const int v = xr[y];
-            float4* d = reinterpret_cast<float4*>(S + (long long)(y - ob0) * P.sp) + sl;
-            if (v >= 0 && sl >= (v & 0xffff) >> 2 && sl <= (v >> 16) >> 2)
-                cp_async16(d, src + (long long)y * (P.pitch / 4) + sl);
-            else
-                *d = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ty < tr) {
+            for (int y = y0 + ty; y <= y1; y += tr) {
+                const int* vr_ = s_xr + (y - ob0) * P.nch;
+                float4* d = reinterpret_cast<float4*>(S + (long long)(y - ob0) * P.sp);
+                const float4* g = src + (long long)y * (P.pitch / 4);
+                for (int sl = sl0 + ti; sl < sl0 + nsl; sl += tc) {
+                    const int ch = sl >> 3;
+                    const int v = ch < P.nch ? vr_[ch] : -1;
+                    if (v >= 0 && sl >= (v & 0xffff) >> 2 && sl <= (v >> 16) >> 2)
+                        cp_async16(d + sl, g + sl);
+                    else
+                        d[sl] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
+        }
+        const int zt = min(ns4, (int)blockDim.x), zr = blockDim.x / zt;
+        const int zi = threadIdx.x % zt, zy = threadIdx.x / zt;
+        const int yr_end = yo_lo + 8 * ngy + K - 1;      // rows [yo_lo, yr_end) are read
+        if (zy < zr) {
+            for (int y = yo_lo + zy; y < yr_end; y += zr) {
+                if (y >= y0 && y <= y1) continue;
+                float4* d = reinterpret_cast<float4*>(S + (long long)(y - ob0) * P.sp);
+                for (int s4 = s4_lo + zi; s4 < s4_lo + ns4; s4 += zt)
+                    d[s4] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
         }
         cp_async_wait_all();
     }
@@ -319,9 +343,8 @@ __global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs
     }
     __syncthreads();
     // y FIR in place: model(yo, xo) = sum_t ur[t] S[yo + t][xo] (rows outside
-    // [y0, y1] are zero), written to S row yo; items of 8 rows x 4 columns in
+    // [y0, y1] were zeroed), written to S row yo; items of 8 rows x 4 columns in
     // ascending rounds of whole 8-row groups
-    const int ngy = (yo_hi - yo_lo + 8) / 8, s4_lo = 2 * g_lo, ns4 = 2 * ns8;
     {
         float ur[K];
 #pragma unroll
@@ -341,10 +364,8 @@ __global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs
                     const int yb = yo_lo + 8 * (gr0 + item / ns4), s4 = s4_lo + item % ns4;
 #pragma unroll
                     for (int m = 0; m < K + 7; ++m) {
-                        const int y = yb + m;
-                        const float4 p = (y >= y0 && y <= y1)
-                            ? reinterpret_cast<const float4*>(S + (long long)(y - ob0) * P.sp)[s4]
-                            : make_float4(0.f, 0.f, 0.f, 0.f);
+                        const float4 p =
+                            reinterpret_cast<const float4*>(S + (long long)(yb + m - ob0) * P.sp)[s4];
 #pragma unroll
                         for (int q = 0; q < 8; ++q) {
                             const int t = m - q;
@@ -380,11 +401,14 @@ __global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs
     float sum = 0.f;
     const long long pbase = (long long)zo * plane;
     if ((P.Nx & 3) == 0) {
+        // flat float4 index over the box, stepped without divisions
         const int nv = (xb_end - xb0) >> 2;        // xb0 and xb_end are multiples of 4
         const int n = (yb_end - yo_lo) * nv;
+        const int dq = KB_THREADS / nv, dr = KB_THREADS % nv;
+        int row = threadIdx.x / nv, col = threadIdx.x % nv;
 #pragma unroll 4
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int yo = yo_lo + i / nv, xo = xb0 + 4 * (i % nv);
+        for (int i = threadIdx.x; i < n; i += KB_THREADS) {
+            const int yo = yo_lo + row, xo = xb0 + 4 * col;
             const float4 m = *reinterpret_cast<const float4*>(S + (long long)(yo - ob0) * P.sp + xo);
             const long long vi = pbase + (long long)yo * P.Nx + xo;
             const float4 o = *reinterpret_cast<const float4*>(P.obs + vi);
@@ -393,16 +417,28 @@ __global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs
             const float r2 = (m.z - o.z) * w.z, r3 = (m.w - o.w) * w.w;
             sum += r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3;
             if (model) *reinterpret_cast<float4*>(model + (long long)yo * P.Nx + xo) = m;
+            row += dq;
+            col += dr;
+            if (col >= nv) {
+                col -= nv;
+                ++row;
+            }
         }
     } else {
-        const int nw = xb_end - xb0, n = (yb_end - yo_lo) * nw;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int yo = yo_lo + i / nw, xo = xb0 + i % nw;
-            const float m = S[(long long)(yo - ob0) * P.sp + xo];
-            const long long vi = pbase + (long long)yo * P.Nx + xo;
-            const float r0 = (m - P.obs[vi]) * P.iw[vi];
-            sum += r0 * r0;
-            if (model) model[(long long)yo * P.Nx + xo] = m;
+        const int nw = xb_end - xb0;
+        const int tc = min(nw, (int)blockDim.x), tr = blockDim.x / tc;
+        const int ti = threadIdx.x % tc, ty = threadIdx.x / tc;
+        if (ty < tr) {
+            for (int yo = yo_lo + ty; yo < yb_end; yo += tr) {
+                for (int j = ti; j < nw; j += tc) {
+                    const int xo = xb0 + j;
+                    const float m = S[(long long)(yo - ob0) * P.sp + xo];
+                    const long long vi = pbase + (long long)yo * P.Nx + xo;
+                    const float r0 = (m - P.obs[vi]) * P.iw[vi];
+                    sum += r0 * r0;
+                    if (model) model[(long long)yo * P.Nx + xo] = m;
+                }
+            }
         }
     }
     if (model) {
