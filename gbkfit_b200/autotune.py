@@ -6,6 +6,8 @@ Knobs (all change speed only, never results beyond fp32 rounding):
   (x even);
 * ``chunk``: parameter sets per pipeline wave (the wave's intermediates
   should stay in L2);
+* ``band``: output rows per PSF block of the direct mode (smaller bands: more
+  resident blocks, more halo rows);
 * ``rows_k1``: spectral rows per shared-memory group of the model kernel.
 
 Coordinate descent from the defaults; every trial builds an evaluator and
@@ -87,25 +89,34 @@ def time_config(w, data, err, nsets, cfg, reps=3):
 
 
 def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
-    """Best {fft_size, chunk, rows_k1} for workload w with nsets sets."""
+    """Best {fft_size, chunk, rows_k1, conv, band} for workload w with nsets sets."""
     key = _key(w, nsets)
     if use_cache:
         c = _load().get(key)
         if c:
             return dict(fft_size=tuple(c['fft_size']), chunk=c['chunk'], rows_k1=c['rows_k1'],
-                        conv=c['conv'])
+                        conv=c['conv'], band=c.get('band', 0))
     g = w.geom
     t_end = time.time() + budget_s
-    # direct separable convolution (when the PSF is low rank): chunk only
+    # direct separable convolution (when the PSF is rank 1): chunk, then band
     best_d, best_dt = None, float('inf')
-    for chunk in (4, 8, 16, 32, 64):
-        cfg = dict(fft_size=(0, 0, 0), chunk=chunk, rows_k1=16, conv='direct')
+    for chunk in (16, 32, 64, 128, 256):
+        cfg = dict(fft_size=(0, 0, 0), chunk=chunk, rows_k1=16, conv='direct', band=0)
         t = time_config(w, data, err, nsets, cfg)
         if t < best_dt:
             best_d, best_dt = cfg, t
+    if best_d is not None:
+        for band in (96, 64, 48, 32):
+            if band >= g.size[1]:
+                continue
+            cfg = dict(best_d, band=band)
+            t = time_config(w, data, err, nsets, cfg)
+            if t < best_dt:
+                best_d, best_dt = cfg, t
     win = [g.size[i] + g.kernel_size[i] - 1 for i in range(3)]
     cand = [smooth_sizes(win[0], even=True), smooth_sizes(win[1]), smooth_sizes(win[2])]
-    best = dict(fft_size=(cand[0][0], cand[1][0], cand[2][0]), chunk=8, rows_k1=16, conv='fft')
+    best = dict(fft_size=(cand[0][0], cand[1][0], cand[2][0]), chunk=8, rows_k1=16, conv='fft',
+                band=0)
     best_t = time_config(w, data, err, nsets, best)
     trials = []
     for knob, values in (('chunk', (2, 4, 8, 16, 32)), ('rows_k1', (8, 16, 32)),

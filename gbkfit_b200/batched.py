@@ -38,6 +38,7 @@ class BatchDesc(ctypes.Structure):
         ('max_sets', c_int), ('chunk', c_int), ('rows_k1', c_int), ('rows_k5', c_int),
         ('conv_mode', c_int), ('psf_rank', c_int),
         ('psf_u', ctypes.POINTER(ctypes.c_double)), ('psf_v', ctypes.POINTER(ctypes.c_double)),
+        ('psf_band', c_int),
     ]
 
 CONV_MODES = dict(auto=0, fft=1, direct=2)
@@ -109,7 +110,7 @@ class BatchedSMDisk:
     data/error/mask: (nz, ny, nx) arrays (host or device) or None."""
 
     def __init__(self, disk, geom, data, error=None, mask=None, weight=1.0, max_sets=512,
-                 chunk=0, fft_size=(0, 0, 0), rows_k1=0, rows_k5=0, conv='auto', device=0,
+                 chunk=0, fft_size=(0, 0, 0), rows_k1=0, rows_k5=0, conv='auto', band=0, device=0,
                  stream=None):
         if disk.traits['rht']:
             raise ValueError("the batched evaluator takes thin disks only")
@@ -163,6 +164,7 @@ class BatchedSMDisk:
         d.weight = float(weight)
         d.max_sets, d.chunk, d.rows_k1, d.rows_k5 = self.max_sets, chunk, rows_k1, rows_k5
         d.conv_mode = CONV_MODES[conv]
+        d.psf_band = int(band)
         rank, fu, fv = separable_factors(psf) if conv != 'fft' else (0, None, None)
         self._fu, self._fv = fu, fv
         d.psf_rank = rank
@@ -229,12 +231,59 @@ class BatchedSMDisk:
         return chi2[:nsets]
 
     def evaluate(self, params, nsets):
-        """Host parameters -> host chi^2 (numpy), end to end."""
-        if self._inputs is None:
-            self._inputs = self.alloc_inputs()
-        self.upload(self.pack(params, nsets), self._inputs, nsets)
-        out = self.evaluate_device(self._inputs, nsets)
-        return out.cpu().numpy()
+        """Host parameters -> host chi^2 (numpy), end to end.
+
+        The batch is split into pieces (whole chunks); each piece is packed
+        into its own pinned host buffer, copied to the device in one
+        transfer and evaluated asynchronously while the next piece is
+        packed; chi^2 comes back through a pinned buffer and the call
+        synchronises once."""
+        nsets = int(nsets)
+        if nsets > self.max_sets:
+            raise ValueError(f"nsets {nsets} > max_sets {self.max_sets}")
+        piece = max(self.chunk, -(-nsets // 4))
+        piece = -(-piece // self.chunk) * self.chunk
+        st = self._e2e_buffers(piece, -(-nsets // piece))
+        per_set = {k: (np.ndim(v) > 0 and np.shape(v)[0] == nsets) for k, v in params.items()}
+        self.last_h2d_bytes = 0
+        with torch.cuda.stream(self.stream):
+            for j, lo in enumerate(range(0, nsets, piece)):
+                hi = min(nsets, lo + piece)
+                sub = {k: (v[lo:hi] if per_set[k] else v) for k, v in params.items()}
+                hv, hflat, dflat, dv = st['pieces'][j]
+                for name, arr in self.pack(sub, hi - lo).items():
+                    hv[name][:hi - lo] = arr
+                dflat.copy_(hflat, non_blocking=True)
+                self.last_h2d_bytes += hflat.numel() * 4
+                self.evaluate_device(dv, hi - lo, chi2=self.chi2[lo:hi])
+            out = st['chi2'][:nsets]
+            out.copy_(self.chi2[:nsets], non_blocking=True)
+        self.stream.synchronize()
+        return out.numpy().copy()
+
+    def _e2e_buffers(self, piece, npieces):
+        """Pinned host and device input buffers of npieces pieces of piece sets."""
+        st = getattr(self, '_e2e', None)
+        if st is not None and st['piece'] == piece and len(st['pieces']) >= npieces:
+            return st
+        names = [n for n in ('vsys', 'xpos', 'ypos', 'posa', 'incl') if n in self.disk.pdescs]
+        widths = [(n, self.disk.common_size(n)) for n in names]
+        widths += [(kind, self.npv[k]) for k, kind in enumerate(KINDS) if self.npv[k]]
+        total = piece * sum(w for _, w in widths)
+        pieces = []
+        for _ in range(npieces):
+            hflat = torch.empty(total, dtype=torch.float32, pin_memory=True)
+            dflat = torch.empty(total, dtype=torch.float32, device=self.dev)
+            hv, dv, off = {}, {}, 0
+            for name, w in widths:
+                hv[name] = hflat[off:off + piece * w].view(piece, w).numpy()
+                dv[name] = dflat[off:off + piece * w].view(piece, w)
+                off += piece * w
+            pieces.append((hv, hflat, dflat, dv))
+        st = dict(piece=piece, pieces=pieces,
+                  chi2=torch.empty(self.max_sets, dtype=torch.float32, pin_memory=True))
+        self._e2e = st
+        return st
 
     def capture(self, bufs, nsets):
         """Capture one evaluate_device call for nsets sets in a CUDA graph."""

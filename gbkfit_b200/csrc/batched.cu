@@ -407,8 +407,8 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     auto smem_b = [&](int band) {
         return (size_t)(band + P.K + 7) * (P.sp + P.nch) * sizeof(float);
     };
-    int band = P.Ny;
-    while (band > 8 && smem_b(band) > two) band = (band + 1) / 2;
+    int band = d->psf_band > 0 ? std::min(d->psf_band, P.Ny) : P.Ny;
+    while (d->psf_band <= 0 && band > 8 && smem_b(band) > two) band = (band + 1) / 2;
     if (smem_b(band) > lim) return GBKB200_ERR_UNSUPPORTED;
     P.nbands = (P.Ny + band - 1) / band;
     P.band = (P.Ny + P.nbands - 1) / P.nbands;

@@ -238,6 +238,7 @@ typedef struct {
     int psf_rank;           /* direct mode: PSF = sum_r u_r(y) v_r(x), rank <= 8 */
     const double* psf_u;    /* host: (psf_rank, kernel_size[1]) */
     const double* psf_v;    /* host: (psf_rank, kernel_size[0]) */
+    int psf_band;           /* direct mode: output rows per PSF block (0 = automatic) */
 } gbkb200_batch_desc;
 
 int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);
