@@ -235,7 +235,7 @@ def run_b200(args):
         b_eval = staged_bytes_per_eval(w.geom)
         achieved = b_eval * nsets / (ms_step / 1e3) / 1e9
         n_chunks = (nsets + ev.chunk - 1) // ev.chunk
-        per_chunk = 2 if ev.conv_mode == 'direct' else 5
+        per_chunk = 3 if ev.conv_mode == 'direct' else 5
         plain = plain_per_call(w, data, err) if args.plain else None
         cpu = cpu_baseline(w, data, err) if args.cpu_baseline else None
         out = dict(

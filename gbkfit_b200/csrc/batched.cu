@@ -34,6 +34,29 @@
 
 namespace gbk {
 
+// The model kernel's range table (row chunk-major, written per warp) to the
+// plane-major layout the PSF kernel reads: a 32 x 32 tiled transpose per set.
+__global__ void __launch_bounds__(256) k_xr_transpose(const int* __restrict__ src,
+                                                      int* __restrict__ dst, int R, int Nz)
+{
+    __shared__ int tile[32][33];
+    const int c = blockIdx.z, r0 = blockIdx.x * 32, z0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int* s = src + (long long)c * R * Nz;
+    int* d = dst + (long long)c * Nz * R;
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const int r = r0 + ty + k, z = z0 + tx;
+        if (r < R && z < Nz) tile[ty + k][tx] = s[(long long)r * Nz + z];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const int z = z0 + ty + k, r = r0 + tx;
+        if (r < R && z < Nz) d[(long long)z * R + r] = tile[tx][ty + k];
+    }
+}
+
 // per-voxel residual factor of the direct path: mask * weight / error
 __global__ void k_iw(BatchKernelArgs P, float* iw, long long n)
 {
@@ -332,6 +355,7 @@ struct gbkb200_batch {
     size_t smemB = 0;
     float *vr = nullptr, *ur = nullptr, *lsfr = nullptr, *mplanes = nullptr;
     int* xr = nullptr;
+    int* xrt = nullptr;
     double* sat = nullptr;
     float* iw = nullptr;
     void (*kb)(BatchKernelArgs) = nullptr;
@@ -395,24 +419,25 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.Kz = d->kernel_size[2];
     if (d->psf_rank != 1 || !d->psf_u || !d->psf_v) return GBKB200_ERR_UNSUPPORTED;
     P.K = std::max(KB_KMIN, std::max(P.Kx, P.Ky) | 1);
-    if (P.K > KB_KMAX || P.Kz > KA_KMAX || P.Nx > 8 * KB_THREADS || P.Wx > 1024)
+    if (P.K > KB_KMAX || P.Kz > KA_KMAX || P.Nx > 4 * KB_THREADS * KB_IT || P.Wx > 1024)
         return GBKB200_ERR_UNSUPPORTED;
     const int NW = (P.K + 7 + 3) / 4;
     P.pitch = (P.Wx + 31) / 32 * 32;
-    P.sp = 8 * ((P.Nx - 1) / 8) + 4 * NW;
-    P.sp += ((4 - P.sp % 32) + 32) % 32;
     P.nch = (P.Wx + 31) / 32;
-    // bands of output rows: two PSF blocks per SM when they fit
-    const size_t lim = 227 * 1024, two = 113 * 1024;
-    auto smem_b = [&](int band) {
-        return (size_t)(band + P.K + 7) * (P.sp + P.nch) * sizeof(float);
-    };
     int band = d->psf_band > 0 ? std::min(d->psf_band, P.Ny) : P.Ny;
-    while (d->psf_band <= 0 && band > 8 && smem_b(band) > two) band = (band + 1) / 2;
-    if (smem_b(band) > lim) return GBKB200_ERR_UNSUPPORTED;
     P.nbands = (P.Ny + band - 1) / band;
     P.band = (P.Ny + P.nbands - 1) / P.nbands;
-    bt->smemB = smem_b(P.band);
+    // shared memory of a PSF block: rows of one pass at the widest box pitch;
+    // at least K + 15 rows (8 output rows a pass), at most the whole band,
+    // otherwise 54 KB (four blocks per SM)
+    int bpmax = 4 * (2 * ((P.Nx + 7) / 8 - 1) + NW);
+    bpmax += ((4 - bpmax % 32) + 32) % 32;
+    const long long need_min = (long long)(P.K + 15) * bpmax;
+    const long long need_all = (long long)(P.band + P.K + 7) * bpmax;
+    const long long cap = std::max(need_min, std::min(need_all, 54LL * 1024 / 4));
+    if (cap * (long long)sizeof(float) > 227LL * 1024) return GBKB200_ERR_UNSUPPORTED;
+    P.cap = (int)cap;
+    bt->smemB = (size_t)cap * sizeof(float);
     std::vector<float> vr(P.K, 0.f), ur(P.K, 0.f), lr(P.Kz);
     for (int s = 0; s < P.Kx; ++s) vr[s] = (float)d->psf_v[P.Kx - 1 - s];
     for (int t = 0; t < P.Ky; ++t) ur[t] = (float)d->psf_u[P.Ky - 1 - t];
@@ -423,6 +448,7 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
         cudaMalloc(&bt->lsfr, lr.size() * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&bt->mplanes, nrows * P.pitch * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&bt->xr, nrows * P.nch * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&bt->xrt, nrows * P.nch * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&bt->sat, (size_t)P.Nz * (P.Ny + 1) * (P.Nx + 1) * sizeof(double)) !=
             cudaSuccess ||
         cudaMalloc(&bt->iw, (size_t)P.Nz * P.Ny * P.Nx * sizeof(float)) != cudaSuccess)
@@ -435,6 +461,7 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.lsfr = bt->lsfr;
     P.mplanes = bt->mplanes;
     P.xr = bt->xr;
+    P.xrt = bt->xrt;
     P.sat = bt->sat;
     P.iw = bt->iw;
     k_sat<<<P.Nz, 128, 0, bt->ctx->stream>>>(P, bt->sat);
@@ -506,6 +533,7 @@ extern "C" int gbkb200_batch_destroy(gbkb200_batch* bt)
     cudaFree(bt->lsfr);
     cudaFree(bt->mplanes);
     cudaFree(bt->xr);
+    cudaFree(bt->xrt);
     cudaFree(bt->sat);
     cudaFree(bt->iw);
     for (cudaEvent_t e : bt->ev) cudaEventDestroy(e);
@@ -722,6 +750,13 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
             bt->ka<<<dim3((P.Wy * P.nch + KA_THREADS / 32 - 1) / (KA_THREADS / 32), cn), KA_THREADS,
                      0, st>>>(P, bt->ctx->d_status);
             stage_mark(bt, 0, false);
+            stage_mark(bt, 1, true);
+            {
+                const int R = P.Wy * P.nch;
+                k_xr_transpose<<<dim3((R + 31) / 32, (P.Nz + 31) / 32, cn), 256, 0, st>>>(
+                    P.xr, P.xrt, R, P.Nz);
+            }
+            stage_mark(bt, 1, false);
             stage_mark(bt, 4, true);
             bt->kb<<<dim3(P.Nz * P.nbands, cn), KB_THREADS, bt->smemB, st>>>(P);
             stage_mark(bt, 4, false);

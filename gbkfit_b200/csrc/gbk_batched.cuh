@@ -34,7 +34,7 @@ struct BatchKernelArgs {
     int Kx, Ky, Kz;       // PSF (x, y) and LSF box sizes
     int K;                // FIR length of the PSF kernel (odd, >= Kx, Ky; zero-padded taps)
     int pitch;            // row pitch of the LSF-convolved planes in HBM (floats, % 32 == 0)
-    int sp;               // row pitch of the PSF kernel's shared rows (floats, % 32 == 4)
+    int cap;              // shared-memory floats of a PSF block (rows of one pass)
     int band, nbands;     // output rows per PSF block, bands per plane
     const float* vr;      // (K): PSF x factor, reversed
     const float* ur;      // (K): PSF y factor, reversed
@@ -43,6 +43,7 @@ struct BatchKernelArgs {
     int nch;              // 32-column chunks per window row, ceil(Wx / 32)
     int* xr;              // (chunk, Wy, nch, Nz): nonzero x range (xmin | xmax << 16) of
                           // each plane row chunk (4-aligned around it is written), or -1
+    int* xrt;             // (chunk, Nz, Wy, nch): the same, plane-major (read by the PSF kernel)
     const double* sat;    // (Nz, Ny + 1, Nx + 1): summed-area table of the zero-model r^2
 };
 
@@ -183,36 +184,40 @@ __device__ __forceinline__ double sat_box(const double* T, int ld, int y0, int y
            T[(long long)y0 * ld + x0];
 }
 
-// KB: one block per (set, output plane zo, band of output rows): the bounding
-// box of the band's nonzero input rows is loaded (cp.async) and convolved in
-// x in place (a warp per 1, 2 or 4 rows, 8 outputs per lane and window), then
-// in y in place (8 x 4 outputs per item, ascending rounds of whole row groups:
-// an output row only overwrites an input row that no later output reads),
-// then the crop, residual (objective.hpp:7-31) and r^2 stream over the box
-// from shared memory against the data; the zero-model residual outside the
-// box comes from the summed-area table.
-constexpr int KB_THREADS = 256;
-constexpr int KB_IT = 2;        // y items per thread and round
+// KB: one block per (set, output plane zo, band of output rows).  The block
+// finds the bounding box of the band's nonzero input row chunks and works
+// through its output rows in passes whose input rows fit the block's shared
+// memory (box-relative row pitch; usually one pass):
+//   - the rows' nonzero segments are loaded from HBM (cp.async), the rest of
+//     the rows that the y FIR reads is zeroed;
+//   - x FIR in place, a warp per 1, 2 or 4 rows, 8 outputs per lane window;
+//   - y FIR in place, 8 x 4 outputs per item, ascending rounds of whole 8-row
+//     groups (an output row only overwrites an input row that no later output
+//     of the pass reads);
+//   - crop, residual (objective.hpp:7-31) and r^2 streamed from shared memory
+//     against the data.
+// The zero-model residual outside the box comes from the summed-area table.
+constexpr int KB_THREADS = 128;
+constexpr int KB_IT = 1;        // y items per thread and round
 
 template<int K>
-__global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs P)
+__global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs P)
 {
     constexpr int NW = (K + 7 + 3) / 4;     // float4 slots of one 8-output x window
+    constexpr int NWARPS = KB_THREADS / 32;
     extern __shared__ float4 sm4[];
-    float* S = reinterpret_cast<float*>(sm4);                   // (band + K + 7, sp), then s_xr
-    __shared__ float warp_part[KB_THREADS / 32];
+    float* S = reinterpret_cast<float*>(sm4);                   // (rows of a pass, bp)
+    __shared__ float warp_part[NWARPS];
+    __shared__ int s_box[4];
     const int zo = blockIdx.x / P.nbands, band = blockIdx.x % P.nbands;
     const int c = blockIdx.y, b = P.set0 + c;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ob0 = band * P.band, ob1 = min(P.Ny, ob0 + P.band);  // output rows [ob0, ob1)
     const int in1 = min(P.Wy, ob1 + K - 1);                        // input rows [ob0, in1)
     const long long prow = ((long long)c * P.Nz + zo) * P.Wy;
-    const int* xr = P.xr + (long long)c * P.Wy * P.nch * P.Nz + zo;   // (y, chunk) at [(y nch + chunk) Nz]
+    const int* xr = P.xrt + prow * P.nch;                          // (y, chunk) at [y nch + chunk]
     const int ld = P.Nx + 1;
     const double* T = P.sat + (long long)zo * (P.Ny + 1) * ld;
-    const int rows_s = P.band + K + 7;
-    int* s_xr = reinterpret_cast<int*>(S + (long long)rows_s * P.sp);   // (in1 - ob0, nch)
-    __shared__ int s_box[4];
     if (threadIdx.x == 0) {
         s_box[0] = INT_MAX; s_box[1] = -1; s_box[2] = INT_MAX; s_box[3] = -1;
     }
@@ -220,12 +225,10 @@ __global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs
     // bounding box of the nonzero input row chunks
     {
         int y0 = INT_MAX, y1 = -1, x0 = INT_MAX, x1 = -1;
-        const int n = (in1 - ob0) * P.nch;
-        for (int i = threadIdx.x; i < n; i += KB_THREADS) {
-            const int v = xr[(long long)(ob0 * P.nch + i) * P.Nz];
-            s_xr[i] = v;
+        for (int i = ob0 * P.nch + threadIdx.x; i < in1 * P.nch; i += KB_THREADS) {
+            const int v = xr[i];
             if (v >= 0) {
-                const int y = ob0 + i / P.nch;
+                const int y = i / P.nch;
                 y0 = min(y0, y);
                 y1 = max(y1, y);
                 x0 = min(x0, v & 0xffff);
@@ -254,197 +257,204 @@ __global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs
     if (y1 < 0) {   // nothing reaches this band: the model is 0 on it
         if (model)
             for (long long i = (long long)ob0 * P.Nx + threadIdx.x; i < (long long)ob1 * P.Nx;
-                 i += blockDim.x)
+                 i += KB_THREADS)
                 model[i] = 0.f;
         if (threadIdx.x == 0) P.partials[part] = sat_box(T, ld, ob0, ob1, 0, P.Nx);
         return;
     }
-    // output box: x in 8-column strips [g_lo, g_hi], y rows [yo_lo, yo_hi]
+    // output box: x in 8-column strips [g_lo, g_hi], rows [yo_lo, yb_end) in 8-row groups
     const int g_lo = max(0, x0 - K + 1) >> 3, g_hi = min(P.Nx - 1, x1) >> 3;
-    const int ns8 = g_hi - g_lo + 1;
+    const int ns8 = g_hi - g_lo + 1, ns4 = 2 * ns8, sl0 = 2 * g_lo;
     const int yo_lo = max(ob0, y0 - K + 1), yo_hi = min(ob1 - 1, y1);
-    const int ngy = (yo_hi - yo_lo + 8) / 8, s4_lo = 2 * g_lo, ns4 = 2 * ns8;
-    // rows [y0, y1], float4 slots [2 g_lo, 2 g_hi + NW): each row chunk's
-    // nonzero range from HBM, zeros elsewhere; the other rows that
-    // the y FIR reads, [yo_lo, y0) and (y1, yo_lo + 8 ngy + K - 2], are zeroed
-    {
-        const int nsl = 2 * (ns8 - 1) + NW, sl0 = 2 * g_lo;
-        const int tc = min(nsl, (int)blockDim.x), tr = blockDim.x / tc;
-        const int ti = threadIdx.x % tc, ty = threadIdx.x / tc;
-        const float4* src = reinterpret_cast<const float4*>(P.mplanes + prow * P.pitch);
-        if (ty < tr) {
-            for (int y = y0 + ty; y <= y1; y += tr) {
-                const int* vr_ = s_xr + (y - ob0) * P.nch;
-                float4* d = reinterpret_cast<float4*>(S + (long long)(y - ob0) * P.sp);
-                const float4* g = src + (long long)y * (P.pitch / 4);
-                for (int sl = sl0 + ti; sl < sl0 + nsl; sl += tc) {
-                    const int ch = sl >> 3;
-                    const int v = ch < P.nch ? vr_[ch] : -1;
-                    if (v >= 0 && sl >= (v & 0xffff) >> 2 && sl <= (v >> 16) >> 2)
-                        cp_async16(d + sl, g + sl);
-                    else
-                        d[sl] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int yb_end = min(ob1, yo_lo + 8 * ((yo_hi - yo_lo + 8) / 8));
+    const int xb0 = 8 * g_lo, xb_end = min(P.Nx, 8 * g_hi + 8);
+    // the zero-model part, issued now so that its loads overlap the passes
+    double outside = 0.0;
+    if (threadIdx.x == 0)
+        outside = sat_box(T, ld, ob0, ob1, 0, P.Nx) - sat_box(T, ld, yo_lo, yb_end, xb0, xb_end);
+    // box-relative rows: float4 slots [sl0, sl0 + nsl), pitch bp (% 32 == 4)
+    const int nsl = 2 * (ns8 - 1) + NW;
+    int bp = 4 * nsl;
+    bp += ((4 - bp % 32) + 32) % 32;
+    const int bo = ((P.cap / bp - (K + 7)) / 8) * 8;        // output rows per pass (>= 8)
+    const float4* src = reinterpret_cast<const float4*>(P.mplanes + prow * P.pitch);
+    const long long pbase = (long long)zo * plane;
+    float sum = 0.f;
+    for (int ys = yo_lo; ys < yb_end; ys += bo) {
+        const int ye = min(yb_end, ys + bo);                 // outputs [ys, ye)
+        const int ng = (ye - ys + 7) / 8;
+        const int rend = ys + 8 * ng + K - 1;                // rows [ys, rend) are read
+        const int ly0 = max(y0, ys), ly1 = min(y1, rend - 1);
+        // load rows [ly0, ly1]: each row chunk's nonzero range, zeros elsewhere
+        if (ly0 <= ly1) {
+            const int tc = min(nsl, KB_THREADS), tr = KB_THREADS / tc;
+            const int ti = threadIdx.x % tc, ty = threadIdx.x / tc;
+            if (ty < tr) {
+                for (int y = ly0 + ty; y <= ly1; y += tr) {
+                    const int* vrow = xr + y * P.nch;
+                    float4* d = reinterpret_cast<float4*>(S + (long long)(y - ys) * bp);
+                    const float4* g = src + (long long)y * (P.pitch / 4);
+                    for (int j = ti; j < nsl; j += tc) {
+                        const int sl = sl0 + j, ch = sl >> 3;
+                        const int v = ch < P.nch ? vrow[ch] : -1;
+                        if (v >= 0 && sl >= (v & 0xffff) >> 2 && sl <= (v >> 16) >> 2)
+                            cp_async16(d + j, g + sl);
+                        else
+                            d[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
                 }
             }
         }
-        const int zt = min(ns4, (int)blockDim.x), zr = blockDim.x / zt;
-        const int zi = threadIdx.x % zt, zy = threadIdx.x / zt;
-        const int yr_end = yo_lo + 8 * ngy + K - 1;      // rows [yo_lo, yr_end) are read
-        if (zy < zr) {
-            for (int y = yo_lo + zy; y < yr_end; y += zr) {
-                if (y >= y0 && y <= y1) continue;
-                float4* d = reinterpret_cast<float4*>(S + (long long)(y - ob0) * P.sp);
-                for (int s4 = s4_lo + zi; s4 < s4_lo + ns4; s4 += zt)
-                    d[s4] = make_float4(0.f, 0.f, 0.f, 0.f);
+        // the other rows that the y FIR reads: zeros in its strips
+        {
+            const int tc = min(ns4, KB_THREADS), tr = KB_THREADS / tc;
+            const int ti = threadIdx.x % tc, ty = threadIdx.x / tc;
+            if (ty < tr) {
+                for (int y = ys + ty; y < rend; y += tr) {
+                    if (y >= ly0 && y <= ly1) continue;
+                    float4* d = reinterpret_cast<float4*>(S + (long long)(y - ys) * bp);
+                    for (int j = ti; j < ns4; j += tc) d[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
             }
         }
         cp_async_wait_all();
-    }
-    __syncthreads();
-    // x FIR in place: S[y][xo] = sum_s vr[s] S[y][xo + s] over the strips; a
-    // warp owns rw whole rows (lane = strip * rw + row), loads before __syncwarp
-    {
-        float vr[K];
+        __syncthreads();
+        // x FIR in place: S[y][xo] = sum_s vr[s] S[y][xo + s]; a warp owns rw
+        // whole rows (lane = strip * rw + row), loads before __syncwarp
+        if (ly0 <= ly1) {
+            float vr[K];
 #pragma unroll
-        for (int s = 0; s < K; ++s) vr[s] = P.vr[s];
-        const int rw = ns8 <= 8 ? 4 : (ns8 <= 16 ? 2 : 1);
-        const int spw = 32 / rw;                    // strips per warp pass
-        const int r = lane % rw, sidx = lane / rw;
-        for (int ry = y0 + warp * rw; ry <= y1; ry += (KB_THREADS / 32) * rw) {
-            const int y = ry + r;
-            float4* row = reinterpret_cast<float4*>(S + (long long)(y - ob0) * P.sp);
-            for (int gs = g_lo; gs <= g_hi; gs += spw) {
-                const int g = gs + sidx;
-                const bool act = g <= g_hi && y <= y1;
-                float w[4 * NW];
-                if (act) {
+            for (int s = 0; s < K; ++s) vr[s] = P.vr[s];
+            const int rw = ns8 <= 8 ? 4 : (ns8 <= 16 ? 2 : 1);
+            const int spw = 32 / rw;                    // strips per warp pass
+            const int r = lane % rw, sidx = lane / rw;
+            for (int ry = ly0 + warp * rw; ry <= ly1; ry += NWARPS * rw) {
+                const int y = ry + r;
+                float4* row = reinterpret_cast<float4*>(S + (long long)(y - ys) * bp);
+                for (int gs = 0; gs < ns8; gs += spw) {
+                    const int gi = gs + sidx;           // strip, box-relative
+                    const bool act = gi < ns8 && y <= ly1;
+                    float w[4 * NW];
+                    if (act) {
 #pragma unroll
-                    for (int m = 0; m < NW; ++m) {
-                        const float4 f = row[2 * g + m];
-                        w[4 * m] = f.x; w[4 * m + 1] = f.y; w[4 * m + 2] = f.z; w[4 * m + 3] = f.w;
+                        for (int m = 0; m < NW; ++m) {
+                            const float4 f = row[2 * gi + m];
+                            w[4 * m] = f.x; w[4 * m + 1] = f.y; w[4 * m + 2] = f.z; w[4 * m + 3] = f.w;
+                        }
                     }
-                }
-                __syncwarp();
-                if (act) {
-                    float o[8];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        float acc = 0.f;
-#pragma unroll
-                        for (int s = 0; s < K; ++s) acc += vr[s] * w[q + s];
-                        o[q] = acc;
-                    }
-                    row[2 * g] = make_float4(o[0], o[1], o[2], o[3]);
-                    row[2 * g + 1] = make_float4(o[4], o[5], o[6], o[7]);
-                }
-                __syncwarp();
-            }
-        }
-    }
-    __syncthreads();
-    // y FIR in place: model(yo, xo) = sum_t ur[t] S[yo + t][xo] (rows outside
-    // [y0, y1] were zeroed), written to S row yo; items of 8 rows x 4 columns in
-    // ascending rounds of whole 8-row groups
-    {
-        float ur[K];
-#pragma unroll
-        for (int t = 0; t < K; ++t) ur[t] = P.ur[t];
-        const int gpr = max(1, KB_THREADS * KB_IT / ns4);   // row groups per round
-        for (int gr0 = 0; gr0 < ngy; gr0 += gpr) {
-            const int nitems = min(gpr, ngy - gr0) * ns4;
-            float acc[KB_IT][8][4];
-#pragma unroll
-            for (int it = 0; it < KB_IT; ++it) {
-                const int item = threadIdx.x + it * KB_THREADS;
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) acc[it][q][k] = 0.f;
-                if (item < nitems) {
-                    const int yb = yo_lo + 8 * (gr0 + item / ns4), s4 = s4_lo + item % ns4;
-#pragma unroll
-                    for (int m = 0; m < K + 7; ++m) {
-                        const float4 p =
-                            reinterpret_cast<const float4*>(S + (long long)(yb + m - ob0) * P.sp)[s4];
+                    __syncwarp();
+                    if (act) {
+                        float o[8];
 #pragma unroll
                         for (int q = 0; q < 8; ++q) {
-                            const int t = m - q;
-                            if (t >= 0 && t < K) {
-                                acc[it][q][0] += ur[t] * p.x;
-                                acc[it][q][1] += ur[t] * p.y;
-                                acc[it][q][2] += ur[t] * p.z;
-                                acc[it][q][3] += ur[t] * p.w;
+                            float acc = 0.f;
+#pragma unroll
+                            for (int s = 0; s < K; ++s) acc += vr[s] * w[q + s];
+                            o[q] = acc;
+                        }
+                        row[2 * gi] = make_float4(o[0], o[1], o[2], o[3]);
+                        row[2 * gi + 1] = make_float4(o[4], o[5], o[6], o[7]);
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        __syncthreads();
+        // y FIR in place: model(yo, xo) = sum_t ur[t] S[yo + t][xo], written to S row yo
+        {
+            float ur[K];
+#pragma unroll
+            for (int t = 0; t < K; ++t) ur[t] = P.ur[t];
+            const int gpr = max(1, KB_THREADS * KB_IT / ns4);   // row groups per round
+            for (int gr0 = 0; gr0 < ng; gr0 += gpr) {
+                const int nitems = min(gpr, ng - gr0) * ns4;
+                float acc[KB_IT][8][4];
+#pragma unroll
+                for (int it = 0; it < KB_IT; ++it) {
+                    const int item = threadIdx.x + it * KB_THREADS;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) acc[it][q][k] = 0.f;
+                    if (item < nitems) {
+                        const int rb = 8 * (gr0 + item / ns4), s4 = item % ns4;
+#pragma unroll
+                        for (int m = 0; m < K + 7; ++m) {
+                            const float4 p =
+                                reinterpret_cast<const float4*>(S + (long long)(rb + m) * bp)[s4];
+#pragma unroll
+                            for (int q = 0; q < 8; ++q) {
+                                const int t = m - q;
+                                if (t >= 0 && t < K) {
+                                    acc[it][q][0] += ur[t] * p.x;
+                                    acc[it][q][1] += ur[t] * p.y;
+                                    acc[it][q][2] += ur[t] * p.z;
+                                    acc[it][q][3] += ur[t] * p.w;
+                                }
                             }
                         }
                     }
                 }
-            }
-            __syncthreads();
+                __syncthreads();
 #pragma unroll
-            for (int it = 0; it < KB_IT; ++it) {
-                const int item = threadIdx.x + it * KB_THREADS;
-                if (item < nitems) {
-                    const int yb = yo_lo + 8 * (gr0 + item / ns4), s4 = s4_lo + item % ns4;
+                for (int it = 0; it < KB_IT; ++it) {
+                    const int item = threadIdx.x + it * KB_THREADS;
+                    if (item < nitems) {
+                        const int rb = 8 * (gr0 + item / ns4), s4 = item % ns4;
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (yb + q < ob1)
-                            reinterpret_cast<float4*>(S + (long long)(yb + q - ob0) * P.sp)[s4] =
-                                make_float4(acc[it][q][0], acc[it][q][1], acc[it][q][2],
-                                            acc[it][q][3]);
+                        for (int q = 0; q < 8; ++q)
+                            if (ys + rb + q < ye)
+                                reinterpret_cast<float4*>(S + (long long)(rb + q) * bp)[s4] =
+                                    make_float4(acc[it][q][0], acc[it][q][1], acc[it][q][2],
+                                                acc[it][q][3]);
+                    }
                 }
+                __syncthreads();
             }
-            __syncthreads();
         }
-    }
-    // crop + residual over the box: rows [yo_lo, yb_end), columns [xb0, xb_end)
-    const int yb_end = min(ob1, yo_lo + 8 * ngy), xb0 = 8 * g_lo, xb_end = min(P.Nx, 8 * g_hi + 8);
-    float sum = 0.f;
-    const long long pbase = (long long)zo * plane;
-    if ((P.Nx & 3) == 0) {
-        // flat float4 index over the box, stepped without divisions
-        const int nv = (xb_end - xb0) >> 2;        // xb0 and xb_end are multiples of 4
-        const int n = (yb_end - yo_lo) * nv;
-        const int dq = KB_THREADS / nv, dr = KB_THREADS % nv;
-        int row = threadIdx.x / nv, col = threadIdx.x % nv;
+        // crop + residual over rows [ys, ye), columns [xb0, xb_end)
+        if ((P.Nx & 3) == 0) {
+            // flat float4 index over the pass, stepped without divisions
+            const int nv = (xb_end - xb0) >> 2;        // xb0 and xb_end are multiples of 4
+            const int n = (ye - ys) * nv;
+            const int dq = KB_THREADS / nv, dr = KB_THREADS % nv;
+            int row = threadIdx.x / nv, col = threadIdx.x % nv;
 #pragma unroll 4
-        for (int i = threadIdx.x; i < n; i += KB_THREADS) {
-            const int yo = yo_lo + row, xo = xb0 + 4 * col;
-            const float4 m = *reinterpret_cast<const float4*>(S + (long long)(yo - ob0) * P.sp + xo);
-            const long long vi = pbase + (long long)yo * P.Nx + xo;
-            const float4 o = *reinterpret_cast<const float4*>(P.obs + vi);
-            const float4 w = *reinterpret_cast<const float4*>(P.iw + vi);
-            const float r0 = (m.x - o.x) * w.x, r1 = (m.y - o.y) * w.y;
-            const float r2 = (m.z - o.z) * w.z, r3 = (m.w - o.w) * w.w;
-            sum += r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3;
-            if (model) *reinterpret_cast<float4*>(model + (long long)yo * P.Nx + xo) = m;
-            row += dq;
-            col += dr;
-            if (col >= nv) {
-                col -= nv;
-                ++row;
-            }
-        }
-    } else {
-        const int nw = xb_end - xb0;
-        const int tc = min(nw, (int)blockDim.x), tr = blockDim.x / tc;
-        const int ti = threadIdx.x % tc, ty = threadIdx.x / tc;
-        if (ty < tr) {
-            for (int yo = yo_lo + ty; yo < yb_end; yo += tr) {
-                for (int j = ti; j < nw; j += tc) {
-                    const int xo = xb0 + j;
-                    const float m = S[(long long)(yo - ob0) * P.sp + xo];
-                    const long long vi = pbase + (long long)yo * P.Nx + xo;
-                    const float r0 = (m - P.obs[vi]) * P.iw[vi];
-                    sum += r0 * r0;
-                    if (model) model[(long long)yo * P.Nx + xo] = m;
+            for (int i = threadIdx.x; i < n; i += KB_THREADS) {
+                const int yo = ys + row, xo = xb0 + 4 * col;
+                const float4 m = *reinterpret_cast<const float4*>(S + (long long)row * bp + 4 * col);
+                const long long vi = pbase + (long long)yo * P.Nx + xo;
+                const float4 o = *reinterpret_cast<const float4*>(P.obs + vi);
+                const float4 w = *reinterpret_cast<const float4*>(P.iw + vi);
+                const float r0 = (m.x - o.x) * w.x, r1 = (m.y - o.y) * w.y;
+                const float r2 = (m.z - o.z) * w.z, r3 = (m.w - o.w) * w.w;
+                sum += r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3;
+                if (model) *reinterpret_cast<float4*>(model + (long long)yo * P.Nx + xo) = m;
+                row += dq;
+                col += dr;
+                if (col >= nv) {
+                    col -= nv;
+                    ++row;
                 }
             }
+        } else {
+            const int nw = xb_end - xb0, n = (ye - ys) * nw;
+            for (int i = threadIdx.x; i < n; i += KB_THREADS) {
+                const int row = i / nw, col = i % nw;
+                const int yo = ys + row, xo = xb0 + col;
+                const float m = S[(long long)row * bp + col];
+                const long long vi = pbase + (long long)yo * P.Nx + xo;
+                const float r0 = (m - P.obs[vi]) * P.iw[vi];
+                sum += r0 * r0;
+                if (model) model[(long long)yo * P.Nx + xo] = m;
+            }
         }
+        __syncthreads();    // S is reloaded by the next pass
     }
     if (model) {
         const int bw = P.Nx;
         for (long long i = (long long)ob0 * bw + threadIdx.x; i < (long long)ob1 * bw;
-             i += blockDim.x) {
+             i += KB_THREADS) {
             const int yo = (int)(i / bw), xo = (int)(i % bw);
             if (yo < yo_lo || yo >= yb_end || xo < xb0 || xo >= xb_end) model[i] = 0.f;
         }
@@ -455,9 +465,7 @@ __global__ void __launch_bounds__(KB_THREADS, 2) kb_psf_residual(BatchKernelArgs
     __syncthreads();
     if (threadIdx.x == 0) {
         float s = 0.f;
-        for (int w = 0; w < KB_THREADS / 32; ++w) s += warp_part[w];
-        const double outside = sat_box(T, ld, ob0, ob1, 0, P.Nx) -
-                               sat_box(T, ld, yo_lo, yb_end, xb0, xb_end);
+        for (int w = 0; w < NWARPS; ++w) s += warp_part[w];
         P.partials[part] = (double)s + outside;
     }
 }
