@@ -53,6 +53,22 @@ def fft_flops_per_eval(geom):
     return 2 * 2.5 * vp * np.log2(vp) + 6 * cp
 
 
+def direct_flops_per_eval(geom):
+    """Dense FIR FLOPs of one direct-mode evaluation: LSF over the window
+    columns, PSF x over the window rows, PSF y over the crop (2 per tap);
+    the kernels skip the exact-zero part of this work."""
+    nx, ny, nz = geom.size
+    kx, ky, kz = geom.kernel_size
+    wx, wy = nx + kx - 1, ny + ky - 1
+    return 2 * (kz * nz * wx * wy + kx * nz * wy * nx + ky * nz * ny * nx)
+
+
+# DRAM bytes (read + write) per evaluation of the direct-mode kernels
+# (ka_lines_lsf + k_xr_transpose + kb_psf_residual), from the ncu capture in
+# profiles/kernels_smdisk_batch128_direct.md (one 128-set launch each, / 128)
+DIRECT_TRAFFIC_PER_EVAL = 4.47e6
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
 
@@ -136,6 +152,20 @@ def barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def fp32_roof(geom, nsets, ms_step, clocks, conv):
+    """Direct mode: dense FIR FLOPs per step over the nominal FP32 CUDA-core
+    peak at the sampled SM clock (148 SMs x 128 lanes x 2 FLOP)."""
+    if conv != 'direct':
+        return None
+    mhz = clocks.get('sm_mhz') or clocks.get('sm_max_mhz') or 1965.0
+    peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    ach = direct_flops_per_eval(geom) * nsets / (ms_step / 1e3) / 1e12
+    return dict(achieved=round(ach, 2), peak=round(peak, 1), unit='TFLOP/s',
+                frac=round(ach / peak, 3), peak_kind='nominal at the sampled SM clock',
+                basis='dense FIR FLOPs per evaluation (LSF + PSF x + PSF y), '
+                      f'{direct_flops_per_eval(geom)} per evaluation')
 
 
 def autotune(w, data, err, nsets, budget_s=60.0):
@@ -250,14 +280,17 @@ def run_b200(args):
                         parallelism=f'dp{world} (independent parameter sets per GPU)'),
             e2e=e2e,
             roofline=dict(bound='hbm', achieved=round(achieved, 1), peak=hbm,
-                          unit='GB/s', frac=round(achieved / hbm, 3), traffic=None,
+                          unit='GB/s', frac=round(achieved / hbm, 3),
+                          traffic=DIRECT_TRAFFIC_PER_EVAL if ev.conv_mode == 'direct' else None,
+                          traffic_unit='DRAM bytes per evaluation (ncu, direct-mode kernels)',
                           peak_kind=peak_kind,
                           basis=f'staged algorithmic bytes per evaluation ({b_eval} B, '
                                 f'reference padding {list(w.geom.size_hi)}) x {nsets} / step time '
                                 '(all kernels of the step)',
                           kernels=kernels, dominant=dominant,
-                          fp32_tflops=round(fft_flops_per_eval(w.geom) * nsets
-                                            / (ms_step / 1e3) / 1e12, 2)),
+                          fft_equiv_tflops=round(fft_flops_per_eval(w.geom) * nsets
+                                                 / (ms_step / 1e3) / 1e12, 2),
+                          fp32=fp32_roof(w.geom, nsets, ms_step, clocks, ev.conv_mode)),
             clocks=clocks,
             gpu_launches=args.steps * (per_chunk * n_chunks + 1),
             plain_per_call=plain,
