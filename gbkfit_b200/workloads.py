@@ -184,20 +184,37 @@ def smdisk_batch128(nsets=512, seed=1234, size=(128, 128, 96), nnodes=30):
 
 
 def smdisk_grad96(seed=99):
+    """The differentiable configuration: 96x96x64 cube, 20 rings on 0-40 px,
+    node-wise surface brightness, rotation and dispersion, PSF FWHM 2.5 px,
+    LSF FWHM 2 channels, 66 parameters (geometry 5, nodes 3 x 20, scale).
+
+    The surface brightness is tapered to 0 at the last node: the disk edge
+    (r = last node) cuts the emission off, and with zero brightness there the
+    model is continuous in the geometry parameters, so finite differences
+    see only the derivatives that the adjoint computes.  ``params`` is the
+    evaluation point, ``extra['truth']`` the parameters of the data cube
+    (noise of sigma = noise_frac x peak), ``extra['scale']`` the evaluation
+    scale."""
     rng = np.random.default_rng(seed)
     nn = 20
     rnodes = np.linspace(0, 40, nn)
     disk = Disk(False, False, rnodes, traits=dict(
         rpt=[traits.bpt('nw_uniform')], vpt=[traits.vpt('nw_tan_uniform')],
         dpt=[traits.dpt('nw_uniform')]))
-    params = dict(vsys=5.0, xpos=48.3, ypos=47.6, posa=35.0, incl=55.0,
-                  bpt_a=np.exp(-rnodes / 12.0) * (1 + 0.1 * rng.standard_normal(nn)),
-                  vpt_vt=200 * np.tanh(rnodes / 6.0) + 5 * rng.standard_normal(nn),
-                  dpt_a=20 + 3 * rng.standard_normal(nn))
+    taper = 1 - (rnodes / rnodes[-1]) ** 4
+    truth = dict(vsys=5.0, xpos=48.3, ypos=47.6, posa=35.0, incl=55.0,
+                 bpt_a=np.exp(-rnodes / 12.0) * (1 + 0.1 * rng.standard_normal(nn)) * taper,
+                 vpt_vt=200 * np.tanh(rnodes / 6.0) + 5 * rng.standard_normal(nn),
+                 dpt_a=20 + 3 * rng.standard_normal(nn))
+    params = dict(vsys=8.0, xpos=48.7, ypos=47.3, posa=37.0, incl=52.0,
+                  bpt_a=truth['bpt_a'] * (1 + 0.05 * rng.standard_normal(nn)),
+                  vpt_vt=truth['vpt_vt'] + 4 * rng.standard_normal(nn),
+                  dpt_a=truth['dpt_a'] + 2 * rng.standard_normal(nn))
     psf = psflsf.PSFGauss(psflsf.gauss_fwhm_to_sigma(2.5))
     lsf = psflsf.LSFGauss(psflsf.gauss_fwhm_to_sigma(2 * 10.0))
     geom = Geometry((96, 96, 64), (1, 1, 10), (0, 0, 31.5), (0, 0, 0), psf, lsf)
-    return Workload('smdisk_grad96', disk, params, geom)
+    return Workload('smdisk_grad96', disk, params, geom,
+                    extra=dict(truth=truth, scale=1.1, noise_seed=seed + 1, noise_frac=0.02))
 
 
 def set_params(w, i):

@@ -190,6 +190,52 @@ int gbkb200_objective_residual_sum_f32(gbkb200_ctx* ctx, const float* residual, 
 int gbkb200_objective_residual_sum_noalloc_f32(const float* residual, int size, int squared,
                                                float* sum, void* stream);
 
+/* ---- differentiable chi^2 of a thin smooth disk (no reference counterpart:
+ *      the reference computes no gradients).  A hand-written adjoint of
+ *      smdisk_evaluate + fft_convolve_cached + crop + residual + residual_sum
+ *      with a multiplicative scale on the convolved model. ------------------ */
+
+/* One pass over the padded cube conv_p (size_p = {px, py, pz}); its crop
+ * [offset, offset + size) is compared with the data (size = {nx, ny, nz}):
+ *   r = (scale * conv - d) / e * mask * weight   (objective.hpp:7-31 order)
+ * Writes g_p = d(chi^2)/d(conv_p) (0 outside the crop; every voxel is written)
+ * and out[0] = chi^2 = sum r^2, out[1] = d(chi^2)/d(scale) (fp64 device
+ * values, block partials summed in a fixed order). */
+int gbkb200_objective_chi2_adjoint_f32(gbkb200_ctx* ctx, const int size_p[3], const int offset[3],
+                                       const int size[3], const float* conv_p, const float* obs_d,
+                                       const float* obs_e, const float* obs_m, float weight,
+                                       float scale, float* g_p, double* out);
+
+/* A thin disk (neither loose nor tilted) with one node-wise surface
+ * brightness (density uid 101), one node-wise rotation curve (velocity uid
+ * 101, traits.hpp:999-1007) and one node-wise dispersion (uid 101); the
+ * sub-node values are those smdisk_evaluate receives as pvalues. */
+typedef struct {
+    int spat_size[2];          /* evaluation grid (x, y) */
+    float spat_step[2];
+    float spat_zero[2];
+    int spec_size;
+    float spec_step;
+    float spec_zero;
+    int nsub;
+    const float* subrnodes;    /* device (nsub) */
+    const float* vsys;         /* device (1), or NULL for 0 */
+    const float *xpos, *ypos, *posa, *incl;   /* device (1 each), degrees for angles */
+    const float *bsub, *vsub, *dsub;          /* device (nsub each) */
+} gbkb200_smdisk_nw_desc;
+
+/* Given g_cube = d(chi^2)/d(scube) on the evaluation grid (spec_size,
+ * spat_size[1], spat_size[0]), overwrites grad (device, 3 nsub + 5 doubles)
+ * with d(chi^2)/d of: the density sub-node values, the rotation sub-node
+ * values, the dispersion sub-node values, vsys, xpos, ypos, posa (per
+ * degree), incl (per degree).  Each spaxel recomputes its ring position,
+ * interpolation weights and line; the truncation of the line window and the
+ * ring boundaries are treated as fixed (derivatives almost everywhere).
+ * Fixed-order fp64 sums across blocks; within a block fp64 shared atomics
+ * (reproducible to rounding).  nsub <= 2046. */
+int gbkb200_gmodel_smdisk_nw_adjoint_f32(gbkb200_ctx* ctx, const gbkb200_smdisk_nw_desc* desc,
+                                         const float* g_cube, double* grad);
+
 /* ---- batched evaluation (no reference counterpart as one call) ---------
  *
  * Evaluates many parameter sets of one thin smooth disk against one data

@@ -313,3 +313,113 @@ def chi2(model, data, error):
     """objective.hpp:7-31 + host/kernels.hpp:502-514 in float64."""
     r = (np.asarray(model, np.float64) - data) / error
     return float(np.sum(r * r))
+
+
+def chi2_gradient_f64(packed, geom, data, error, scale):
+    """fp64 reference gradient of chi^2 for a thin flat disk with node-wise
+    density (uid 101), rotation (uid 101) and dispersion (uid 101): the
+    smdisk line model of gmodels.hpp:645-958 (sky -> disk, math.hpp:63-71;
+    ring interpolation, traits.hpp:138-141, 999-1007; line, gmodels.hpp
+    :92-116) on the padded grid, the circular convolution with geom.pcube()
+    (fft.hpp:98-207), the crop, r = (scale conv - d) / e (objective.hpp:7-31),
+    differentiated analytically in float64 (numpy), every spaxel's line
+    window held fixed.  Returns (chi^2, d chi^2 / d sub-node and geometry
+    values) in the layout of gbkb200_gmodel_smdisk_nw_adjoint_f32 (density,
+    rotation, dispersion sub-nodes, vsys, xpos, ypos, posa, incl), and
+    d chi^2 / d scale."""
+    import scipy.fft
+    f = np.float64
+    sub = np.asarray(packed['subrnodes'], f)
+    ns = len(sub)
+    bs = np.asarray(packed['rpt']['pvalues'], f)
+    vs = np.asarray(packed['vpt']['pvalues'], f)
+    ds = np.asarray(packed['dpt']['pvalues'], f)
+    vsys = float(packed['vsys'][0]) if packed['vsys'] is not None else 0.0
+    xpos, ypos = float(packed['xpos'][0]), float(packed['ypos'][0])
+    phi, inc = np.deg2rad(float(packed['posa'][0])), np.deg2rad(float(packed['incl'][0]))
+    sp, cp, si, ci = np.sin(phi), np.cos(phi), np.sin(inc), np.cos(inc)
+    px, py, pz = geom.size_hi
+    (sx, sy, _), (stx, sty, _), (zx, zy, _) = geom.spat()
+    nz, dz, z0 = geom.spec()
+    X = zx + np.arange(sx) * stx
+    Y = zy + np.arange(sy) * sty
+    xn = X[None, :] - xpos + 0 * Y[:, None]
+    yn = Y[:, None] - ypos + 0 * X[None, :]
+    xr = -xn * sp + yn * cp
+    yr = -xn * cp - yn * sp
+    yd = yr / ci
+    r = np.sqrt(xr * xr + yd * yd)
+    on = (r >= sub[0]) & (r < sub[-1])
+    k = np.clip(np.searchsorted(sub, r, side='right'), 1, ns - 1)
+    s0, s1 = sub[k - 1], sub[k]
+    t = (r - s0) / (s1 - s0)
+    bl = bs[k - 1] + t * (bs[k] - bs[k - 1])
+    on &= bl != 0
+    rho = bl / ci
+    rs = np.where(r > 0, r, 1.0)
+    c = np.where(r > 0, xr / rs, 0.0)
+    sn = np.where(r > 0, yd / rs, 0.0)
+    vrot = vs[k - 1] + t * (vs[k] - vs[k - 1])
+    vv = np.where(r > 0, vrot * c * si, 0.0) + vsys
+    draw = ds[k - 1] + t * (ds[k] - ds[k - 1])
+    sig = np.abs(draw)
+    sgn = np.where(draw < 0, -1.0, 1.0)
+    sig_s = np.where(on, sig, 1.0)
+    lo = np.maximum(np.rint((vv - 5 * sig - z0) / dz), 0)
+    hi = np.minimum(np.rint((vv + 5 * sig - z0) / dz), nz - 1)
+    on &= lo <= hi
+    zv = z0 + np.arange(nz)[:, None, None] * dz
+    iz = np.arange(nz)[:, None, None]
+    win = on[None] & (iz >= lo[None]) & (iz <= hi[None])
+    d = zv - vv[None]
+    L = np.where(win, np.exp(-d * d / (2 * sig_s[None] ** 2)) / (sig_s[None] * np.sqrt(2 * np.pi)),
+                 0.0)
+    model = np.zeros((pz, py, px), f)
+    model[:nz] = rho[None] * L
+    pc = np.asarray(geom.pcube(f), f)
+    K = scipy.fft.rfftn(pc)
+    conv = scipy.fft.irfftn(scipy.fft.rfftn(model) * K, s=model.shape)
+    ex, ey, ez = geom.edge
+    Nx, Ny, Nz = geom.size
+    cc = conv[ez:ez + Nz, ey:ey + Ny, ex:ex + Nx]
+    e = np.asarray(error, f)
+    res = (scale * cc - np.asarray(data, f)) / e
+    chi2 = float(np.sum(res * res))
+    dscale = float(np.sum(2 * res / e * cc))
+    gP = np.zeros_like(model)
+    gP[ez:ez + Nz, ey:ey + Ny, ex:ex + Nx] = 2 * res / e * scale
+    G = scipy.fft.irfftn(scipy.fft.rfftn(gP) * np.conj(K), s=model.shape)[:nz]
+    GL = G * L
+    S0 = GL.sum(0)
+    S1 = (GL * d).sum(0)
+    S2 = (GL * d * d).sum(0)
+    drho = S0
+    dvv = rho * S1 / sig_s ** 2
+    dsig = rho * (S2 / sig_s ** 3 - S0 / sig_s)
+    wb = np.where(on, drho / ci, 0.0)
+    wv = np.where(on & (r > 0), dvv * c * si, 0.0)
+    wd = np.where(on, dsig * sgn, 0.0)
+    grad = np.zeros(3 * ns + 5)
+    for j, w_ in enumerate((wb, wv, wd)):
+        np.add.at(grad, (j * ns + k - 1)[on], ((1 - t) * w_)[on])
+        np.add.at(grad, (j * ns + k)[on], (t * w_)[on])
+    ds_ = s1 - s0
+    dr = wb * (bs[k] - bs[k - 1]) / ds_ + wv * (vs[k] - vs[k - 1]) / ds_ + \
+        wd * (ds[k] - ds[k - 1]) / ds_
+    dc = np.where(r > 0, dvv * vrot * si, 0.0)
+    ti = si / ci
+    di = drho * rho * ti + np.where(r > 0, dvv * vrot * c * ci, 0.0)
+    dxr = np.where(r > 0, dr * c + dc * sn * sn / rs, 0.0)
+    dyd = np.where(r > 0, dr * sn - dc * c * sn / rs, 0.0)
+    dyr = dyd / ci
+    di = di + dyd * yd * ti
+    dxn = -dxr * sp - dyr * cp
+    dyn = dxr * cp - dyr * sp
+    dphi = dxr * yr - dyr * xr
+    g0 = 3 * ns
+    grad[g0 + 0] = np.sum(np.where(on, dvv, 0.0))
+    grad[g0 + 1] = -np.sum(np.where(on, dxn, 0.0))
+    grad[g0 + 2] = -np.sum(np.where(on, dyn, 0.0))
+    grad[g0 + 3] = np.deg2rad(np.sum(np.where(on, dphi, 0.0)))
+    grad[g0 + 4] = np.deg2rad(np.sum(np.where(on, di, 0.0)))
+    return chi2, grad, dscale

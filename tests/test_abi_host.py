@@ -116,3 +116,45 @@ def test_shard_sets_partition():
             parts = [shard_sets(n, r, world) for r in range(world)]
             idx = np.concatenate([np.arange(a, b) for a, b in parts])
             assert np.array_equal(idx, np.arange(n))
+
+
+def test_adjoint_parameter_layout_and_interpolation_jacobian():
+    """The differentiable configuration has 66 parameters; the node -> sub-node
+    Jacobian reproduces the packed sub-node values (_disk.py:107-125)."""
+    from gbkfit_b200 import workloads
+    from gbkfit_b200.adjoint import NW_TRAITS, interpolation_jacobian
+    w = workloads.smdisk_grad96()
+    nn = len(w.disk.rnodes)
+    assert 5 + 3 * nn + 1 == 66
+    jac = interpolation_jacobian(w.disk)
+    assert jac.shape == (nn, w.disk.nsub)
+    packed = w.disk.pack(w.params)
+    for kind, _, pname in NW_TRAITS:
+        sub = np.asarray(w.params[pname], np.float64) @ jac
+        assert np.allclose(sub, packed[kind]['pvalues'], rtol=1e-6, atol=1e-6)
+    assert w.extra['truth']['bpt_a'][-1] == 0.0     # tapered edge
+
+
+def test_adjoint_rejects_unsupported_disks():
+    import pytest
+    from gbkfit_b200 import traits
+    from gbkfit_b200.adjoint import SMDiskChi2
+    from gbkfit_b200.disk import Disk
+    from gbkfit_b200 import workloads
+    g = workloads.smdisk_grad96().geom
+    rn = np.linspace(0, 10, 5)
+    bad = [
+        Disk(False, False, rn, traits=dict(rpt=[traits.bpt('exponential')],
+                                           vpt=[traits.vpt('nw_tan_uniform')],
+                                           dpt=[traits.dpt('nw_uniform')])),
+        Disk(True, False, rn, traits=dict(rpt=[traits.bpt('nw_uniform')],
+                                          vpt=[traits.vpt('nw_tan_uniform')],
+                                          dpt=[traits.dpt('nw_uniform')])),
+        Disk(False, False, rn, traits=dict(rpt=[traits.bpt('nw_uniform')],
+                                           vpt=[traits.vpt('nw_tan_uniform')],
+                                           dpt=[traits.dpt('nw_uniform')],
+                                           wpt=[traits.wpt_axis_range(0, 10, 1)])),
+    ]
+    for d in bad:
+        with pytest.raises(ValueError):
+            SMDiskChi2(d, g, np.zeros(g.size[::-1], np.float32))
