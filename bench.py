@@ -267,6 +267,7 @@ def run_b200(args):
         n_chunks = (nsets + ev.chunk - 1) // ev.chunk
         per_chunk = 3 if ev.conv_mode == 'direct' else 5
         plain = plain_per_call(w, data, err) if args.plain else None
+        serving = serving_run() if args.serving else None
         cpu = cpu_baseline(w, data, err) if args.cpu_baseline else None
         out = dict(
             metric=METRIC, value=round(value, 1), unit=UNIT, n_gpus=world, steps=args.steps,
@@ -294,6 +295,7 @@ def run_b200(args):
             clocks=clocks,
             gpu_launches=args.steps * (per_chunk * n_chunks + 1),
             plain_per_call=plain,
+            serving=serving,
             cpu_baseline=cpu,
         )
     if world > 1:
@@ -301,6 +303,56 @@ def run_b200(args):
         ev._graph = None
         dist.destroy_process_group()
     return out
+
+
+def serving_run(nrequests=10000, slots=8, load=0.8):
+    """The serving stream (workloads.serving_stream: 64 datasets, 70 % smdisk /
+    30 % mcdisk, sides 32-256 px, 32-192 channels, 1e5-1e7 clouds): capacity
+    with every request queued at once, then Poisson arrivals at `load` x
+    capacity; latency = completion - scheduled arrival."""
+    import torch
+    from gbkfit_b200 import workloads
+    from gbkfit_b200.serving import ModelServer, Request
+    st = workloads.serving_stream(nrequests=nrequests, ndatasets=64, rate=1.0, seed=7)
+
+    def reqs():
+        out = []
+        for q in st.requests:
+            d = st.datasets[q['dataset']]
+            r = Request(q['dataset'], q['kind'], d[q['kind']], q['params'], cflux=q['cflux'],
+                        thick=q['thick'])
+            r.prepare()
+            out.append(r)
+        return out
+
+    with ModelServer(slots=slots, hbm_budget=40 << 30) as srv:
+        for d in st.datasets:
+            srv.register(d['key'], d['geom'], d['data'], d['error'])
+        [f.result() for f in [srv.submit(r) for r in reqs()[:300]]]     # plans, allocator
+        srv.stats(reset=True)
+        [f.result() for f in [srv.submit(r) for r in reqs()]]
+        cap = srv.stats(reset=True)['evals_per_s']
+        rate = load * cap
+        arr = np.cumsum(np.random.default_rng(1).exponential(1 / rate, nrequests))
+        rs = reqs()
+        t0 = time.perf_counter()
+        futs = []
+        for r, a in zip(rs, arr):
+            now = time.perf_counter() - t0
+            if a > now:
+                time.sleep(a - now)
+            r.arrival = t0 + a
+            futs.append(srv.submit(r))
+        [f.result() for f in futs]
+        s = srv.stats(reset=True)
+        resident = srv._resident
+    return dict(requests=nrequests, slots=slots, capacity_evals_per_s=round(cap, 1),
+                offered_evals_per_s=round(rate, 1), evals_per_s=round(s['evals_per_s'], 1),
+                p50_ms=round(s['p50_ms'], 3), p99_ms=round(s['p99_ms'], 3),
+                max_ms=round(s['max_ms'], 3), resident_gb=round(resident / 1e9, 3),
+                workload='serving_stream: 64 datasets (sides log-U 32-256 px, channels '
+                         'log-U 32-192, PSF FWHM U(1.5,4) px, LSF FWHM U(1,3) ch), '
+                         '70% smdisk / 30% mcdisk (1e5-1e7 clouds), chi^2 per request')
 
 
 def plain_per_call(w, data, err, nsets=16):
@@ -424,6 +476,7 @@ def main():
     ap.add_argument('--no-tune', dest='tune', action='store_false')
     ap.add_argument('--tune-budget', type=float, default=40.0)
     ap.add_argument('--no-plain', dest='plain', action='store_false')
+    ap.add_argument('--no-serving', dest='serving', action='store_false')
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
     ap.add_argument('--conv', choices=['fft', 'direct'], default=None,
                     help='force the convolution mode (default: tuned)')

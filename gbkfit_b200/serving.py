@@ -1,0 +1,371 @@
+"""Serving loop: continuous batching of model evaluations of uneven sizes.
+
+No reference counterpart (GBKFIT evaluates one model per call).  Samplers and
+fitters register their datasets (cube geometry, PSF, LSF, data and error
+cubes) and then submit model evaluations against them from any thread; each
+submission returns a ``concurrent.futures.Future`` of its chi^2 (and,
+optionally, its model cube).
+
+* Resident state: per dataset the PSF x LSF spectrum on the FFT grid
+  (computed once, _dcube.py:189-207 + fft.hpp:98-125), the data and error
+  cubes; the FFT plans live in the slots' native contexts and are reused by
+  every request of the same grid size.
+* Continuous batching: a scheduler thread keeps up to ``slots`` requests in
+  flight, one per CUDA stream (a native context per stream), so requests of
+  different sizes overlap on the device.  A request is admitted, in arrival
+  order, as soon as a slot is free and the in-flight HBM footprint plus its
+  own fits the budget; completions are polled through CUDA events and the
+  freed slot and memory are given to the next request at once.
+* Per request (all enqueued on its slot's stream): smdisk or mcdisk on the
+  padded grid (gmodels.hpp), the FFT convolution with the dataset's spectrum,
+  the crop (dmodels.hpp:7-46), the residual and its sum of squares
+  (objective.hpp:7-31, host/kernels.hpp:502-514), chi^2 copied to pinned host
+  memory.
+* Latency: completion minus arrival (the submit time, or the arrival time a
+  caller passes).  ``ModelServer.stats()`` gives p50/p99 and throughput.
+"""
+
+import collections
+import threading
+import time
+from concurrent.futures import Future
+
+import numpy as np
+import torch
+
+from . import _native
+from ._native import c_float, c_int, check
+from .disk import KINDS
+
+c_int3 = c_int * 3
+_lib = _native.lib()
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def _cbytes(size_hi):
+    px, py, pz = size_hi
+    return 8 * (px // 2 + 1) * py * pz
+
+
+class Dataset:
+    """A registered dataset: geometry (workloads.Geometry, with PSF/LSF),
+    data and error cubes (nz, ny, nx); resident on the device with the
+    PSF x LSF spectrum of its FFT grid."""
+
+    def __init__(self, key, geom, data, error, ctx, dev, stream):
+        self.key, self.geom = key, geom
+        f32 = lambda a: None if a is None else torch.as_tensor(
+            np.ascontiguousarray(a, np.float32)).to(dev)
+        self.obs, self.err = f32(data), f32(error)
+        self.size_hi = tuple(geom.size_hi)
+        px, py, pz = self.size_hi
+        pcube = f32(geom.pcube(np.float32))
+        self.spectrum = torch.empty(_cbytes(self.size_hi) // 4, dtype=torch.float32, device=dev)
+        with torch.cuda.stream(stream):
+            check(_lib.gbkb200_fft_r2c_f32(ctx.handle, c_int3(*self.size_hi), _ptr(pcube),
+                                           _ptr(self.spectrum)), 'fft_r2c')
+        stream.synchronize()
+        self.footprint = self.spectrum.numel() * 4 + 2 * 4 * int(np.prod(geom.size))
+
+    def request_footprint(self):
+        """Device bytes of one in-flight request: padded cube, its spectrum,
+        the cropped model and the residual."""
+        px, py, pz = self.size_hi
+        return 4 * px * py * pz + _cbytes(self.size_hi) + 8 * int(np.prod(self.geom.size))
+
+
+class Request:
+    """One model evaluation: kind 'smdisk' or 'mcdisk'; disk
+    (gbkfit_b200.disk.Disk) and its parameter dict; for mcdisk the cloud
+    flux; thick: evaluate on the 3-D spatial grid (thick disks)."""
+
+    def __init__(self, dataset, kind, disk, params, cflux=None, thick=False, want_model=False,
+                 arrival=None):
+        if kind not in ('smdisk', 'mcdisk'):
+            raise ValueError(f"unknown request kind '{kind}'")
+        if kind == 'mcdisk' and not cflux:
+            raise ValueError("an mcdisk request needs its cloud flux")
+        self.dataset, self.kind, self.disk, self.params = dataset, kind, disk, params
+        self.cflux, self.thick, self.want_model = cflux, thick, want_model
+        self.arrival = arrival
+        self.admit = self.done = None
+        self.future = Future()
+        self.blob = self.layout = None
+
+    def prepare(self):
+        """Pack the parameters (Disk.pack, and the cloud budget of mcdisk)
+        into one byte blob: the arrays at 16-byte aligned offsets."""
+        packed = self.disk.pack(self.params)
+        arrays = []
+        for k in ('subrnodes', 'vsys', 'xpos', 'ypos', 'posa', 'incl'):
+            arrays.append((k, packed[k]))
+        for k in KINDS:
+            t = packed[k]
+            for f in ('uids', 'cvalues', 'ccounts', 'pvalues', 'pcounts'):
+                arrays.append((k + '.' + f, None if t is None else t[f]))
+        if self.kind == 'mcdisk':
+            csum = self.disk.ncloudscsum(self.params, self.cflux)
+            arrays.append(('csum', np.asarray(csum, np.int32)))
+            arrays.append(('hoi', np.asarray(self.disk.hasordint(), np.uint8)))
+        layout, off, chunks = {}, 0, []
+        for name, a in arrays:
+            if a is None:
+                layout[name] = (None, 0)
+                continue
+            a = np.ascontiguousarray(a)
+            if a.dtype == np.float64:
+                a = a.astype(np.float32)
+            b = a.view(np.uint8).ravel()
+            layout[name] = (off, a.size)
+            chunks.append((off, b))
+            off += (b.size + 15) // 16 * 16
+        blob = np.zeros(max(off, 16), np.uint8)
+        for o, b in chunks:
+            blob[o:o + b.size] = b
+        if self.kind == 'mcdisk':
+            c = layout['csum']
+            self.nclouds = int(arrays[-2][1][-1]) if c[1] else 0
+        self.blob, self.layout = blob, layout
+
+
+class _Slot:
+    STAGE = 1 << 20     # bytes of a request's packed parameters at most
+
+    def __init__(self, dev, mc_seed):
+        self.stream = torch.cuda.Stream(dev)
+        self.h_stage = torch.empty(self.STAGE, dtype=torch.uint8, pin_memory=True)
+        self.d_stage = torch.empty(self.STAGE, dtype=torch.uint8, device=dev)
+        self.ctx = _native.Context(device=dev.index, stream=self.stream, sync=False)
+        self.ctx.set_mcdisk(mc_seed, 0)
+        self.event = torch.cuda.Event()
+        self.out = torch.empty(1, dtype=torch.float32, pin_memory=True)
+        self.req = None
+        self.keep = None
+        self.bytes = 0
+
+
+class ModelServer:
+    """Continuous-batching model-evaluation server on one GPU.
+
+    hbm_budget: device bytes for the registered datasets plus the in-flight
+    requests; slots: requests in flight at most (one CUDA stream each)."""
+
+    def __init__(self, device=0, hbm_budget=8 << 30, slots=8, mc_seed=42):
+        self.dev = torch.device('cuda', device)
+        self.budget = int(hbm_budget)
+        self._setup_stream = torch.cuda.Stream(self.dev)
+        self._setup_ctx = _native.Context(device=device, stream=self._setup_stream, sync=False)
+        self.datasets = {}
+        self._slots = [_Slot(self.dev, mc_seed) for _ in range(int(slots))]
+        self._queue = collections.deque()
+        self._cv = threading.Condition()
+        self._stop = False
+        self._resident = 0          # dataset bytes
+        self._inflight = 0          # in-flight request bytes
+        self.max_inflight_bytes = 0
+        self.max_inflight = 0
+        self._done = []
+        self._error = None
+        self._thread = threading.Thread(target=self._run, name='gbkb200-serving', daemon=True)
+        self._thread.start()
+
+    # ---- datasets --------------------------------------------------------------
+    def register(self, key, geom, data, error=None):
+        """Make a dataset resident (its spectrum is computed now)."""
+        with torch.cuda.device(self.dev):
+            ds = Dataset(key, geom, data, error, self._setup_ctx, self.dev, self._setup_stream)
+        with self._cv:
+            if key in self.datasets:
+                raise KeyError(f"dataset {key!r} is already registered")
+            if self._resident + ds.footprint + ds.request_footprint() > self.budget:
+                raise MemoryError(f"dataset {key!r} does not fit the HBM budget")
+            self.datasets[key] = ds
+            self._resident += ds.footprint
+        return ds
+
+    def unregister(self, key):
+        with self._cv:
+            ds = self.datasets.pop(key)
+            self._resident -= ds.footprint
+
+    # ---- requests --------------------------------------------------------------
+    def submit(self, request):
+        """Queue a Request; returns its Future (result: dict(chi2=..., and
+        model=(nz, ny, nx) array when want_model))."""
+        if request.dataset not in self.datasets:
+            raise KeyError(f"unknown dataset {request.dataset!r}")
+        if request.arrival is None:
+            request.arrival = time.perf_counter()
+        if request.blob is None:
+            request.prepare()
+        if request.blob.size > _Slot.STAGE:
+            raise ValueError("the request's parameter arrays exceed the staging buffer")
+        with self._cv:
+            if self._error is not None:
+                raise RuntimeError("the serving loop stopped") from self._error
+            self._queue.append(request)
+            self._cv.notify()
+        return request.future
+
+    def evaluate(self, request):
+        """Submit and wait."""
+        return self.submit(request).result()
+
+    def close(self):
+        with self._cv:
+            self._stop = True
+            self._cv.notify()
+        self._thread.join()
+        for s in self._slots:
+            s.stream.synchronize()
+            s.ctx.close()
+        self._setup_ctx.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def stats(self, reset=False):
+        """Latency percentiles (ms), throughput and occupancy of the
+        completed requests since the last reset."""
+        with self._cv:
+            done = list(self._done)
+            if reset:
+                self._done.clear()
+        if not done:
+            return dict(requests=0)
+        lat = np.array([r.done - r.arrival for r in done]) * 1e3
+        t0 = min(r.arrival for r in done)
+        t1 = max(r.done for r in done)
+        return dict(requests=len(done), p50_ms=float(np.percentile(lat, 50)),
+                    p99_ms=float(np.percentile(lat, 99)), mean_ms=float(lat.mean()),
+                    max_ms=float(lat.max()), evals_per_s=len(done) / max(t1 - t0, 1e-9),
+                    max_inflight=self.max_inflight, max_inflight_bytes=self.max_inflight_bytes)
+
+    # ---- scheduler -------------------------------------------------------------
+    def _run(self):
+        try:
+            with torch.cuda.device(self.dev):
+                while True:
+                    with self._cv:
+                        busy = [s for s in self._slots if s.req is not None]
+                        if self._stop and not busy and not self._queue:
+                            return
+                        if not busy and not self._queue:
+                            self._cv.wait()
+                            continue
+                    progressed = False
+                    for s in busy:
+                        if s.event.query():
+                            self._complete(s)
+                            progressed = True
+                    while True:
+                        with self._cv:
+                            free = [s for s in self._slots if s.req is None]
+                            if not free or not self._queue:
+                                break
+                            req = self._queue[0]
+                            need = self.datasets[req.dataset].request_footprint()
+                            if self._resident + self._inflight + need > self.budget and \
+                                    self._inflight > 0:
+                                break
+                            self._queue.popleft()
+                            self._inflight += need
+                            nbusy = len(self._slots) - len(free) + 1
+                            self.max_inflight = max(self.max_inflight, nbusy)
+                            self.max_inflight_bytes = max(self.max_inflight_bytes, self._inflight)
+                        self._launch(free[0], req, need)
+                        progressed = True
+                    if not progressed:
+                        time.sleep(2e-5)
+        except BaseException as e:      # fail every pending future, not the process
+            with self._cv:
+                self._error = e
+                pending = list(self._queue) + [s.req for s in self._slots if s.req is not None]
+                self._queue.clear()
+            for r in pending:
+                if not r.future.done():
+                    r.future.set_exception(e)
+
+    def _launch(self, slot, req, need):
+        ds = self.datasets[req.dataset]
+        g = ds.geom
+        req.admit = time.perf_counter()
+        slot.req, slot.bytes = req, need
+        px, py, pz = ds.size_hi
+        nx, ny, nz = g.size
+        h = slot.ctx.handle
+        # parameters: one pinned -> device copy into the slot's staging buffers
+        nb = req.blob.size
+        slot.h_stage.numpy()[:nb] = req.blob
+        base = slot.d_stage.data_ptr()
+        lay = req.layout
+        P = lambda name: None if lay[name][0] is None else base + lay[name][0]
+        N = lambda name: lay[name][1]
+        with torch.cuda.stream(slot.stream):
+            slot.d_stage[:nb].copy_(slot.h_stage[:nb], non_blocking=True)
+            scube = torch.zeros((pz, py, px), device=self.dev)
+            work = torch.empty(_cbytes(ds.size_hi) // 4, dtype=torch.float32, device=self.dev)
+            crop = torch.empty((nz, ny, nx), device=self.dev)
+            res = torch.empty((nz, ny, nx), device=self.dev)
+            total = torch.empty(1, dtype=torch.float32, device=self.dev)
+            ss, st, sz = g.spat(req.thick)
+            spec = g.spec()
+            args = [N('subrnodes'), P('subrnodes'), P('vsys'), P('xpos'), P('ypos'), P('posa'),
+                    P('incl')]
+            for k, counted in (('rpt', True), ('rht', False), ('vpt', True), ('vht', False),
+                               ('dpt', True), ('dht', False), ('zpt', True), ('spt', True),
+                               ('wpt', True)):
+                if counted:
+                    args.append(N(k + '.uids'))
+                args += [P(k + '.' + f) for f in ('uids', 'cvalues', 'ccounts', 'pvalues',
+                                                  'pcounts')]
+            args.append(None)   # opacity
+            args += [int(ss[0]), int(ss[1]), int(ss[2]), float(st[0]), float(st[1]),
+                     float(st[2]), float(sz[0]), float(sz[1]), float(sz[2]), int(spec[0]),
+                     float(spec[1]), float(spec[2])]
+            args += [None, scube.data_ptr()] + [None] * 8
+            loose, tilted = int(req.disk.loose), int(req.disk.tilted)
+            if req.kind == 'smdisk':
+                check(_lib.gbkb200_gmodel_smdisk_evaluate_f32(h, loose, tilted, *args),
+                      'smdisk_evaluate')
+            else:
+                check(_lib.gbkb200_gmodel_mcdisk_evaluate_f32(
+                    h, float(req.cflux), req.nclouds, P('csum'), N('csum'), P('hoi'), loose,
+                    tilted, *args), 'mcdisk_evaluate')
+            check(_lib.gbkb200_fft_convolve_f32(h, c_int3(*ds.size_hi), _ptr(scube), _ptr(work),
+                                                _ptr(ds.spectrum)), 'fft_convolve')
+            check(_lib.gbkb200_dmodel_dcube_downscale_f32(h, c_int3(1, 1, 1), c_int3(*g.edge),
+                                                          c_int3(*ds.size_hi), c_int3(*g.size),
+                                                          _ptr(scube), _ptr(crop)), 'crop')
+            check(_lib.gbkb200_objective_residual_f32(h, _ptr(ds.obs), _ptr(ds.err), None,
+                                                      _ptr(crop), None, None, crop.numel(),
+                                                      c_float(1.0), _ptr(res)), 'residual')
+            check(_lib.gbkb200_objective_residual_sum_f32(h, _ptr(res), res.numel(), 1,
+                                                          _ptr(total)), 'residual_sum')
+            slot.out.copy_(total, non_blocking=True)
+            slot.event.record(slot.stream)
+        slot.keep = (scube, work, crop, res, total)
+
+    def _complete(self, slot):
+        req = slot.req
+        out = dict(chi2=float(slot.out[0]))
+        if req.want_model:
+            out['model'] = slot.keep[2].cpu().numpy()
+        st = slot.ctx.handle
+        # status raised by the kernels of this request (unknown trait uid)
+        rc = _lib.gbkb200_ctx_synchronize(st)
+        req.done = time.perf_counter()
+        with self._cv:
+            self._inflight -= slot.bytes
+            slot.req, slot.keep, slot.bytes = None, None, 0
+            self._done.append(req)
+        if rc:
+            req.future.set_exception(_native.NativeError(rc, 'serving request'))
+        else:
+            req.future.set_result(out)

@@ -20,6 +20,10 @@ objective workloads, a seeded noisy data cube.
   peak)^2); Gaussian PSF FWHM 3 px, Gaussian LSF FWHM 1.5 channels.
 * ``smdisk_grad96``: 96x96x64 cube, 20 rings, node-wise vrot/vdisp/surface
   brightness (the 66-parameter gradient workload).
+* ``serving_stream``: Poisson-arriving requests, 70 % smdisk / 30 % mcdisk,
+  against datasets with log-uniform sides 32-256 px and 32-192 channels, each
+  with its own Gaussian PSF (FWHM 1.5-4 px) and LSF (FWHM 1-3 channels);
+  mcdisk requests draw 1e5-1e7 clouds log-uniformly.
 """
 
 import numpy as np
@@ -221,3 +225,78 @@ def set_params(w, i):
     """Parameter set i of a batched workload as a single-set dict."""
     return {k: (v[i] if np.ndim(v) and np.shape(v)[0] == w.nsets else v)
             for k, v in w.params.items()}
+
+
+class ServingStream:
+    """Datasets and requests of a serving run (see serving_stream)."""
+
+    def __init__(self, datasets, requests, arrivals):
+        self.datasets = datasets        # list of dict(key, geom, data, error, smdisk, mcdisk)
+        self.requests = requests        # list of dict(dataset, kind, params, cflux, thick)
+        self.arrivals = arrivals        # seconds from the start, increasing
+
+
+def _loguniform(rng, lo, hi, n=None):
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+
+
+def serving_stream(nrequests=10000, ndatasets=64, rate=2000.0, seed=7, max_side=256,
+                   max_channels=192, max_clouds=1e7, nrings=30):
+    """A request stream of samplers and fitters: ndatasets datasets (cube
+    sides log-uniform 32-max_side px, channels 32-max_channels, 10 km/s
+    channels; Gaussian PSF FWHM U(1.5, 4) px, Gaussian LSF FWHM U(1, 3)
+    channels; data and error: seeded noise), and nrequests requests arriving
+    as a Poisson process of the given rate (1/s), each against a uniformly
+    drawn dataset: 70 % smdisk (thin disk, node-wise surface brightness
+    exp(N(0, 0.5)), rotation U(50, 300) km/s, dispersion U(5, 40) km/s,
+    incl U(20, 80), PA U(0, 360), as the batched configuration) and 30 %
+    mcdisk (thick exponential disk with a sech2 height profile, flat rotation
+    beyond a linear rise, constant dispersion, clouds log-uniform 1e5 to
+    max_clouds)."""
+    rng = np.random.default_rng(seed)
+    datasets = []
+    for i in range(ndatasets):
+        nx, ny = (int(round(v)) for v in _loguniform(rng, 32, max_side, 2))
+        nz = int(round(_loguniform(rng, 32, max_channels)))
+        psf = psflsf.PSFGauss(psflsf.gauss_fwhm_to_sigma(rng.uniform(1.5, 4.0)))
+        lsf = psflsf.LSFGauss(psflsf.gauss_fwhm_to_sigma(rng.uniform(1.0, 3.0) * 10.0))
+        geom = Geometry((nx, ny, nz), (1, 1, 10), (0, 0, (nz - 1) / 2), (0, 0, 0), psf, lsf)
+        rmax = 0.45 * min(nx, ny)
+        sm = Disk(False, False, np.linspace(0, rmax, nrings), traits=dict(
+            rpt=[traits.bpt('nw_uniform')], vpt=[traits.vpt('nw_tan_uniform')],
+            dpt=[traits.dpt('nw_uniform')]))
+        mc = Disk(False, False, np.linspace(0, rmax, 21), traits=dict(
+            rpt=[traits.bpt('exponential')], rht=[traits.bht('sech2')],
+            vpt=[traits.vpt('tan_lramp')], vht=[traits.vht_one()],
+            dpt=[traits.dpt('uniform')], dht=[traits.dht_one()]))
+        sigma = 0.01
+        data = rng.standard_normal((nz, ny, nx), dtype=np.float32) * np.float32(sigma)
+        err = np.full((nz, ny, nx), sigma, np.float32)
+        datasets.append(dict(key=i, geom=geom, data=data, error=err, smdisk=sm, mcdisk=mc,
+                             centre=((nx - 1) / 2, (ny - 1) / 2)))
+    requests = []
+    for j in range(nrequests):
+        d = datasets[int(rng.integers(ndatasets))]
+        cx, cy = d['centre']
+        if rng.uniform() < 0.7:
+            disk = d['smdisk']
+            nn = len(disk.rnodes)
+            params = dict(vsys=0.0, xpos=cx, ypos=cy, posa=rng.uniform(0, 360),
+                          incl=rng.uniform(20, 80), bpt_a=np.exp(rng.normal(0, 0.5, nn)),
+                          vpt_vt=rng.uniform(50, 300, nn), dpt_a=rng.uniform(5, 40, nn))
+            requests.append(dict(dataset=d['key'], kind='smdisk', params=params, cflux=None,
+                                 thick=False))
+        else:
+            disk = d['mcdisk']
+            rmax = disk.rnodes[-1]
+            params = dict(vsys=0.0, xpos=cx, ypos=cy, posa=rng.uniform(0, 360),
+                          incl=rng.uniform(20, 80), bpt_a=1.0, bpt_s=rmax / 4,
+                          bht_s=rng.uniform(1, 3), vpt_rt=rmax / 10,
+                          vpt_vt=rng.uniform(150, 300), dpt_a=rng.uniform(10, 30))
+            n = _loguniform(rng, 1e5, max_clouds)
+            total = np.sum(disk.traits['rpt'][0].integrate(dict(a=1.0, s=rmax / 4),
+                                                           disk.subrnodes[1:-1]))
+            requests.append(dict(dataset=d['key'], kind='mcdisk', params=params,
+                                 cflux=float(total / n), thick=True))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nrequests))
+    return ServingStream(datasets, requests, arrivals)

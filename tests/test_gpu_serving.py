@@ -1,0 +1,99 @@
+"""Serving loop (gbkfit_b200.serving): every result is the same alone and in
+the mix, chi^2 agrees with the fp64 oracle, and admission keeps the in-flight
+footprint inside the HBM budget."""
+
+import numpy as np
+import pytest
+
+from tests.helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_stream(n=48, seed=11):
+    from gbkfit_b200 import workloads
+    return workloads.serving_stream(nrequests=n, ndatasets=10, rate=1e4, seed=seed, max_side=96,
+                                    max_channels=64, max_clouds=2e5, nrings=12)
+
+
+def _requests(stream, want_model=False):
+    from gbkfit_b200.serving import Request
+    out = []
+    for q in stream.requests:
+        d = stream.datasets[q['dataset']]
+        out.append(Request(q['dataset'], q['kind'], d[q['kind']], q['params'], cflux=q['cflux'],
+                           thick=q['thick'], want_model=want_model))
+    return out
+
+
+def _register(server, stream):
+    for d in stream.datasets:
+        server.register(d['key'], d['geom'], d['data'], d['error'])
+
+
+def test_results_same_alone_and_in_mix(gpu):
+    from gbkfit_b200.serving import ModelServer
+    stream = _small_stream()
+    kinds = [q['kind'] for q in stream.requests]
+    assert 'smdisk' in kinds and 'mcdisk' in kinds
+    with ModelServer(slots=1) as alone:
+        _register(alone, stream)
+        ref = [alone.evaluate(r) for r in _requests(stream, want_model=True)]
+        assert alone.stats()['max_inflight'] == 1
+    with ModelServer(slots=8) as mix:
+        _register(mix, stream)
+        futs = [mix.submit(r) for r in _requests(stream, want_model=True)]
+        got = [f.result() for f in futs]
+        assert mix.stats()['max_inflight'] > 1      # the requests overlapped
+    for k, a, b in zip(kinds, ref, got):
+        if k == 'smdisk':
+            assert a['chi2'] == b['chi2'] and np.array_equal(a['model'], b['model'])
+        else:   # cloud splatting with atomics: summation order differs in the last bit
+            assert abs(a['chi2'] - b['chi2']) <= 1e-5 * abs(a['chi2'])
+            assert rel_err(b['model'], a['model']) <= 1e-5
+
+
+def test_chi2_matches_oracle(gpu, oracle_built):
+    from oracle.oracle import chi2, scube_pipeline
+    from gbkfit_b200.serving import ModelServer
+    stream = _small_stream(n=12, seed=5)
+    reqs = [r for r in _requests(stream) if r.kind == 'smdisk'][:3]
+    assert reqs
+    with ModelServer(slots=4) as srv:
+        _register(srv, stream)
+        got = [f.result()['chi2'] for f in [srv.submit(r) for r in reqs]]
+    for r, c in zip(reqs, got):
+        d = stream.datasets[r.dataset]
+        m = scube_pipeline(r.disk.pack(r.params), d['geom'])
+        ref = chi2(m, d['data'], d['error'])
+        assert abs(c - ref) <= 1e-4 * ref, (c, ref)
+
+
+def test_admission_respects_hbm_budget(gpu):
+    from gbkfit_b200.serving import ModelServer
+    stream = _small_stream(n=30, seed=3)
+    with ModelServer(slots=8) as probe:
+        _register(probe, stream)
+        resident = probe._resident
+        need = max(ds.request_footprint() for ds in probe.datasets.values())
+    budget = resident + int(2.5 * need)
+    with ModelServer(slots=8, hbm_budget=budget) as srv:
+        _register(srv, stream)
+        futs = [srv.submit(r) for r in _requests(stream)]
+        for f in futs:
+            assert np.isfinite(f.result()['chi2'])
+        st = srv.stats()
+    assert st['requests'] == len(futs)
+    assert st['max_inflight_bytes'] <= budget - resident
+    assert st['max_inflight'] <= 8
+
+
+def test_unknown_dataset_and_budget_errors(gpu):
+    from gbkfit_b200.serving import ModelServer, Request
+    stream = _small_stream(n=2)
+    d = stream.datasets[0]
+    with ModelServer(slots=2, hbm_budget=1 << 20) as srv:
+        with pytest.raises(MemoryError):
+            srv.register(d['key'], d['geom'], d['data'], d['error'])
+        with pytest.raises(KeyError):
+            srv.submit(Request(123, 'smdisk', d['smdisk'], stream.requests[0]['params']))
