@@ -77,6 +77,8 @@ struct gbkb200_ctx {
     void* fft_state = nullptr;    // FFT plan / spectrum caches (fft.cu)
     void* reduce_scratch = nullptr;
     size_t reduce_scratch_bytes = 0;
+    void* mc_scratch = nullptr;     // fixed-point accumulators of deterministic mcdisk
+    size_t mc_scratch_bytes = 0;
 };
 
 int gbk_finish(gbkb200_ctx* ctx);   // launch check, and sync + status read in sync mode

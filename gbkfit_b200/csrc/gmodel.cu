@@ -363,6 +363,112 @@ __global__ void __launch_bounds__(256) mcdisk_kernel(DiskArgs a, McArgs m, int* 
     if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
 }
 
+// ---- deterministic mcdisk: 64-bit fixed-point accumulation ------------------
+// Integer addition is associative, so the sums do not depend on the order in
+// which clouds land.  A bound pass finds the largest contribution M of the
+// call (the line peak |orv| / (sigma sqrt(2 pi)) for the cube, |orv| and |rv|
+// for the maps); contributions are scaled by 2^k with nclouds * M * 2^k <
+// 2^62 (no overflow whatever the cloud positions), rounded to integers and
+// added with 64-bit atomics; the sums are then added to the float outputs.
+
+__device__ __forceinline__ void atomic_max_abs(unsigned* m, float v)
+{
+    // non-negative floats order as their bit patterns
+    v = fabsf(v);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(m, __float_as_uint(v));
+}
+
+// exponent k of the fixed-point scale 2^k for the bound M (bit pattern)
+__device__ __forceinline__ int fixed_shift(unsigned mbits, int nclouds)
+{
+    const float M = __uint_as_float(mbits);
+    int e = 0;
+    frexpf(M > 0.f ? M : 1.f, &e);            // M < 2^e
+    const int cb = 32 - __clz(nclouds);       // nclouds < 2^cb
+    return 62 - cb - e;
+}
+
+__device__ __forceinline__ void fixed_add(long long* acc, float v, int k)
+{
+    const long long q = llrint((double)v * ldexp(1.0, k));
+    atomicAdd(reinterpret_cast<unsigned long long*>(acc), (unsigned long long)q);
+}
+
+// bound[0]: cube contributions, bound[1]: map contributions
+__global__ void __launch_bounds__(256) mcdisk_bound_kernel(DiskArgs a, McArgs m, unsigned* bound)
+{
+    int bad = 0;
+    for (int base = blockIdx.x * blockDim.x; base < m.nclouds; base += gridDim.x * blockDim.x) {
+        const int ci = base + threadIdx.x;
+        float vc = 0.f, vm = 0.f;
+        int x, y, z;
+        SpaxelOut o;
+        if (ci < m.nclouds && mcdisk_cloud(a, m, ci, x, y, z, o, bad)) {
+            int zlo, zhi;
+            if (a.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi))
+                vc = o.orv * (1 / (o.dv * sqrtf(2 * GBK_PI)));
+            vm = fmaxf(fabsf(o.orv), fabsf(o.rv));
+        }
+        atomic_max_abs(&bound[0], vc);
+        atomic_max_abs(&bound[1], vm);
+    }
+}
+
+struct McFixed {
+    long long *scube, *image, *rdata, *rdata_cmp, *ordata, *ordata_cmp;
+    const unsigned* bound;
+};
+
+__global__ void __launch_bounds__(256) mcdisk_fixed_kernel(DiskArgs a, McArgs m, McFixed f,
+                                                           int* status)
+{
+    int bad = 0;
+    const int kc = fixed_shift(f.bound[0], m.nclouds), km = fixed_shift(f.bound[1], m.nclouds);
+    for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < m.nclouds;
+         ci += gridDim.x * blockDim.x) {
+        int x, y, z;
+        SpaxelOut o;
+        if (!mcdisk_cloud(a, m, ci, x, y, z, o, bad)) continue;
+        const long long sp = x + (long long)a.sx * y;
+        if (f.image) fixed_add(&f.image[sp], o.orv, km);
+        int zlo, zhi;
+        if (f.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
+            const float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
+            const float inv2c2 = 2 * o.dv * o.dv;
+            const long long plane = (long long)a.sx * a.sy;
+            for (int zs = zlo; zs <= zhi; ++zs) {
+                const float zv = a.spec_zero + zs * a.spec_step;
+                const float d = zv - o.vv;
+                fixed_add(&f.scube[sp + plane * zs], o.orv * (amp * expf(-d * d / inv2c2)), kc);
+            }
+        }
+        const long long idx = idx3(x, y, z, a.sx, a.sy);
+        // last-writer-wins assignments, racy as in the reference
+        if (a.wdata) a.wdata[idx] = o.wv;
+        if (a.wdata_cmp) a.wdata_cmp[idx] = o.wv;
+        if (f.rdata) fixed_add(&f.rdata[idx], o.rv, km);
+        if (f.rdata_cmp) fixed_add(&f.rdata_cmp[idx], o.rv, km);
+        if (f.ordata) fixed_add(&f.ordata[idx], o.orv, km);
+        if (f.ordata_cmp) fixed_add(&f.ordata_cmp[idx], o.orv, km);
+        if (a.vdata_cmp) a.vdata_cmp[idx] = o.vv;
+        if (a.ddata_cmp) a.ddata_cmp[idx] = o.dv;
+    }
+    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
+}
+
+// out[i] += acc[i] / 2^k
+__global__ void fixed_to_float_kernel(const long long* acc, float* out, long long n,
+                                      const unsigned* bound, int which, int nclouds)
+{
+    const int k = fixed_shift(bound[which], nclouds);
+    const double inv = ldexp(1.0, -k);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        if (acc[i]) out[i] += (float)((double)acc[i] * inv);
+}
+
 // ---- wcube (gmodels.hpp:52-82) -----------------------------------------------
 __global__ void wcube_kernel(int sx, int sy, int sz, int spec_z, const float* spat, float* spec)
 {
@@ -482,7 +588,49 @@ extern "C" int gbkb200_gmodel_mcdisk_evaluate_f32(gbkb200_ctx* ctx, float cflux,
     m.seed = ctx->seed;
     int blocks = (nclouds + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    mcdisk_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, ctx->d_status);
+    if (ctx->mc_mode != 1) {
+        mcdisk_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, ctx->d_status);
+        GBK_CUDA_TRY(cudaGetLastError());
+        return gbk_finish(ctx);
+    }
+    // deterministic: fixed-point accumulators in the context's scratch
+    const long long nsp = (long long)a.sx * a.sy, nsv = nsp * a.sz;
+    const long long ncube = a.scube ? nsp * a.spec_size : 0;
+    float* outs[6] = {a.scube, a.image, a.rdata, a.rdata_cmp, a.ordata, a.ordata_cmp};
+    const long long lens[6] = {ncube, a.image ? nsp : 0, a.rdata ? nsv : 0,
+                               a.rdata_cmp ? nsv : 0, a.ordata ? nsv : 0, a.ordata_cmp ? nsv : 0};
+    long long total = 2;    // the two bounds, as one 8-byte slot
+    for (long long l : lens) total += l;
+    const size_t need = (size_t)total * sizeof(long long);
+    if (ctx->mc_scratch_bytes < need) {
+        if (ctx->mc_scratch) cudaFree(ctx->mc_scratch);
+        ctx->mc_scratch = nullptr;
+        ctx->mc_scratch_bytes = 0;
+        if (cudaMalloc(&ctx->mc_scratch, need) != cudaSuccess) return GBKB200_ERR_OOM;
+        ctx->mc_scratch_bytes = need;
+    }
+    GBK_CUDA_TRY(cudaMemsetAsync(ctx->mc_scratch, 0, need, ctx->stream));
+    unsigned* bound = static_cast<unsigned*>(ctx->mc_scratch);
+    long long* acc = static_cast<long long*>(ctx->mc_scratch) + 2;
+    long long* ptrs[6];
+    long long off = 0;
+    for (int i = 0; i < 6; ++i) {
+        ptrs[i] = lens[i] ? acc + off : nullptr;
+        off += lens[i];
+    }
+    McFixed f;
+    f.scube = ptrs[0]; f.image = ptrs[1]; f.rdata = ptrs[2]; f.rdata_cmp = ptrs[3];
+    f.ordata = ptrs[4]; f.ordata_cmp = ptrs[5];
+    f.bound = bound;
+    mcdisk_bound_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, bound);
+    mcdisk_fixed_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, f, ctx->d_status);
+    for (int i = 0; i < 6; ++i) {
+        if (!lens[i]) continue;
+        long long g = (lens[i] + 255) / 256;
+        if (g > 148 * 8) g = 148 * 8;
+        fixed_to_float_kernel<<<(int)g, 256, 0, ctx->stream>>>(ptrs[i], outs[i], lens[i], bound,
+                                                             i == 0 ? 0 : 1, nclouds);
+    }
     GBK_CUDA_TRY(cudaGetLastError());
     return gbk_finish(ctx);
 }

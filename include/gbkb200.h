@@ -57,8 +57,14 @@ int gbkb200_ctx_set_stream(gbkb200_ctx* ctx, void* stream);
  * ends every call with cudaDeviceSynchronize); sync = 0: enqueue only */
 int gbkb200_ctx_set_sync(gbkb200_ctx* ctx, int sync);
 /* seed of the counter-based cloud generator of mcdisk_evaluate; mode 0 =
- * fast (atomics, run-to-run order dependent in the last fp32 bit), mode 1 =
- * deterministic (bit-identical run to run) */
+ * fast (fp32 atomics: sums depend on the order clouds land in, in the last
+ * bits), mode 1 = deterministic: the accumulated outputs (scube, image, rdata,
+ * ordata and their _cmp forms) are summed in 64-bit fixed point, bit-identical
+ * run to run and exact to ~2^-(62 - log2 nclouds) of the largest contribution;
+ * it takes an extra bound pass over the clouds and scratch of 8 bytes per
+ * accumulated element held by the context.  The assigned maps (wdata,
+ * vdata_cmp, ddata_cmp) keep the reference's last-writer-wins race in both
+ * modes. */
 int gbkb200_ctx_set_mcdisk(gbkb200_ctx* ctx, unsigned long long seed, int mode);
 /* waits for the context's stream, then returns the status raised by kernels
  * since the last call (GBKB200_OK, _BAD_TRAIT or _TIMEOUT) and clears it */

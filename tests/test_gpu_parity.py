@@ -269,3 +269,44 @@ def test_mcdisk_flux_and_clouds(be, oracle_built):
     diff = np.abs(rd - oh['rdata'])
     assert np.sum(diff > 0.5 * per_cloud) <= 1e-3 * nclouds
     assert rel_err(outs['scube'].cpu().numpy(), oh['scube']) < 1e-2
+
+
+def test_mcdisk_deterministic_mode(be, oracle_built):
+    """Mode 1 (64-bit fixed-point accumulation) gives bit-identical cubes and
+    maps run to run, and agrees with the fast fp32-atomic mode."""
+    import torch
+    from gbkfit_b200 import workloads
+    w = workloads.mcdisk_cube256(nclouds=300_000)
+    w.geom = workloads.Geometry((64, 64, 32), (1, 1, 10), (0, 0, 15.5), (0, 0, 0),
+                                w.geom.psf, w.geom.lsf)
+    w.params = dict(w.params, xpos=32.0, ypos=32.0, bpt_s=8.0)
+    w.disk = workloads.Disk(False, False, np.linspace(0, 40, 21), traits=w.disk.traits)
+    csum = w.disk.ncloudscsum(w.params, 1e-3)
+    hoi = w.disk.hasordint()
+    g = w.geometry_args(spat_z=32)
+    nx, ny, sz = g['spat_size']
+    nz = g['spec_size']
+    pd = upload(w.disk.pack(w.params), 'cuda')
+
+    def run(mode):
+        be['gmodel'].set_mcdisk(seed=7, mode=mode)
+        outs = dict(scube=torch.zeros((nz, ny, nx), device='cuda'),
+                    image=torch.zeros((ny, nx), device='cuda'),
+                    rdata=torch.zeros((sz, ny, nx), device='cuda'))
+        gpu_mcdisk(be['gmodel'], 1e-3, int(csum[-1]), torch.from_numpy(csum).cuda(),
+                   torch.from_numpy(hoi).cuda(), pd, g, outs)
+        return {k: v.cpu().numpy() for k, v in outs.items()}
+
+    a, b, fast = run(1), run(1), run(0)
+    be['gmodel'].set_mcdisk(seed=42, mode=0)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    # every cloud adds cflux / (dx dy) to the maps: the fixed-point sums are
+    # whole cloud counts; the fast mode's fp32 atomics lose ~n eps per element
+    per_cloud = 1e-3 / (g['spat_step'][0] * g['spat_step'][1])
+    for k in ('image', 'rdata'):
+        n = a[k].astype(np.float64) / per_cloud
+        assert np.all(np.abs(n - np.rint(n)) <= 1e-6 * np.maximum(1.0, n)), k
+        assert rel_err(fast[k], a[k]) <= 1e-4, (k, rel_err(fast[k], a[k]))
+    assert rel_err(fast['scube'], a['scube']) <= 1e-5
+    assert abs(a['scube'].sum() - fast['scube'].sum()) <= 1e-5 * abs(a['scube'].sum())
