@@ -216,7 +216,8 @@ class BatchedSMDisk:
 
     def upload(self, packed, bufs, nsets):
         for k, v in packed.items():
-            bufs[k][:nsets].copy_(torch.from_numpy(v), non_blocking=True)
+            if v.size:      # kinds without parameters have no buffer
+                bufs[k][:nsets].copy_(torch.from_numpy(v), non_blocking=True)
 
     # ---- evaluation ---------------------------------------------------------
     def evaluate_device(self, bufs, nsets, chi2=None, model=None):
@@ -252,7 +253,8 @@ class BatchedSMDisk:
                 sub = {k: (v[lo:hi] if per_set[k] else v) for k, v in params.items()}
                 hv, hflat, dflat, dv = st['pieces'][j]
                 for name, arr in self.pack(sub, hi - lo).items():
-                    hv[name][:hi - lo] = arr
+                    if arr.size:
+                        hv[name][:hi - lo] = arr
                 dflat.copy_(hflat, non_blocking=True)
                 self.last_h2d_bytes += hflat.numel() * 4
                 self.evaluate_device(dv, hi - lo, chi2=self.chi2[lo:hi])

@@ -424,6 +424,24 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     const int NW = (P.K + 7 + 3) / 4;
     P.pitch = (P.Wx + 31) / 32 * 32;
     P.nch = (P.Wx + 31) / 32;
+    // the node-wise fast path of the spaxel evaluation: exactly one trait of
+    // uid 101 for rpt, vpt, dpt and none of the other kinds
+    {
+        bool fast = !d->loose && !d->tilted;
+        for (int k = 0; k < 9 && fast; ++k) {
+            const bool want = k == 0 || k == 2 || k == 4;
+            if (!want) {
+                fast = d->ntraits[k] == 0;
+                continue;
+            }
+            int uid = 0;
+            fast = d->ntraits[k] == 1 && d->uids[k] &&
+                   cudaMemcpy(&uid, d->uids[k], sizeof(int), cudaMemcpyDeviceToHost) ==
+                       cudaSuccess &&
+                   uid == 101;
+        }
+        P.nwfast = fast ? 1 : 0;
+    }
     int band = d->psf_band > 0 ? std::min(d->psf_band, P.Ny) : P.Ny;
     P.nbands = (P.Ny + band - 1) / band;
     P.band = (P.Ny + P.nbands - 1) / P.nbands;

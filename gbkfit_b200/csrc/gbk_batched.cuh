@@ -41,6 +41,7 @@ struct BatchKernelArgs {
     const float* lsfr;    // (Kz): LSF reversed
     float* mplanes;       // (chunk, Nz, Wy, pitch): written where xr is not empty
     int nch;              // 32-column chunks per window row, ceil(Wx / 32)
+    int nwfast;           // the disk's traits are exactly rpt/vpt/dpt uid 101 (smdisk_spaxel_nw)
     int* xr;              // (chunk, Wy, nch, Nz): nonzero x range (xmin | xmax << 16) of
                           // each plane row chunk (4-aligned around it is written), or -1
     int* xrt;             // (chunk, Nz, Wy, nch): the same, plane-major (read by the PSF kernel)
@@ -88,7 +89,7 @@ constexpr int KA_THREADS = 128;        // 4 independent (row, chunk) warps per b
 // taps per output), each output plane row chunk stored as one coalesced
 // 128-byte segment.  Per plane the chunk's nonzero x range is stored.
 template<int KZ>
-__global__ void __launch_bounds__(KA_THREADS, 4) ka_lines_lsf(BatchKernelArgs P, int* status)
+__global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(BatchKernelArgs P, int* status)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int item = blockIdx.x * (KA_THREADS / 32) + warp;
@@ -102,8 +103,9 @@ __global__ void __launch_bounds__(KA_THREADS, 4) ka_lines_lsf(BatchKernelArgs P,
     SpaxelOut o{};
     int lo = INT_MAX, hi = -1;
     float amp = 0.f, rinv = 0.f;
-    if (x < P.Wx && smdisk_spaxel(a, kc, x, y, 0, o, bad) &&
-        line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo, hi)) {
+    const bool on = x < P.Wx && (P.nwfast ? smdisk_spaxel_nw(a, kc, x, y, o)
+                                           : smdisk_spaxel(a, kc, x, y, 0, o, bad));
+    if (on && line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo, hi)) {
         amp = o.orv * (1 / (o.dv * sqrtf(2 * GBK_PI)));
         rinv = 1 / (2 * o.dv * o.dv);
     } else {
@@ -117,8 +119,8 @@ __global__ void __launch_bounds__(KA_THREADS, 4) ka_lines_lsf(BatchKernelArgs P,
         return (z >= lo && z <= hi) ? amp * expf(-(d * d) * rinv) : 0.f;
     };
     // the lane's and the warp's output channel ranges
-    const bool on = lo <= hi;
-    const int olo = on ? max(0, lo - KZ + 1) : INT_MAX, ohi = on ? min(P.Nz - 1, hi) : -1;
+    const bool lit = lo <= hi;
+    const int olo = lit ? max(0, lo - KZ + 1) : INT_MAX, ohi = lit ? min(P.Nz - 1, hi) : -1;
     int zlo = olo, zhi = ohi;
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) {
@@ -225,14 +227,25 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
     // bounding box of the nonzero input row chunks
     {
         int y0 = INT_MAX, y1 = -1, x0 = INT_MAX, x1 = -1;
-        for (int i = ob0 * P.nch + threadIdx.x; i < in1 * P.nch; i += KB_THREADS) {
-            const int v = xr[i];
-            if (v >= 0) {
-                const int y = i / P.nch;
-                y0 = min(y0, y);
-                y1 = max(y1, y);
-                x0 = min(x0, v & 0xffff);
-                x1 = max(x1, v >> 16);
+        // the entries of rows [ob0, in1), eight loads in flight per thread
+        const int* src = xr + ob0 * P.nch;
+        const int n = (in1 - ob0) * P.nch;
+        for (int i0 = 0; i0 < n; i0 += 8 * KB_THREADS) {
+            int v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int i = i0 + u * KB_THREADS + threadIdx.x;
+                v[u] = i < n ? src[i] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (v[u] >= 0) {
+                    const int y = ob0 + (i0 + u * KB_THREADS + (int)threadIdx.x) / P.nch;
+                    y0 = min(y0, y);
+                    y1 = max(y1, y);
+                    x0 = min(x0, v[u] & 0xffff);
+                    x1 = max(x1, v[u] >> 16);
+                }
             }
         }
 #pragma unroll

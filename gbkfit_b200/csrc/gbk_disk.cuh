@@ -120,6 +120,42 @@ static __device__ bool smdisk_spaxel(const DiskArgs& a, const DiskConst& kc, int
     return true;
 }
 
+// smdisk_spaxel for a flat thin disk whose only traits are one node-wise
+// density (rpt uid 101), one node-wise rotation curve (vpt uid 101) and one
+// node-wise dispersion (dpt uid 101), without opacity: the same fp32
+// operations in the same order as the generic path (gmodels.hpp:645-914,
+// traits.hpp:138-141, 999-1007), without the trait dispatch.
+__device__ __forceinline__ bool smdisk_spaxel_nw(const DiskArgs& a, const DiskConst& kc, int x,
+                                                 int y, SpaxelOut& o)
+{
+    float xn = a.zx + x * a.stx, yn = a.zy + y * a.sty;
+    xn -= a.xpos[0];
+    yn -= a.ypos[0];
+    rot_lh_z(xn, yn, kc.sin_pa, kc.cos_pa);
+    yn /= kc.cos_in;
+    const float theta = atan2f(yn, xn);
+    const float r = sqrtf(xn * xn + yn * yn);
+    int k;
+    if (!disk_info(k, r, a.nrnodes, a.rnodes)) return false;
+    float rv = 0;
+    rv += lerp(r, k, a.rnodes, a.rpt.pv, 0) * 1.f;
+    if (!rv) return false;
+    rv /= cosf(kc.incli);
+    const float mtan = cosf(theta) * sinf(kc.incli);
+    const float vt = r == 0 ? 0.f : lerp(r, k, a.rnodes, a.vpt.pv, 0) * mtan;
+    float vv = 0;
+    vv += vt * 1.f;
+    vv += a.vsys ? a.vsys[0] : 0.f;
+    float dv = 0;
+    dv += lerp(r, k, a.rnodes, a.dpt.pv, 0) * 1.f;
+    o.rv = rv;
+    o.vv = vv;
+    o.dv = fabsf(dv);
+    o.wv = 1;
+    o.orv = rv;
+    return true;
+}
+
 // gmodels.hpp:930-957: the non-spectral outputs of an smdisk spaxel
 __device__ __forceinline__ void smdisk_side_outputs(const DiskArgs& a, int x, int y, int z,
                                                     const SpaxelOut& o)

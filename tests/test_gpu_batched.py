@@ -162,3 +162,29 @@ def test_batched_direct_empty_planes(gpu, oracle_built):
         c_ref = chi2(ref, data, err)
         assert abs(got[i] - c_ref) / c_ref < 1e-4, (i, got[i], c_ref)
     assert abs(got[1] - chi2(0 * data, data, err)) / got[1] < 1e-6
+
+
+def test_batched_nodewise_fast_path_matches_generic(gpu):
+    """The node-wise spaxel fast path (rpt/vpt/dpt uid 101 only) gives the
+    same bits as the generic trait dispatch: a weight trait (which does not
+    touch the cube) forces the generic path on an otherwise identical disk."""
+    import torch
+    from gbkfit_b200 import traits
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    from gbkfit_b200.disk import Disk
+    w = _small_batch_workload(4)
+    data, err, _ = synthetic_data(w)
+    d2 = Disk(False, False, w.disk.rnodes, traits=dict(
+        rpt=w.disk.traits['rpt'], vpt=w.disk.traits['vpt'], dpt=w.disk.traits['dpt'],
+        wpt=[traits.wpt_axis_range(0, 30.0, 0.5)]))
+    out = []
+    for disk in (w.disk, d2):
+        ev = BatchedSMDisk(disk, w.geom, data, err, max_sets=4, conv='direct')
+        bufs = ev.alloc_inputs(4)
+        ev.upload(ev.pack(w.params, 4), bufs, 4)
+        model = torch.zeros((4,) + tuple(w.geom.size[::-1]), device='cuda')
+        c = ev.evaluate_device(bufs, 4, model=model).cpu().numpy().copy()
+        out.append((c, model.cpu().numpy(), ev.evaluate(w.params, 4)))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2]) and np.array_equal(out[0][0], out[0][2])
