@@ -353,7 +353,7 @@ struct gbkb200_batch {
     int nper = 0;
     int direct = 0;
     size_t smemB = 0;
-    float *vr = nullptr, *ur = nullptr, *lsfr = nullptr, *mplanes = nullptr;
+    float* mplanes = nullptr;
     int* xr = nullptr;
     int* xrt = nullptr;
     double* sat = nullptr;
@@ -461,22 +461,18 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     for (int t = 0; t < P.Ky; ++t) ur[t] = (float)d->psf_u[P.Ky - 1 - t];
     for (int t = 0; t < P.Kz; ++t) lr[t] = (float)d->lsf[P.Kz - 1 - t];
     const size_t nrows = (size_t)bt->chunk * P.Nz * P.Wy;
-    if (cudaMalloc(&bt->vr, vr.size() * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&bt->ur, ur.size() * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&bt->lsfr, lr.size() * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&bt->mplanes, nrows * P.pitch * sizeof(float)) != cudaSuccess ||
+    for (int i = 0; i < 33; ++i) {
+        P.vr[i] = i < P.K ? vr[i] : 0.f;
+        P.ur[i] = i < P.K ? ur[i] : 0.f;
+        P.lsfr[i] = i < P.Kz ? lr[i] : 0.f;
+    }
+    if (cudaMalloc(&bt->mplanes, nrows * P.pitch * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&bt->xr, nrows * P.nch * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&bt->xrt, nrows * P.nch * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&bt->sat, (size_t)P.Nz * (P.Ny + 1) * (P.Nx + 1) * sizeof(double)) !=
             cudaSuccess ||
         cudaMalloc(&bt->iw, (size_t)P.Nz * P.Ny * P.Nx * sizeof(float)) != cudaSuccess)
         return GBKB200_ERR_OOM;
-    GBK_CUDA_TRY(cudaMemcpy(bt->vr, vr.data(), vr.size() * sizeof(float), cudaMemcpyHostToDevice));
-    GBK_CUDA_TRY(cudaMemcpy(bt->ur, ur.data(), ur.size() * sizeof(float), cudaMemcpyHostToDevice));
-    GBK_CUDA_TRY(cudaMemcpy(bt->lsfr, lr.data(), lr.size() * sizeof(float), cudaMemcpyHostToDevice));
-    P.vr = bt->vr;
-    P.ur = bt->ur;
-    P.lsfr = bt->lsfr;
     P.mplanes = bt->mplanes;
     P.xr = bt->xr;
     P.xrt = bt->xrt;
@@ -546,9 +542,6 @@ extern "C" int gbkb200_batch_destroy(gbkb200_batch* bt)
     cudaFree(bt->kspec);
     cudaFree(bt->work);
     cudaFree(bt->partials);
-    cudaFree(bt->vr);
-    cudaFree(bt->ur);
-    cudaFree(bt->lsfr);
     cudaFree(bt->mplanes);
     cudaFree(bt->xr);
     cudaFree(bt->xrt);
@@ -776,7 +769,7 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
             }
             stage_mark(bt, 1, false);
             stage_mark(bt, 4, true);
-            bt->kb<<<dim3(P.Nz * P.nbands, cn), KB_THREADS, bt->smemB, st>>>(P);
+            bt->kb<<<dim3(cn, P.Nz * P.nbands), KB_THREADS, bt->smemB, st>>>(P);
             stage_mark(bt, 4, false);
         }
         stage_mark(bt, 5, true);

@@ -36,9 +36,10 @@ struct BatchKernelArgs {
     int pitch;            // row pitch of the LSF-convolved planes in HBM (floats, % 32 == 0)
     int cap;              // shared-memory floats of a PSF block (rows of one pass)
     int band, nbands;     // output rows per PSF block, bands per plane
-    const float* vr;      // (K): PSF x factor, reversed
-    const float* ur;      // (K): PSF y factor, reversed
-    const float* lsfr;    // (Kz): LSF reversed
+    // FIR coefficients in the parameter block (constant bank, uniform loads)
+    float vr[33];         // (K): PSF x factor, reversed, zero-padded
+    float ur[33];         // (K): PSF y factor, reversed, zero-padded
+    float lsfr[33];       // (Kz): LSF reversed
     float* mplanes;       // (chunk, Nz, Wy, pitch): written where xr is not empty
     int nch;              // 32-column chunks per window row, ceil(Wx / 32)
     int nwfast;           // the disk's traits are exactly rpt/vpt/dpt uid 101 (smdisk_spaxel_nw)
@@ -186,7 +187,7 @@ __device__ __forceinline__ double sat_box(const double* T, int ld, int y0, int y
            T[(long long)y0 * ld + x0];
 }
 
-// KB: one block per (set, output plane zo, band of output rows).  The block
+// KB: one block per (set, output plane zo, band of output rows), sets fastest.  The block
 // finds the bounding box of the band's nonzero input row chunks and works
 // through its output rows in passes whose input rows fit the block's shared
 // memory (box-relative row pitch; usually one pass):
@@ -211,8 +212,9 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
     float* S = reinterpret_cast<float*>(sm4);                   // (rows of a pass, bp)
     __shared__ float warp_part[NWARPS];
     __shared__ int s_box[4];
-    const int zo = blockIdx.x / P.nbands, band = blockIdx.x % P.nbands;
-    const int c = blockIdx.y, b = P.set0 + c;
+    // sets vary fastest: the blocks in flight share a few planes of the data
+    const int zo = blockIdx.y / P.nbands, band = blockIdx.y % P.nbands;
+    const int c = blockIdx.x, b = P.set0 + c;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ob0 = band * P.band, ob1 = min(P.Ny, ob0 + P.band);  // output rows [ob0, ob1)
     const int in1 = min(P.Wy, ob1 + K - 1);                        // input rows [ob0, in1)
@@ -338,7 +340,7 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
             float vr[K];
 #pragma unroll
             for (int s = 0; s < K; ++s) vr[s] = P.vr[s];
-            const int rw = ns8 <= 8 ? 4 : (ns8 <= 16 ? 2 : 1);
+            const int rw = ns8 >= 32 ? 1 : 32 / ns8;     // rows per warp
             const int spw = 32 / rw;                    // strips per warp pass
             const int r = lane % rw, sidx = lane / rw;
             for (int ry = ly0 + warp * rw; ry <= ly1; ry += NWARPS * rw) {
@@ -346,7 +348,7 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
                 float4* row = reinterpret_cast<float4*>(S + (long long)(y - ys) * bp);
                 for (int gs = 0; gs < ns8; gs += spw) {
                     const int gi = gs + sidx;           // strip, box-relative
-                    const bool act = gi < ns8 && y <= ly1;
+                    const bool act = sidx < spw && gi < ns8 && y <= ly1;
                     float w[4 * NW];
                     if (act) {
 #pragma unroll
@@ -378,7 +380,9 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
             float ur[K];
 #pragma unroll
             for (int t = 0; t < K; ++t) ur[t] = P.ur[t];
-            const int gpr = max(1, KB_THREADS * KB_IT / ns4);   // row groups per round
+            const int gmax = max(1, KB_THREADS * KB_IT / ns4);  // row groups per round at most
+            const int rounds = (ng + gmax - 1) / gmax;
+            const int gpr = (ng + rounds - 1) / rounds;         // balanced rounds
             for (int gr0 = 0; gr0 < ng; gr0 += gpr) {
                 const int nitems = min(gpr, ng - gr0) * ns4;
                 float acc[KB_IT][8][4];
@@ -487,6 +491,7 @@ typedef void (*KaFn)(BatchKernelArgs, int*);
 typedef void (*KbFn)(BatchKernelArgs);
 constexpr int KA_KMAX = 33;                 // longest LSF of the direct path
 constexpr int KB_KMIN = 5, KB_KMAX = 33;    // PSF FIR lengths (odd)
+static_assert(KA_KMAX <= 33 && KB_KMAX <= 33, "coefficient arrays of BatchKernelArgs");
 // fill t[Kz / 2] (model kernel) and t[(K - KB_KMIN) / 2] (PSF kernel)
 void ka_register_short(KaFn* t);
 void ka_register_long(KaFn* t);
