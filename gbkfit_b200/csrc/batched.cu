@@ -450,12 +450,13 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     // otherwise 54 KB (four blocks per SM)
     int bpmax = 4 * (2 * ((P.Nx + 7) / 8 - 1) + NW);
     bpmax += ((4 - bpmax % 32) + 32) % 32;
+    const long long xr_bytes = (long long)(P.band + P.K - 1) * P.nch * sizeof(int);
     const long long need_min = (long long)(P.K + 15) * bpmax;
     const long long need_all = (long long)(P.band + P.K + 7) * bpmax;
-    const long long cap = std::max(need_min, std::min(need_all, 54LL * 1024 / 4));
-    if (cap * (long long)sizeof(float) > 227LL * 1024) return GBKB200_ERR_UNSUPPORTED;
+    const long long cap = std::max(need_min, std::min(need_all, (55LL * 1024 - xr_bytes) / 4));
+    if (cap * (long long)sizeof(float) + xr_bytes > 227LL * 1024) return GBKB200_ERR_UNSUPPORTED;
     P.cap = (int)cap;
-    bt->smemB = (size_t)cap * sizeof(float);
+    bt->smemB = (size_t)cap * sizeof(float) + (size_t)xr_bytes;
     std::vector<float> vr(P.K, 0.f), ur(P.K, 0.f), lr(P.Kz);
     for (int s = 0; s < P.Kx; ++s) vr[s] = (float)d->psf_v[P.Kx - 1 - s];
     for (int t = 0; t < P.Ky; ++t) ur[t] = (float)d->psf_u[P.Ky - 1 - t];

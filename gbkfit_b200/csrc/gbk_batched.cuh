@@ -210,6 +210,7 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
     constexpr int NWARPS = KB_THREADS / 32;
     extern __shared__ float4 sm4[];
     float* S = reinterpret_cast<float*>(sm4);                   // (rows of a pass, bp)
+    int* s_xr = reinterpret_cast<int*>(S + P.cap);              // (in1 - ob0, nch) entries
     __shared__ float warp_part[NWARPS];
     __shared__ int s_box[4];
     // sets vary fastest: the blocks in flight share a few planes of the data
@@ -238,6 +239,7 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
             for (int u = 0; u < 8; ++u) {
                 const int i = i0 + u * KB_THREADS + threadIdx.x;
                 v[u] = i < n ? src[i] : -1;
+                if (i < n) s_xr[i] = v[u];
             }
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
@@ -306,7 +308,7 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
             const int ti = threadIdx.x % tc, ty = threadIdx.x / tc;
             if (ty < tr) {
                 for (int y = ly0 + ty; y <= ly1; y += tr) {
-                    const int* vrow = xr + y * P.nch;
+                    const int* vrow = s_xr + (y - ob0) * P.nch;
                     float4* d = reinterpret_cast<float4*>(S + (long long)(y - ys) * bp);
                     const float4* g = src + (long long)y * (P.pitch / 4);
                     for (int j = ti; j < nsl; j += tc) {
