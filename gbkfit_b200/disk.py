@@ -40,6 +40,29 @@ def default_rstep(rnodes):
     return min(1.0, float(np.min(np.diff(np.asarray(rnodes, dtype=np.float64)))) / 2)
 
 
+_LINEAR_CACHE = {}
+
+
+def _linear_matrix(x, xnew):
+    """(n, m) matrix W of linear interpolation from nodes x to points xnew
+    (y_new = y @ W, clamped at the ends like numpy.interp); cached, since a
+    disk's nodes and sub-nodes do not change."""
+    key = (np.asarray(x, np.float64).tobytes(), np.asarray(xnew, np.float64).tobytes())
+    hit = _LINEAR_CACHE.get(key)
+    if hit is None:
+        idx = np.clip(np.searchsorted(x, xnew, side='right') - 1, 0, len(x) - 2)
+        x0, x1 = x[idx], x[idx + 1]
+        t = np.clip((xnew - x0) / (x1 - x0), 0.0, 1.0)
+        hit = np.zeros((len(x), len(xnew)))
+        cols = np.arange(len(xnew))
+        np.add.at(hit, (idx, cols), 1.0 - t)
+        np.add.at(hit, (idx + 1, cols), t)
+        if len(_LINEAR_CACHE) > 256:
+            _LINEAR_CACHE.clear()
+        _LINEAR_CACHE[key] = hit
+    return hit
+
+
 def _interp(kind, x, y, xnew):
     """Node -> sub-node interpolation (math/interpolation.py:16-50)."""
     y = np.asarray(y, dtype=np.float64)
@@ -47,10 +70,7 @@ def _interp(kind, x, y, xnew):
         if y.ndim == 1:
             return np.interp(xnew, x, y)
         # batched: y (B, n)
-        idx = np.clip(np.searchsorted(x, xnew, side='right') - 1, 0, len(x) - 2)
-        x0, x1 = x[idx], x[idx + 1]
-        t = np.clip((xnew - x0) / (x1 - x0), 0.0, 1.0)
-        return y[..., idx] + t * (y[..., idx + 1] - y[..., idx])
+        return y @ _linear_matrix(x, xnew)
     if kind == 'akima':
         return scipy.interpolate.Akima1DInterpolator(x, y, axis=-1)(xnew)
     if kind == 'pchip':
