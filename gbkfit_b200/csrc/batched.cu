@@ -414,10 +414,34 @@ static KbFn kb_fn(int K)
 static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
 {
     BatchKernelArgs& P = bt->P;
-    P.Kx = d->kernel_size[0];
-    P.Ky = d->kernel_size[1];
-    P.Kz = d->kernel_size[2];
     if (d->psf_rank != 1 || !d->psf_u || !d->psf_v) return GBKB200_ERR_UNSUPPORTED;
+    // Taps below 2^-35 of their factor's largest are dropped from both ends
+    // (symmetrically, the centre stays): they change no output by more than
+    // ~1e-10 of its peak, below fp32 resolution.  The evaluation window then
+    // starts t taps later along each axis and is 2 t shorter, so every kept
+    // tap meets the same model voxel as before.
+    auto trim = [](const double* a, int n) {
+        double m = 0;
+        for (int i = 0; i < n; ++i) m = std::max(m, std::fabs(a[i]));
+        const double thr = std::ldexp(m, -35);
+        int t = 0;
+        while (2 * t + 1 < n && std::fabs(a[t]) < thr && std::fabs(a[n - 1 - t]) < thr) ++t;
+        return t;
+    };
+    const int tx = trim(d->psf_v, d->kernel_size[0]), ty = trim(d->psf_u, d->kernel_size[1]);
+    const int tz = trim(d->lsf, d->kernel_size[2]);
+    P.Kx = d->kernel_size[0] - 2 * tx;
+    P.Ky = d->kernel_size[1] - 2 * ty;
+    P.Kz = d->kernel_size[2] - 2 * tz;
+    P.Wx = P.Nx + P.Kx - 1;
+    P.Wy = P.Ny + P.Ky - 1;
+    P.Wz = P.Nz + P.Kz - 1;
+    P.disk.sx = P.Wx;
+    P.disk.sy = P.Wy;
+    P.disk.spec_size = P.Wz;
+    P.disk.zx = d->spat_zero[0] + tx * d->spat_step[0];
+    P.disk.zy = d->spat_zero[1] + ty * d->spat_step[1];
+    P.disk.spec_zero = d->spec_zero + tz * d->spec_step;
     P.K = std::max(KB_KMIN, std::max(P.Kx, P.Ky) | 1);
     if (P.K > KB_KMAX || P.Kz > KA_KMAX || P.Nx > 4 * KB_THREADS * KB_IT || P.Wx > 1024)
         return GBKB200_ERR_UNSUPPORTED;
@@ -458,9 +482,9 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.cap = (int)cap;
     bt->smemB = (size_t)cap * sizeof(float) + (size_t)xr_bytes;
     std::vector<float> vr(P.K, 0.f), ur(P.K, 0.f), lr(P.Kz);
-    for (int s = 0; s < P.Kx; ++s) vr[s] = (float)d->psf_v[P.Kx - 1 - s];
-    for (int t = 0; t < P.Ky; ++t) ur[t] = (float)d->psf_u[P.Ky - 1 - t];
-    for (int t = 0; t < P.Kz; ++t) lr[t] = (float)d->lsf[P.Kz - 1 - t];
+    for (int s = 0; s < P.Kx; ++s) vr[s] = (float)d->psf_v[d->kernel_size[0] - 1 - tx - s];
+    for (int t = 0; t < P.Ky; ++t) ur[t] = (float)d->psf_u[d->kernel_size[1] - 1 - ty - t];
+    for (int t = 0; t < P.Kz; ++t) lr[t] = (float)d->lsf[d->kernel_size[2] - 1 - tz - t];
     const size_t nrows = (size_t)bt->chunk * P.Nz * P.Wy;
     for (int i = 0; i < 33; ++i) {
         P.vr[i] = i < P.K ? vr[i] : 0.f;
@@ -621,7 +645,9 @@ extern "C" int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* 
     P.scale = 1.0f / (float)((long long)P.Px * P.Py * P.Pz);
     // direct separable convolution when requested or (automatic) when it applies
     if (d->conv_mode != 1) {
+        const BatchKernelArgs saved = P;     // the direct set-up trims the window
         rc = setup_direct(bt, d);
+        if (rc != GBKB200_OK) P = saved;
         if (rc == GBKB200_OK) {
             GBK_CUDA_TRY(cudaGetLastError());
             *out = bt;
