@@ -141,26 +141,29 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
         for (int t = 0; t < KZ - 1; ++t) w[t] = line(zlo + t);
         float* dst = P.mplanes + ((long long)c * P.Nz * P.Wy + y) * P.pitch + x;
         const long long zstride = (long long)P.Wy * P.pitch;
-        int mlo = 0, mhi = -1, mz = zlo;     // range of the 32 planes zo in [mz, mz + 32)
+        unsigned mm = 0u;
+        int mz = zlo;     // lane (zo - mz) keeps the ballot of plane zo, flushed every 32 planes
         for (int zb = zlo; zb <= zhi; zb += KZ) {
 #pragma unroll
             for (int k = 0; k < KZ; ++k) {
                 const int zo = zb + k;
                 if (zo > zhi) break;
                 w[(k + KZ - 1) % KZ] = line(zo + KZ - 1);
-                float acc = 0.f;
+                // two independent accumulation chains (even and odd taps)
+                float acc0 = 0.f, acc1 = 0.f;
 #pragma unroll
-                for (int t = 0; t < KZ; ++t) acc += lz[t] * w[(k + t) % KZ];
-                dst[zo * zstride] = acc;
+                for (int t = 0; t < KZ; t += 2) acc0 += lz[t] * w[(k + t) % KZ];
+#pragma unroll
+                for (int t = 1; t < KZ; t += 2) acc1 += lz[t] * w[(k + t) % KZ];
+                dst[zo * zstride] = acc0 + acc1;
                 const unsigned m = __ballot_sync(0xffffffffu, zo >= olo && zo <= ohi);
-                // lane (zo - mz) keeps plane zo's range; flushed every 32 planes
-                if (lane == zo - mz) {
-                    mlo = m ? chunk * 32 + __ffs(m) - 1 : 0;
-                    mhi = m ? chunk * 32 + 31 - __clz(m) : -1;
-                }
+                if (lane == zo - mz) mm = m;
                 if (zo - mz == 31 || zo == zhi) {
                     const int zz = mz + lane;
-                    if (zz <= zo) xr[zz] = mhi >= 0 ? (mlo | (mhi << 16)) : -1;
+                    if (zz <= zo)
+                        xr[zz] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
+                                       ((chunk * 32 + 31 - __clz(mm)) << 16))
+                                    : -1;
                     mz = zo + 1;
                 }
             }
