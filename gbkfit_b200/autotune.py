@@ -100,7 +100,7 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
     t_end = time.time() + budget_s
     # direct separable convolution (when the PSF is rank 1): chunk, then band
     best_d, best_dt = None, float('inf')
-    for chunk in (16, 32, 64, 128, 256):
+    for chunk in (32, 64, 128, 256, 512):
         cfg = dict(fft_size=(0, 0, 0), chunk=chunk, rows_k1=16, conv='direct', band=0)
         t = time_config(w, data, err, nsets, cfg)
         if t < best_dt:

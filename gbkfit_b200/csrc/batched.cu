@@ -443,7 +443,8 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.disk.zy = d->spat_zero[1] + ty * d->spat_step[1];
     P.disk.spec_zero = d->spec_zero + tz * d->spec_step;
     P.K = std::max(KB_KMIN, std::max(P.Kx, P.Ky) | 1);
-    if (P.K > KB_KMAX || P.Kz > KA_KMAX || P.Nx > 4 * KB_THREADS * KB_IT || P.Wx > 1024)
+    if (P.K > KB_KMAX || P.Kz > KA_KMAX || P.Nx > 4 * KB_THREADS * KB_IT || P.Wx > 1024 ||
+        (long long)P.Nx * P.Ny * P.Nz >= (1LL << 31))
         return GBKB200_ERR_UNSUPPORTED;
     const int NW = (P.K + 7 + 3) / 4;
     P.pitch = (P.Wx + 31) / 32 * 32;

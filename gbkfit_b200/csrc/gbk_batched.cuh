@@ -296,9 +296,10 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
     const int nsl = 2 * (ns8 - 1) + NW;
     int bp = 4 * nsl;
     bp += ((4 - bp % 32) + 32) % 32;
+    const int bp4 = bp / 4;
     const int bo = ((P.cap / bp - (K + 7)) / 8) * 8;        // output rows per pass (>= 8)
     const float4* src = reinterpret_cast<const float4*>(P.mplanes + prow * P.pitch);
-    const long long pbase = (long long)zo * plane;
+    const int pbase = zo * P.Ny * P.Nx;       // the data cube has < 2^31 voxels
     float sum = 0.f;
     for (int ys = yo_lo; ys < yb_end; ys += bo) {
         const int ye = min(yb_end, ys + bo);                 // outputs [ys, ye)
@@ -312,7 +313,7 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
             if (ty < tr) {
                 for (int y = ly0 + ty; y <= ly1; y += tr) {
                     const int* vrow = s_xr + (y - ob0) * P.nch;
-                    float4* d = reinterpret_cast<float4*>(S + (long long)(y - ys) * bp);
+                    float4* d = reinterpret_cast<float4*>(S) + (y - ys) * bp4;
                     const float4* g = src + (long long)y * (P.pitch / 4);
                     for (int j = ti; j < nsl; j += tc) {
                         const int sl = sl0 + j, ch = sl >> 3;
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
             if (ty < tr) {
                 for (int y = ys + ty; y < rend; y += tr) {
                     if (y >= ly0 && y <= ly1) continue;
-                    float4* d = reinterpret_cast<float4*>(S + (long long)(y - ys) * bp);
+                    float4* d = reinterpret_cast<float4*>(S) + (y - ys) * bp4;
                     for (int j = ti; j < ns4; j += tc) d[j] = make_float4(0.f, 0.f, 0.f, 0.f);
                 }
             }
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
             const int r = lane % rw, sidx = lane / rw;
             for (int ry = ly0 + warp * rw; ry <= ly1; ry += NWARPS * rw) {
                 const int y = ry + r;
-                float4* row = reinterpret_cast<float4*>(S + (long long)(y - ys) * bp);
+                float4* row = reinterpret_cast<float4*>(S) + (y - ys) * bp4;
                 for (int gs = 0; gs < ns8; gs += spw) {
                     const int gi = gs + sidx;           // strip, box-relative
                     const bool act = sidx < spw && gi < ns8 && y <= ly1;
@@ -400,10 +401,10 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
                         for (int k = 0; k < 4; ++k) acc[it][q][k] = 0.f;
                     if (item < nitems) {
                         const int rb = 8 * (gr0 + item / ns4), s4 = item % ns4;
+                        const float4* colp = reinterpret_cast<const float4*>(S) + rb * bp4 + s4;
 #pragma unroll
                         for (int m = 0; m < K + 7; ++m) {
-                            const float4 p =
-                                reinterpret_cast<const float4*>(S + (long long)(rb + m) * bp)[s4];
+                            const float4 p = colp[m * bp4];
 #pragma unroll
                             for (int q = 0; q < 8; ++q) {
                                 const int t = m - q;
@@ -426,7 +427,7 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
 #pragma unroll
                         for (int q = 0; q < 8; ++q)
                             if (ys + rb + q < ye)
-                                reinterpret_cast<float4*>(S + (long long)(rb + q) * bp)[s4] =
+                                reinterpret_cast<float4*>(S)[(rb + q) * bp4 + s4] =
                                     make_float4(acc[it][q][0], acc[it][q][1], acc[it][q][2],
                                                 acc[it][q][3]);
                     }
@@ -444,14 +445,14 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
 #pragma unroll 4
             for (int i = threadIdx.x; i < n; i += KB_THREADS) {
                 const int yo = ys + row, xo = xb0 + 4 * col;
-                const float4 m = *reinterpret_cast<const float4*>(S + (long long)row * bp + 4 * col);
-                const long long vi = pbase + (long long)yo * P.Nx + xo;
+                const float4 m = reinterpret_cast<const float4*>(S)[row * bp4 + col];
+                const int vi = pbase + yo * P.Nx + xo;
                 const float4 o = *reinterpret_cast<const float4*>(P.obs + vi);
                 const float4 w = *reinterpret_cast<const float4*>(P.iw + vi);
                 const float r0 = (m.x - o.x) * w.x, r1 = (m.y - o.y) * w.y;
                 const float r2 = (m.z - o.z) * w.z, r3 = (m.w - o.w) * w.w;
                 sum += r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3;
-                if (model) *reinterpret_cast<float4*>(model + (long long)yo * P.Nx + xo) = m;
+                if (model) *reinterpret_cast<float4*>(model + yo * P.Nx + xo) = m;
                 row += dq;
                 col += dr;
                 if (col >= nv) {
@@ -464,11 +465,11 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
             for (int i = threadIdx.x; i < n; i += KB_THREADS) {
                 const int row = i / nw, col = i % nw;
                 const int yo = ys + row, xo = xb0 + col;
-                const float m = S[(long long)row * bp + col];
-                const long long vi = pbase + (long long)yo * P.Nx + xo;
+                const float m = S[row * bp + col];
+                const int vi = pbase + yo * P.Nx + xo;
                 const float r0 = (m - P.obs[vi]) * P.iw[vi];
                 sum += r0 * r0;
-                if (model) model[(long long)yo * P.Nx + xo] = m;
+                if (model) model[yo * P.Nx + xo] = m;
             }
         }
         __syncthreads();    // S is reloaded by the next pass
