@@ -66,7 +66,7 @@ def direct_flops_per_eval(geom):
 # DRAM bytes (read + write) per evaluation of the direct-mode kernels
 # (ka_lines_lsf + k_xr_transpose + kb_psf_residual), from the ncu capture in
 # profiles/kernels_smdisk_batch128_direct.md (one 128-set launch each, / 128)
-DIRECT_TRAFFIC_PER_EVAL = 4.47e6
+DIRECT_TRAFFIC_PER_EVAL = 4.2e6
 
 
 class ClockSampler:
