@@ -66,6 +66,29 @@ DISK_ARGS += [(n, c_void_p) for n in ('image', 'scube', 'wdata', 'wdata_cmp', 'r
                                       'ddata_cmp')]
 DISK_TYPES = [t for _, t in DISK_ARGS]
 
+c_ll = ctypes.c_longlong
+
+
+class ServeArgs(ctypes.Structure):
+    """gbkb200_serve_args (include/gbkb200.h): one serving request; the
+    parameter arrays are byte offsets into the request's blob (-1 = absent)."""
+    _fields_ = [('kind', c_int), ('cflux', c_float), ('nclouds', c_int), ('loose', c_int),
+                ('tilted', c_int), ('blob_dev', c_void_p), ('blob_host', c_void_p),
+                ('blob_bytes', c_ll), ('off_rnodes', c_ll), ('nrnodes', c_int),
+                ('off_vsys', c_ll), ('off_xpos', c_ll), ('off_ypos', c_ll), ('off_posa', c_ll),
+                ('off_incl', c_ll), ('ntraits', c_int * 9), ('off_uids', c_ll * 9),
+                ('off_cvalues', c_ll * 9), ('off_ccounts', c_ll * 9),
+                ('off_pvalues', c_ll * 9), ('off_pcounts', c_ll * 9), ('off_csum', c_ll),
+                ('csum_len', c_int), ('off_hasordint', c_ll), ('spat_size', c_int * 3),
+                ('spat_step', c_float * 3), ('spat_zero', c_float * 3), ('spec_size', c_int),
+                ('spec_step', c_float), ('spec_zero', c_float), ('size_hi', c_int * 3),
+                ('edge', c_int * 3), ('size', c_int * 3), ('scube', c_void_p),
+                ('work', c_void_p), ('spectrum', c_void_p), ('crop', c_void_p),
+                ('res', c_void_p), ('obs', c_void_p), ('err', c_void_p), ('msk', c_void_p),
+                ('weight', c_float), ('chi2_dev', c_void_p), ('chi2_host', c_void_p),
+                ('status_host', c_void_p)]
+
+
 _SIGS = {
     'gbkb200_ctx_create': [ctypes.POINTER(c_void_p), c_int],
     'gbkb200_ctx_destroy': [c_void_p],
@@ -93,6 +116,7 @@ _SIGS = {
     'gbkb200_objective_residual_f32': [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                        c_void_p, c_void_p, c_int, c_float, c_void_p],
     'gbkb200_objective_residual_sum_f32': [c_void_p, c_void_p, c_int, c_int, c_void_p],
+    'gbkb200_serve_scube_chi2_f32': [c_void_p, ctypes.POINTER(ServeArgs)],
 }
 
 EXPORTED = sorted(_SIGS) + ['gbkb200_error_string', 'gbkb200_last_cuda_error']

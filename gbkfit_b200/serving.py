@@ -16,11 +16,14 @@ optionally, its model cube).
   order, as soon as a slot is free and the in-flight HBM footprint plus its
   own fits the budget; completions are polled through CUDA events and the
   freed slot and memory are given to the next request at once.
-* Per request (all enqueued on its slot's stream): smdisk or mcdisk on the
-  padded grid (gmodels.hpp), the FFT convolution with the dataset's spectrum,
-  the crop (dmodels.hpp:7-46), the residual and its sum of squares
-  (objective.hpp:7-31, host/kernels.hpp:502-514), chi^2 copied to pinned host
-  memory.
+* Per request, one native call (gbkb200_serve_scube_chi2_f32) enqueues on
+  its slot's stream: the copy of the packed parameters from pinned memory,
+  smdisk or mcdisk on the padded grid (gmodels.hpp), the FFT convolution with
+  the dataset's spectrum, the crop (dmodels.hpp:7-46), the residual and its
+  sum of squares (objective.hpp:7-31, host/kernels.hpp:502-514), and the
+  copies of chi^2 and the kernel status word to pinned host memory; the
+  argument block is filled in the submitting thread, so the scheduler only
+  sets the slot's buffers and makes the call.
 * Latency: completion minus arrival (the submit time, or the arrival time a
   caller passes).  ``ModelServer.stats()`` gives p50/p99 and throughput.
 """
@@ -34,7 +37,7 @@ import numpy as np
 import torch
 
 from . import _native
-from ._native import c_float, c_int, check
+from ._native import c_int, check
 from .disk import KINDS
 
 c_int3 = c_int * 3
@@ -70,11 +73,22 @@ class Dataset:
         stream.synchronize()
         self.footprint = self.spectrum.numel() * 4 + 2 * 4 * int(np.prod(geom.size))
 
-    def request_footprint(self):
-        """Device bytes of one in-flight request: padded cube, its spectrum,
-        the cropped model and the residual."""
+    def request_layout(self):
+        """Byte offsets of one in-flight request's device buffers (padded
+        cube, its spectrum, cropped model, residual, chi^2), 256-byte
+        aligned, and their total."""
         px, py, pz = self.size_hi
-        return 4 * px * py * pz + _cbytes(self.size_hi) + 8 * int(np.prod(self.geom.size))
+        n = int(np.prod(self.geom.size))
+        off, lay = 0, {}
+        for name, nb in (('scube', 4 * px * py * pz), ('work', _cbytes(self.size_hi)),
+                         ('crop', 4 * n), ('res', 4 * n), ('chi2', 4)):
+            lay[name] = off
+            off += (nb + 255) // 256 * 256
+        return lay, off
+
+    def request_footprint(self):
+        """Device bytes of one in-flight request."""
+        return self.request_layout()[1]
 
 
 class Request:
@@ -93,7 +107,7 @@ class Request:
         self.arrival = arrival
         self.admit = self.done = None
         self.future = Future()
-        self.blob = self.layout = None
+        self.blob = self.layout = self.args = None
 
     def prepare(self):
         """Pack the parameters (Disk.pack, and the cloud budget of mcdisk)
@@ -130,6 +144,42 @@ class Request:
             self.nclouds = int(arrays[-2][1][-1]) if c[1] else 0
         self.blob, self.layout = blob, layout
 
+    def serve_args(self, ds):
+        """The native argument block of this request against dataset ds
+        (everything but the slot's buffers, which the scheduler sets)."""
+        lay, g = self.layout, ds.geom
+        off = lambda name: -1 if lay[name][0] is None else lay[name][0]
+        a = _native.ServeArgs()
+        a.kind = 0 if self.kind == 'smdisk' else 1
+        if a.kind == 1:
+            a.cflux, a.nclouds = float(self.cflux), int(self.nclouds)
+            a.off_csum, a.csum_len = off('csum'), lay['csum'][1]
+            a.off_hasordint = off('hoi')
+        else:
+            a.off_csum = a.off_hasordint = -1
+        a.loose, a.tilted = int(self.disk.loose), int(self.disk.tilted)
+        a.blob_bytes = self.blob.size
+        a.off_rnodes, a.nrnodes = off('subrnodes'), lay['subrnodes'][1]
+        a.off_vsys, a.off_xpos, a.off_ypos = off('vsys'), off('xpos'), off('ypos')
+        a.off_posa, a.off_incl = off('posa'), off('incl')
+        for i, k in enumerate(KINDS):
+            a.ntraits[i] = lay[k + '.uids'][1]
+            a.off_uids[i], a.off_cvalues[i] = off(k + '.uids'), off(k + '.cvalues')
+            a.off_ccounts[i], a.off_pvalues[i] = off(k + '.ccounts'), off(k + '.pvalues')
+            a.off_pcounts[i] = off(k + '.pcounts')
+        ss, st, sz = g.spat(self.thick)
+        spec = g.spec()
+        a.spat_size[:] = [int(v) for v in ss]
+        a.spat_step[:] = [float(v) for v in st]
+        a.spat_zero[:] = [float(v) for v in sz]
+        a.spec_size, a.spec_step, a.spec_zero = int(spec[0]), float(spec[1]), float(spec[2])
+        a.size_hi[:] = list(ds.size_hi)
+        a.edge[:] = [int(v) for v in g.edge]
+        a.size[:] = [int(v) for v in g.size]
+        a.spectrum, a.obs, a.err = _ptr(ds.spectrum), _ptr(ds.obs), _ptr(ds.err)
+        a.msk, a.weight = None, 1.0
+        return a
+
 
 class _Slot:
     STAGE = 1 << 20     # bytes of a request's packed parameters at most
@@ -142,6 +192,7 @@ class _Slot:
         self.ctx.set_mcdisk(mc_seed, 0)
         self.event = torch.cuda.Event()
         self.out = torch.empty(1, dtype=torch.float32, pin_memory=True)
+        self.status = torch.zeros(1, dtype=torch.int32, pin_memory=True)
         self.req = None
         self.keep = None
         self.bytes = 0
@@ -203,6 +254,7 @@ class ModelServer:
             request.prepare()
         if request.blob.size > _Slot.STAGE:
             raise ValueError("the request's parameter arrays exceed the staging buffer")
+        request.args = request.serve_args(self.datasets[request.dataset])
         with self._cv:
             if self._error is not None:
                 raise RuntimeError("the serving loop stopped") from self._error
@@ -294,72 +346,36 @@ class ModelServer:
 
     def _launch(self, slot, req, need):
         ds = self.datasets[req.dataset]
-        g = ds.geom
         req.admit = time.perf_counter()
         slot.req, slot.bytes = req, need
-        px, py, pz = ds.size_hi
-        nx, ny, nz = g.size
-        h = slot.ctx.handle
-        # parameters: one pinned -> device copy into the slot's staging buffers
+        lay, total = ds.request_layout()
         nb = req.blob.size
         slot.h_stage.numpy()[:nb] = req.blob
-        base = slot.d_stage.data_ptr()
-        lay = req.layout
-        P = lambda name: None if lay[name][0] is None else base + lay[name][0]
-        N = lambda name: lay[name][1]
         with torch.cuda.stream(slot.stream):
-            slot.d_stage[:nb].copy_(slot.h_stage[:nb], non_blocking=True)
-            scube = torch.zeros((pz, py, px), device=self.dev)
-            work = torch.empty(_cbytes(ds.size_hi) // 4, dtype=torch.float32, device=self.dev)
-            crop = torch.empty((nz, ny, nx), device=self.dev)
-            res = torch.empty((nz, ny, nx), device=self.dev)
-            total = torch.empty(1, dtype=torch.float32, device=self.dev)
-            ss, st, sz = g.spat(req.thick)
-            spec = g.spec()
-            args = [N('subrnodes'), P('subrnodes'), P('vsys'), P('xpos'), P('ypos'), P('posa'),
-                    P('incl')]
-            for k, counted in (('rpt', True), ('rht', False), ('vpt', True), ('vht', False),
-                               ('dpt', True), ('dht', False), ('zpt', True), ('spt', True),
-                               ('wpt', True)):
-                if counted:
-                    args.append(N(k + '.uids'))
-                args += [P(k + '.' + f) for f in ('uids', 'cvalues', 'ccounts', 'pvalues',
-                                                  'pcounts')]
-            args.append(None)   # opacity
-            args += [int(ss[0]), int(ss[1]), int(ss[2]), float(st[0]), float(st[1]),
-                     float(st[2]), float(sz[0]), float(sz[1]), float(sz[2]), int(spec[0]),
-                     float(spec[1]), float(spec[2])]
-            args += [None, scube.data_ptr()] + [None] * 8
-            loose, tilted = int(req.disk.loose), int(req.disk.tilted)
-            if req.kind == 'smdisk':
-                check(_lib.gbkb200_gmodel_smdisk_evaluate_f32(h, loose, tilted, *args),
-                      'smdisk_evaluate')
-            else:
-                check(_lib.gbkb200_gmodel_mcdisk_evaluate_f32(
-                    h, float(req.cflux), req.nclouds, P('csum'), N('csum'), P('hoi'), loose,
-                    tilted, *args), 'mcdisk_evaluate')
-            check(_lib.gbkb200_fft_convolve_f32(h, c_int3(*ds.size_hi), _ptr(scube), _ptr(work),
-                                                _ptr(ds.spectrum)), 'fft_convolve')
-            check(_lib.gbkb200_dmodel_dcube_downscale_f32(h, c_int3(1, 1, 1), c_int3(*g.edge),
-                                                          c_int3(*ds.size_hi), c_int3(*g.size),
-                                                          _ptr(scube), _ptr(crop)), 'crop')
-            check(_lib.gbkb200_objective_residual_f32(h, _ptr(ds.obs), _ptr(ds.err), None,
-                                                      _ptr(crop), None, None, crop.numel(),
-                                                      c_float(1.0), _ptr(res)), 'residual')
-            check(_lib.gbkb200_objective_residual_sum_f32(h, _ptr(res), res.numel(), 1,
-                                                          _ptr(total)), 'residual_sum')
-            slot.out.copy_(total, non_blocking=True)
-            slot.event.record(slot.stream)
-        slot.keep = (scube, work, crop, res, total)
+            buf = torch.empty(total, dtype=torch.uint8, device=self.dev)
+        b = buf.data_ptr()
+        a = req.args
+        a.blob_dev, a.blob_host = slot.d_stage.data_ptr(), slot.h_stage.data_ptr()
+        a.scube, a.work, a.crop = b + lay['scube'], b + lay['work'], b + lay['crop']
+        a.res, a.chi2_dev = b + lay['res'], b + lay['chi2']
+        a.chi2_host, a.status_host = slot.out.data_ptr(), slot.status.data_ptr()
+        check(_lib.gbkb200_serve_scube_chi2_f32(slot.ctx.handle, a), 'serve_scube_chi2')
+        slot.event.record(slot.stream)
+        slot.keep = (buf, lay['crop'])
 
     def _complete(self, slot):
         req = slot.req
         out = dict(chi2=float(slot.out[0]))
         if req.want_model:
-            out['model'] = slot.keep[2].cpu().numpy()
-        st = slot.ctx.handle
-        # status raised by the kernels of this request (unknown trait uid)
-        rc = _lib.gbkb200_ctx_synchronize(st)
+            buf, o = slot.keep
+            n = int(np.prod(self.datasets[req.dataset].geom.size))
+            nx, ny, nz = self.datasets[req.dataset].geom.size
+            out['model'] = buf[o:o + 4 * n].view(torch.float32).reshape(nz, ny, nx).cpu().numpy()
+        rc = 0
+        if int(slot.status[0]):
+            # a kernel of this request raised the status word (unknown trait
+            # uid): the context's synchronize reports and clears it
+            rc = _lib.gbkb200_ctx_synchronize(slot.ctx.handle)
         req.done = time.perf_counter()
         with self._cv:
             self._inflight -= slot.bytes

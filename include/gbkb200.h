@@ -196,6 +196,55 @@ int gbkb200_objective_residual_sum_f32(gbkb200_ctx* ctx, const float* residual, 
 int gbkb200_objective_residual_sum_noalloc_f32(const float* residual, int size, int squared,
                                                float* sum, void* stream);
 
+/* ---- one serving request in one call (no reference counterpart) --------
+ * The chain a serving loop runs per request, enqueued on the context's
+ * stream: the packed parameters are copied from pinned host memory
+ * (blob_host -> blob_dev, blob_bytes), the model cube (size_hi = padded
+ * {px, py, pz}) is zeroed and evaluated by smdisk_evaluate (kind 0) or
+ * mcdisk_evaluate (kind 1) with the parameter arrays found at byte offsets
+ * into blob_dev (-1 = absent; the trait counts of rht/vht/dht are those of
+ * rpt/vpt/dpt, as in GBKB200_DISK_ARGS), convolved with the resident
+ * spectrum by fft_convolve (work: complex work space of the padded grid),
+ * cropped at edge to size into crop, compared with the data (residual into
+ * res) and summed (chi2_dev); chi^2 and the context's kernel status word are
+ * then copied to chi2_host and status_host (pinned host memory): the result
+ * is there once the stream reaches the end of the call.  A nonzero status
+ * stays set in the context until gbkb200_ctx_synchronize clears it. */
+typedef struct {
+    int kind;
+    float cflux;
+    int nclouds;
+    int loose, tilted;
+    void* blob_dev;
+    const void* blob_host;
+    long long blob_bytes;
+    long long off_rnodes;
+    int nrnodes;
+    long long off_vsys, off_xpos, off_ypos, off_posa, off_incl;
+    int ntraits[9];            /* rpt, rht, vpt, vht, dpt, dht, zpt, spt, wpt */
+    long long off_uids[9], off_cvalues[9], off_ccounts[9], off_pvalues[9], off_pcounts[9];
+    long long off_csum;
+    int csum_len;
+    long long off_hasordint;
+    int spat_size[3];
+    float spat_step[3], spat_zero[3];
+    int spec_size;
+    float spec_step, spec_zero;
+    int size_hi[3], edge[3], size[3];
+    float* scube;
+    void* work;
+    const void* spectrum;
+    float* crop;
+    float* res;
+    const float *obs, *err, *msk;
+    float weight;
+    float* chi2_dev;
+    float* chi2_host;
+    int* status_host;
+} gbkb200_serve_args;
+
+int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serve_args* args);
+
 /* ---- differentiable chi^2 of a thin smooth disk (no reference counterpart:
  *      the reference computes no gradients).  A hand-written adjoint of
  *      smdisk_evaluate + fft_convolve_cached + crop + residual + residual_sum

@@ -158,3 +158,25 @@ def test_adjoint_rejects_unsupported_disks():
     for d in bad:
         with pytest.raises(ValueError):
             SMDiskChi2(d, g, np.zeros(g.size[::-1], np.float32))
+
+
+def test_serve_args_layout_matches_header(tmp_path):
+    """The ctypes mirror of gbkb200_serve_args has the C struct's size and
+    field offsets (a C program built from the header prints them)."""
+    import ctypes
+    import subprocess
+    from gbkfit_b200._native import ServeArgs
+    names = [f[0] for f in ServeArgs._fields_]
+    src = tmp_path / 'layout.c'
+    body = '\n'.join(f'  printf("{n} %zu\\n", offsetof(gbkb200_serve_args, {n}));' for n in names)
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "gbkb200.h"\n'
+                   'int main(void) {\n' + body +
+                   '\n  printf("sizeof %zu\\n", sizeof(gbkb200_serve_args));\n  return 0;\n}\n')
+    exe = tmp_path / 'layout'
+    subprocess.run(['gcc', '-I', os.path.join(ROOT, 'include'), str(src), '-o', str(exe)],
+                   check=True)
+    got = dict(line.split() for line in subprocess.run(
+        [str(exe)], check=True, capture_output=True, text=True).stdout.splitlines())
+    assert int(got.pop('sizeof')) == ctypes.sizeof(ServeArgs)
+    for n in names:
+        assert int(got[n]) == getattr(ServeArgs, n).offset, n
