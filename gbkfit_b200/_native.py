@@ -84,7 +84,7 @@ class ServeArgs(ctypes.Structure):
                 ('spec_step', c_float), ('spec_zero', c_float), ('size_hi', c_int * 3),
                 ('edge', c_int * 3), ('size', c_int * 3), ('scube', c_void_p),
                 ('work', c_void_p), ('spectrum', c_void_p), ('crop', c_void_p),
-                ('res', c_void_p), ('obs', c_void_p), ('err', c_void_p), ('msk', c_void_p),
+                ('obs', c_void_p), ('err', c_void_p), ('msk', c_void_p),
                 ('weight', c_float), ('chi2_dev', c_void_p), ('chi2_host', c_void_p),
                 ('status_host', c_void_p)]
 

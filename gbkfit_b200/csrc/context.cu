@@ -45,6 +45,7 @@ extern "C" int gbkb200_ctx_destroy(gbkb200_ctx* ctx)
     gbk_fft_state_destroy(ctx);
     if (ctx->reduce_scratch) cudaFree(ctx->reduce_scratch);
     if (ctx->mc_scratch) cudaFree(ctx->mc_scratch);
+    if (ctx->serve_scratch) cudaFree(ctx->serve_scratch);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     delete ctx;

@@ -79,6 +79,7 @@ struct gbkb200_ctx {
     size_t reduce_scratch_bytes = 0;
     void* mc_scratch = nullptr;     // fixed-point accumulators of deterministic mcdisk
     size_t mc_scratch_bytes = 0;
+    void* serve_scratch = nullptr;  // block partials + last-block counter (serve.cu)
 };
 
 int gbk_finish(gbkb200_ctx* ctx);   // launch check, and sync + status read in sync mode

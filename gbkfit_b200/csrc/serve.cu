@@ -7,12 +7,72 @@
 // sum of squares taken (objective.hpp:7-31, host/kernels.hpp:502-514), and
 // chi^2 and the context's kernel status word are copied to pinned host
 // memory, so that the caller sees the result without another CUDA call.
+// The crop, residual and sum run as one fused kernel.
+#include <algorithm>
+
 #include "gbk_common.cuh"
+
+namespace gbk {
+
+constexpr int TAIL_BLOCKS = 296;   // 2 x 148 SMs
+constexpr int TAIL_THREADS = 256;
+
+// Crop of the convolved cube (dmodels.hpp:7-46 at scale 1: a copy), the
+// residual (model - data) / error x mask x weight (objective.hpp:7-31) and its sum of
+// squares, in one pass: fp32 within a block, one fp64 partial per block,
+// and the last block to finish adds the partials in block order (a fixed
+// order for a given size, so the sum does not depend on the schedule).
+__global__ void __launch_bounds__(TAIL_THREADS)
+    serve_tail_kernel(const float* __restrict__ scube, int px, int py, int ex, int ey, int ez,
+                      int nx, int ny, int n, const float* __restrict__ obs,
+                      const float* __restrict__ err, const float* __restrict__ msk, float weight,
+                      float* __restrict__ crop,
+                      double* part, unsigned* counter, float* chi2)
+{
+    __shared__ float ws[TAIL_THREADS / 32];
+    __shared__ bool last;
+    float acc = 0.f;
+    const int nxy = nx * ny;
+    for (int i = blockIdx.x * TAIL_THREADS + threadIdx.x; i < n; i += gridDim.x * TAIL_THREADS) {
+        const int z = i / nxy, rem = i - z * nxy;
+        const int y = rem / nx, x = rem - y * nx;
+        const float m = scube[(long long)(ez + z) * px * py + (long long)(ey + y) * px + (ex + x)];
+        if (crop) crop[i] = m;
+        float r = m - obs[i];
+        if (err) r /= err[i];
+        if (msk) r *= msk[i];
+        r *= weight;
+        acc += r * r;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float v = 0.f;
+        for (int w = 0; w < TAIL_THREADS / 32; ++w) v += ws[w];
+        part[blockIdx.x] = (double)v;
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double s = 0;
+        for (int b = 0; b < (int)gridDim.x; ++b) s += ((volatile double*)part)[b];
+        chi2[0] = (float)s;
+        *counter = 0u;   // ready for the next request on this context
+    }
+}
+
+}  // namespace gbk
+
+using namespace gbk;
 
 extern "C" int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serve_args* a)
 {
-    if (!ctx || !a || !a->blob_dev || !a->scube || !a->work || !a->spectrum || !a->crop ||
-        !a->res || !a->obs || !a->chi2_dev || !a->chi2_host || !a->status_host)
+    if (!ctx || !a || !a->blob_dev || !a->scube || !a->work || !a->spectrum || !a->obs ||
+        !a->chi2_dev || !a->chi2_host || !a->status_host)
         return GBKB200_ERR_INVALID_ARG;
     if (a->kind != 0 && a->kind != 1) return GBKB200_ERR_INVALID_ARG;
     for (int k = 0; k < 3; ++k)
@@ -59,15 +119,19 @@ extern "C" int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serv
 #undef GBK_T
     if (rc) return rc;
     if ((rc = gbkb200_fft_convolve_f32(ctx, a->size_hi, a->scube, a->work, a->spectrum))) return rc;
-    const int one[3] = {1, 1, 1};
-    if ((rc = gbkb200_dmodel_dcube_downscale_f32(ctx, one, a->edge, a->size_hi, a->size, a->scube,
-                                                 a->crop)))
-        return rc;
-    const int n = a->size[0] * a->size[1] * a->size[2];
-    if ((rc = gbkb200_objective_residual_f32(ctx, a->obs, a->err, a->msk, a->crop, nullptr,
-                                             nullptr, n, a->weight, a->res)))
-        return rc;
-    if ((rc = gbkb200_objective_residual_sum_f32(ctx, a->res, n, 1, a->chi2_dev))) return rc;
+    if (!ctx->serve_scratch) {
+        const size_t bytes = TAIL_BLOCKS * sizeof(double) + 256;
+        if (cudaMalloc(&ctx->serve_scratch, bytes) != cudaSuccess) return GBKB200_ERR_OOM;
+        GBK_CUDA_TRY(cudaMemsetAsync(ctx->serve_scratch, 0, bytes, st));
+    }
+    double* part = static_cast<double*>(ctx->serve_scratch);
+    unsigned* counter = reinterpret_cast<unsigned*>(part + TAIL_BLOCKS);
+    const long long n = (long long)a->size[0] * a->size[1] * a->size[2];
+    if (n >= (1ll << 31) || vhi >= (1ll << 31)) return GBKB200_ERR_TOO_LARGE;
+    int blocks = (int)std::min<long long>(TAIL_BLOCKS, (n + 4 * TAIL_THREADS - 1) / (4 * TAIL_THREADS));
+    serve_tail_kernel<<<blocks, TAIL_THREADS, 0, st>>>(
+        a->scube, a->size_hi[0], a->size_hi[1], a->edge[0], a->edge[1], a->edge[2], a->size[0],
+        a->size[1], (int)n, a->obs, a->err, a->msk, a->weight, a->crop, part, counter, a->chi2_dev);
     GBK_CUDA_TRY(cudaMemcpyAsync(a->chi2_host, a->chi2_dev, sizeof(float),
                                  cudaMemcpyDeviceToHost, st));
     GBK_CUDA_TRY(cudaMemcpyAsync(a->status_host, ctx->d_status, sizeof(int),

@@ -75,13 +75,13 @@ class Dataset:
 
     def request_layout(self):
         """Byte offsets of one in-flight request's device buffers (padded
-        cube, its spectrum, cropped model, residual, chi^2), 256-byte
+        cube, its spectrum, cropped model, chi^2), 256-byte
         aligned, and their total."""
         px, py, pz = self.size_hi
         n = int(np.prod(self.geom.size))
         off, lay = 0, {}
         for name, nb in (('scube', 4 * px * py * pz), ('work', _cbytes(self.size_hi)),
-                         ('crop', 4 * n), ('res', 4 * n), ('chi2', 4)):
+                         ('crop', 4 * n), ('chi2', 4)):
             lay[name] = off
             off += (nb + 255) // 256 * 256
         return lay, off
@@ -351,13 +351,15 @@ class ModelServer:
         lay, total = ds.request_layout()
         nb = req.blob.size
         slot.h_stage.numpy()[:nb] = req.blob
-        with torch.cuda.stream(slot.stream):
-            buf = torch.empty(total, dtype=torch.uint8, device=self.dev)
+        # allocated on the scheduler's stream and released only after the
+        # slot's event has completed, so the allocator never hands it out
+        # while the slot's stream still uses it
+        buf = torch.empty(total, dtype=torch.uint8, device=self.dev)
         b = buf.data_ptr()
         a = req.args
         a.blob_dev, a.blob_host = slot.d_stage.data_ptr(), slot.h_stage.data_ptr()
-        a.scube, a.work, a.crop = b + lay['scube'], b + lay['work'], b + lay['crop']
-        a.res, a.chi2_dev = b + lay['res'], b + lay['chi2']
+        a.scube, a.work, a.chi2_dev = b + lay['scube'], b + lay['work'], b + lay['chi2']
+        a.crop = b + lay['crop'] if req.want_model else None
         a.chi2_host, a.status_host = slot.out.data_ptr(), slot.status.data_ptr()
         check(_lib.gbkb200_serve_scube_chi2_f32(slot.ctx.handle, a), 'serve_scube_chi2')
         slot.event.record(slot.stream)

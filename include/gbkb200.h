@@ -205,8 +205,9 @@ int gbkb200_objective_residual_sum_noalloc_f32(const float* residual, int size, 
  * into blob_dev (-1 = absent; the trait counts of rht/vht/dht are those of
  * rpt/vpt/dpt, as in GBKB200_DISK_ARGS), convolved with the resident
  * spectrum by fft_convolve (work: complex work space of the padded grid),
- * cropped at edge to size into crop, compared with the data (residual into
- * res) and summed (chi2_dev); chi^2 and the context's kernel status word are
+ * cropped at edge to size (into crop, when not NULL), compared with the data
+ * ((model - obs) / err * msk * weight; err and msk may be NULL) and
+ * summed in squares (chi2_dev); chi^2 and the context's kernel status word are
  * then copied to chi2_host and status_host (pinned host memory): the result
  * is there once the stream reaches the end of the call.  A nonzero status
  * stays set in the context until gbkb200_ctx_synchronize clears it. */
@@ -235,7 +236,6 @@ typedef struct {
     void* work;
     const void* spectrum;
     float* crop;
-    float* res;
     const float *obs, *err, *msk;
     float weight;
     float* chi2_dev;
