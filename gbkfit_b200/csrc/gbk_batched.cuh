@@ -381,38 +381,40 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
             }
         }
         __syncthreads();
-        // y FIR in place: model(yo, xo) = sum_t ur[t] S[yo + t][xo], written to S row yo
+        // y FIR in place: model(yo, xo) = sum_t ur[t] S[yo + t][xo], written to S row yo.
+        // Packed FP32 pairs (FFMA2: two lanes of fma, each rounded as fmaf),
+        // columns (x, x+1) and (x+2, x+3) of a float4 per instruction
         {
-            float ur[K];
+            float2 u2[K];
 #pragma unroll
-            for (int t = 0; t < K; ++t) ur[t] = P.ur[t];
+            for (int t = 0; t < K; ++t) u2[t] = make_float2(P.ur[t], P.ur[t]);
             const int gmax = max(1, KB_THREADS * KB_IT / ns4);  // row groups per round at most
             const int rounds = (ng + gmax - 1) / gmax;
             const int gpr = (ng + rounds - 1) / rounds;         // balanced rounds
             for (int gr0 = 0; gr0 < ng; gr0 += gpr) {
                 const int nitems = min(gpr, ng - gr0) * ns4;
-                float acc[KB_IT][8][4];
+                float2 acc[KB_IT][8][2];
 #pragma unroll
                 for (int it = 0; it < KB_IT; ++it) {
                     const int item = threadIdx.x + it * KB_THREADS;
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) acc[it][q][k] = 0.f;
+                    for (int q = 0; q < 8; ++q) {
+                        acc[it][q][0] = make_float2(0.f, 0.f);
+                        acc[it][q][1] = make_float2(0.f, 0.f);
+                    }
                     if (item < nitems) {
                         const int rb = 8 * (gr0 + item / ns4), s4 = item % ns4;
                         const float4* colp = reinterpret_cast<const float4*>(S) + rb * bp4 + s4;
 #pragma unroll
                         for (int m = 0; m < K + 7; ++m) {
                             const float4 p = colp[m * bp4];
+                            const float2 pxy = make_float2(p.x, p.y), pzw = make_float2(p.z, p.w);
 #pragma unroll
                             for (int q = 0; q < 8; ++q) {
                                 const int t = m - q;
                                 if (t >= 0 && t < K) {
-                                    acc[it][q][0] += ur[t] * p.x;
-                                    acc[it][q][1] += ur[t] * p.y;
-                                    acc[it][q][2] += ur[t] * p.z;
-                                    acc[it][q][3] += ur[t] * p.w;
+                                    acc[it][q][0] = __ffma2_rn(u2[t], pxy, acc[it][q][0]);
+                                    acc[it][q][1] = __ffma2_rn(u2[t], pzw, acc[it][q][1]);
                                 }
                             }
                         }
@@ -428,8 +430,8 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
                         for (int q = 0; q < 8; ++q)
                             if (ys + rb + q < ye)
                                 reinterpret_cast<float4*>(S)[(rb + q) * bp4 + s4] =
-                                    make_float4(acc[it][q][0], acc[it][q][1], acc[it][q][2],
-                                                acc[it][q][3]);
+                                    make_float4(acc[it][q][0].x, acc[it][q][0].y,
+                                                acc[it][q][1].x, acc[it][q][1].y);
                     }
                 }
                 __syncthreads();
