@@ -465,6 +465,199 @@ def run_reference(args):
                          d2h_bytes_per_step=0))
 
 
+# ---- secondary workloads (one JSON line each; not the headline metric) -------
+
+KINDS = ('rpt', 'rht', 'vpt', 'vht', 'dpt', 'dht', 'zpt', 'spt', 'wpt')
+
+
+def _device_packed(packed, dev):
+    """Disk.pack() host arrays -> torch tensors on the device."""
+    import torch
+    out = {}
+    for k, v in packed.items():
+        if v is None:
+            out[k] = None
+        elif isinstance(v, dict):
+            out[k] = {f: torch.from_numpy(np.ascontiguousarray(a)).to(dev) for f, a in v.items()}
+        else:
+            out[k] = torch.from_numpy(np.ascontiguousarray(v)).to(dev)
+    return out
+
+
+def _trait_args(pd):
+    args = []
+    for k in KINDS:
+        t = pd[k]
+        args += [None] * 5 if t is None else [t['uids'], t['cvalues'], t['ccounts'],
+                                              t['pvalues'], t['pcounts']]
+    return args
+
+
+def _events_ms(fn, steps, warmup):
+    """Mean device ms of fn() over `steps` calls (CUDA events on the current
+    stream, L2 flushed before every call), after `warmup` calls."""
+    import torch
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    stream = torch.cuda.current_stream()
+    for i in range(steps):
+        flush.fill_(float(i))
+        e0[i].record(stream)
+        fn()
+        e1[i].record(stream)
+    torch.cuda.synchronize()
+    return float(np.mean([a.elapsed_time(b) for a, b in zip(e0, e1)]))
+
+
+def run_mcdisk(args):
+    """mcdisk_cube256: 1e7 clouds of a thick exponential disk into the
+    320x320x320 (spatial) x 160 (channels) padded grid, through the drop-in
+    gmodel backend (fast and deterministic modes); the reference's mcdisk
+    template (OpenMP) on the host cores for the same call."""
+    import torch
+    from gbkfit_b200 import workloads
+    from gbkfit_b200.driver import DriverB200
+    w = workloads.mcdisk_cube256()
+    csum = w.disk.ncloudscsum(w.params, w.cflux)
+    hoi = w.disk.hasordint()
+    n = int(csum[-1])
+    g = w.geometry_args()
+    nx, ny, _ = g['spat_size']
+    nz = g['spec_size']
+    packed = w.disk.pack(w.params)
+    pd = _device_packed(packed, 'cuda')
+    cs, hs = torch.from_numpy(csum).cuda(), torch.from_numpy(hoi).cuda()
+    scube = torch.zeros((nz, ny, nx), device='cuda')
+    gm = DriverB200(torch.cuda.current_device()).backends().gmodel(np.float32)
+
+    def call():
+        scube.zero_()
+        gm.mcdisk_evaluate(w.cflux, n, cs, hs, g['loose'], g['tilted'], pd['subrnodes'],
+                           pd['vsys'], pd['xpos'], pd['ypos'], pd['posa'], pd['incl'],
+                           *_trait_args(pd), g.get('opacity'), g['spat_size'], g['spat_step'],
+                           g['spat_zero'], 0.0, g['spec_size'], g['spec_step'],
+                           g['spec_zero'], None, scube, None, None, None, None, None, None,
+                           None, None)
+
+    ms = {}
+    for mode, name in ((0, 'fast'), (1, 'deterministic')):
+        gm.set_mcdisk(seed=42, mode=mode)
+        ms[name] = _events_ms(call, args.steps, args.warmup)
+    gm.set_mcdisk(seed=42, mode=0)
+    cpu = None
+    if args.cpu_baseline:
+        from oracle.oracle import Reference, build
+        if not Reference.available():
+            build()
+        ref = Reference()
+        h = np.zeros((nz, ny, nx), np.float32)
+        t0 = time.perf_counter()
+        ref.mcdisk_evaluate(w.cflux, n, csum, hoi, packed, g, dict(scube=h))
+        dt = time.perf_counter() - t0
+        cpu = dict(value=round(1 / dt, 3), unit='evals/s', cores=ref.num_threads(),
+                   kind='reference', sample='one full call (1e7 clouds)')
+    return dict(metric='mcdisk evals/s (1e7 clouds, thick disk, padded 320x320x320 x 160 grid)',
+                value=round(1e3 / ms['fast'], 2), unit='evals/s', n_gpus=1, steps=args.steps,
+                warmup=args.warmup, ms_per_step=round(ms['fast'], 4),
+                ms_deterministic=round(ms['deterministic'], 4), higher_is_better=True,
+                dtype='f32', data='synthetic', gpu_launches=args.steps,
+                config=dict(workload='mcdisk_cube256', nclouds=n, grid=[nx, ny, g['spat_size'][2], nz],
+                            l2='flushed before every call (256 MB write)'),
+                cpu_baseline=cpu)
+
+
+def run_smdisk64(args):
+    """smdisk_cube64: the reference-style per-call drop-in path (DModelSCube
+    + smdisk, one synchronous call chain) on a 64^3 cube."""
+    import torch
+    from gbkfit_b200 import model as M, workloads
+    from gbkfit_b200.driver import DriverB200
+    w0 = workloads.smdisk_cube64()
+    drv = DriverB200(torch.cuda.current_device())
+    comp = M.SpectralSMDisk2D(False, False, w0.disk.traits['rpt'], w0.disk.traits['vpt'],
+                              w0.disk.traits['dpt'], rnodes=w0.disk.rnodes)
+    g0 = w0.geom
+    dm = M.DModelSCube(g0.size, g0.step, rpix=(0, 0, (g0.size[2] - 1) / 2), rval=(0, 0, 0),
+                       psf=g0.psf, lsf=g0.lsf)
+    mdl = M.Model(drv, dm, M.GModelKinematics2D([comp]))
+    for _ in range(args.warmup):
+        mdl.evaluate_d(w0.params)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        mdl.evaluate_d(w0.params)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) / args.steps * 1e3
+    cpu = None
+    if args.cpu_baseline:
+        from oracle.oracle import Reference, build
+        if not Reference.available():
+            build()
+        ref = Reference()
+        ga = w0.geometry_args()
+        hh = np.zeros((ga['spec_size'], ga['spat_size'][1], ga['spat_size'][0]), np.float32)
+        t0 = time.perf_counter()
+        for _ in range(5):
+            hh[:] = 0
+            ref.smdisk_evaluate(w0.disk.pack(w0.params), ga, dict(scube=hh))
+        cpu = dict(value=round(5 / (time.perf_counter() - t0), 2), unit='evals/s',
+                   cores=ref.num_threads(), kind='reference',
+                   sample='5 smdisk calls into the 96^3 padded cube (model stage only)')
+    return dict(metric='smdisk_cube64 drop-in model evaluations/s (per call, synchronous)',
+                value=round(1e3 / ms, 1), unit='evals/s', n_gpus=1, steps=args.steps,
+                warmup=args.warmup, ms_per_step=round(ms, 4), higher_is_better=True,
+                dtype='f32', data='synthetic',
+                config=dict(workload='smdisk_cube64: 64^3 cube, 20 nodes, Gaussian PSF x LSF, '
+                                     'padded 96^3', path='Model.evaluate_d (DModelSCube)'),
+                cpu_baseline=cpu)
+
+
+def run_grad96(args):
+    """grad96: chi^2 and its gradient (66 parameters) of smdisk + PSF/LSF on a
+    96x96x64 cube through the hand-written adjoint; the data are the GPU
+    model of the truth parameters plus seeded noise of 2 % of the peak."""
+    import torch
+    from gbkfit_b200 import workloads
+    from gbkfit_b200.adjoint import SMDiskChi2, to_vector
+    w = workloads.smdisk_grad96()
+    shape = tuple(w.geom.size[::-1])
+    probe = SMDiskChi2(w.disk, w.geom, np.zeros(shape, np.float32), np.ones(shape, np.float32))
+    probe.value(to_vector(w.extra['truth'], 1.0))
+    ex, ey, ez = w.geom.edge
+    nx, ny, nz = w.geom.size
+    m = probe.scube[ez:ez + nz, ey:ey + ny, ex:ex + nx].double().cpu().numpy()
+    rng = np.random.default_rng(w.extra['noise_seed'])
+    sigma = w.extra['noise_frac'] * float(np.max(m))
+    data = (m + rng.normal(0.0, sigma, m.shape)).astype(np.float32)
+    err = np.full(m.shape, sigma, np.float32)
+    model = SMDiskChi2(w.disk, w.geom, data, err)
+    theta = to_vector(w.params, w.extra['scale'])
+    for _ in range(args.warmup):
+        model.value_and_grad(theta)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        model.value_and_grad(theta)
+    ms = (time.perf_counter() - t0) / args.steps * 1e3
+    return dict(metric='grad96 chi^2 + gradient evaluations/s (66 parameters)',
+                value=round(1e3 / ms, 1), unit='evals/s', n_gpus=1, steps=args.steps,
+                warmup=args.warmup, ms_per_step=round(ms, 4), higher_is_better=True,
+                dtype='f32', data='synthetic',
+                config=dict(workload='smdisk_grad96: 96x96x64 cube, 20 nodes, 66 parameters',
+                            path='SMDiskChi2.value_and_grad (host vector in, host gradient out)'))
+
+
+def run_serving(args):
+    out = serving_run(nrequests=args.requests)
+    return dict(metric='serving capacity evals/s and latency (ms)',
+                value=out['capacity_evals_per_s'], unit='evals/s', n_gpus=1,
+                higher_is_better=True, dtype='f32', data='synthetic', serving=out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -483,10 +676,21 @@ def main():
     ap.add_argument('--chunk', type=int, default=0, help='force the sets per wave (default: tuned)')
     ap.add_argument('--band', type=int, default=0,
                     help='force the output rows per PSF block of the direct mode (default: tuned)')
+    ap.add_argument('--workload', default='smdisk_batch128',
+                    choices=['smdisk_batch128', 'mcdisk_cube256', 'smdisk_cube64', 'grad96',
+                             'serving'],
+                    help='smdisk_batch128 is the headline; the others print their own line')
+    ap.add_argument('--requests', type=int, default=10000, help='serving workload: requests')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == 'reference':
+    other = dict(mcdisk_cube256=run_mcdisk, smdisk_cube64=run_smdisk64, grad96=run_grad96,
+                 serving=run_serving)
+    if args.workload in other and args.impl != 'reference':
+        import torch
+        torch.cuda.set_device(0)
+        out = other[args.workload](args)
+    elif args.impl == 'reference':
         out = run_reference(args)
     else:
         out = run_b200(args)
