@@ -108,7 +108,8 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
                                            : smdisk_spaxel(a, kc, x, y, 0, o, bad));
     if (on && line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo, hi)) {
         amp = o.orv * (1 / (o.dv * sqrtf(2 * GBK_PI)));
-        rinv = 1 / (2 * o.dv * o.dv);
+        // exp(-d^2 / (2 sigma^2)) as exp2(-d^2 * log2(e) / (2 sigma^2))
+        rinv = 1.4426950408889634f / (2 * o.dv * o.dv);
     } else {
         lo = INT_MAX;
         hi = -1;
@@ -117,7 +118,7 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
     // gmodels.hpp:109-115: the line at window channel z (0 outside [lo, hi])
     auto line = [&](int z) {
         const float d = (z0 + z * dz) - v;
-        return (z >= lo && z <= hi) ? amp * expf(-(d * d) * rinv) : 0.f;
+        return (z >= lo && z <= hi) ? amp * exp2f(-(d * d) * rinv) : 0.f;
     };
     // the lane's and the warp's output channel ranges
     const bool lit = lo <= hi;
