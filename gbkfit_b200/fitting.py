@@ -182,12 +182,14 @@ class DynestyLikelihood:
 
 
 class BatchPool:
-    """A pool for dynesty (``pool=BatchPool(), queue_size=q``): ``map`` of a
-    batched likelihood (a DynestyLikelihood, or a wrapper that holds one in
-    ``.func``, as dynesty wraps its callables) is one batched evaluation;
-    anything else is mapped point by point."""
+    """A pool for dynesty (``pool=BatchPool(size)``; dynesty queues ``size``
+    points when no ``queue_size`` is given): ``map`` of a batched likelihood
+    (a DynestyLikelihood, or a wrapper that holds one in ``.func``, as dynesty
+    wraps its callables) is one batched evaluation; anything else is mapped
+    point by point."""
 
-    size = 1
+    def __init__(self, size=512):
+        self.size = int(size)
 
     def map(self, fn, iterable):
         pts = list(iterable)
