@@ -450,24 +450,35 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
             const int n = (ye - ys) * nv;
             const int dq = KB_THREADS / nv, dr = KB_THREADS % nv;
             int row = threadIdx.x / nv, col = threadIdx.x % nv;
+            // running offsets: si in S (float4), vi in the data plane (float)
+            int si = row * bp4 + col, vi = pbase + (ys + row) * P.Nx + xb0 + 4 * col;
+            const int dsi = dq * bp4 + dr, dvi = dq * P.Nx + 4 * dr;
+            float2 s2 = make_float2(0.f, 0.f);
 #pragma unroll 4
             for (int i = threadIdx.x; i < n; i += KB_THREADS) {
-                const int yo = ys + row, xo = xb0 + 4 * col;
-                const float4 m = reinterpret_cast<const float4*>(S)[row * bp4 + col];
-                const int vi = pbase + yo * P.Nx + xo;
+                const float4 m = reinterpret_cast<const float4*>(S)[si];
                 const float4 o = *reinterpret_cast<const float4*>(P.obs + vi);
                 const float4 w = *reinterpret_cast<const float4*>(P.iw + vi);
-                const float r0 = (m.x - o.x) * w.x, r1 = (m.y - o.y) * w.y;
-                const float r2 = (m.z - o.z) * w.z, r3 = (m.w - o.w) * w.w;
-                sum += r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3;
-                if (model) *reinterpret_cast<float4*>(model + yo * P.Nx + xo) = m;
-                row += dq;
+                // packed pairs: r = (m - o) w, s2 += r^2
+                const float2 r01 = __fmul2_rn(__fadd2_rn(make_float2(m.x, m.y),
+                                                         make_float2(-o.x, -o.y)),
+                                              make_float2(w.x, w.y));
+                const float2 r23 = __fmul2_rn(__fadd2_rn(make_float2(m.z, m.w),
+                                                         make_float2(-o.z, -o.w)),
+                                              make_float2(w.z, w.w));
+                s2 = __ffma2_rn(r01, r01, s2);
+                s2 = __ffma2_rn(r23, r23, s2);
+                if (model) *reinterpret_cast<float4*>(model + (vi - pbase)) = m;
                 col += dr;
+                si += dsi;
+                vi += dvi;
                 if (col >= nv) {
                     col -= nv;
-                    ++row;
+                    si += bp4 - nv;
+                    vi += P.Nx - 4 * nv;
                 }
             }
+            sum += s2.x + s2.y;
         } else {
             const int nw = xb_end - xb0, n = (ye - ys) * nw;
             for (int i = threadIdx.x; i < n; i += KB_THREADS) {
