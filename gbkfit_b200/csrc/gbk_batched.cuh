@@ -118,15 +118,19 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
     // gmodels.hpp:109-115: the line at window channel z (0 outside [lo, hi]);
     // 2^x by the PTX ex2.approx instruction (relative error ~2^-22; the
     // argument is >= -18.1 inside the +-5 sigma window, far from underflow)
+    // (one unsigned compare for z in [lo, hi]; a lane without a line has
+    // amp = 0 and rinv = 0, so its value is 0 whatever the compare says)
+    const unsigned wlen = (unsigned)hi - (unsigned)lo;
     auto line = [&](int z) {
         const float d = (z0 + z * dz) - v;
         float e;
         asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-(d * d) * rinv));
-        return (z >= lo && z <= hi) ? amp * e : 0.f;
+        return (unsigned)z - (unsigned)lo <= wlen ? amp * e : 0.f;
     };
     // the lane's and the warp's output channel ranges
     const bool lit = lo <= hi;
     const int olo = lit ? max(0, lo - KZ + 1) : INT_MAX, ohi = lit ? min(P.Nz - 1, hi) : -1;
+    const unsigned olen = lit ? (unsigned)(ohi - olo) : 0u;
     int zlo = olo, zhi = ohi;
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) {
@@ -162,7 +166,9 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
                 for (int t = 1; t < KZ; t += 2) acc1 += lz[t] * w[(k + t) % KZ];
                 *dp = acc0 + acc1;      // plane zo
                 dp += zstride;
-                const unsigned m = __ballot_sync(0xffffffffu, zo >= olo && zo <= ohi);
+                // zo in [olo, ohi] (false for a lane without a line: olo = INT_MAX, ohi = -1)
+                const unsigned m = __ballot_sync(0xffffffffu,
+                                                 (unsigned)zo - (unsigned)olo <= olen);
                 if (lane == zo - mz) mm = m;
                 if (zo - mz == 31 || zo == zhi) {
                     const int zz = mz + lane;
