@@ -180,3 +180,14 @@ def test_serve_args_layout_matches_header(tmp_path):
     assert int(got.pop('sizeof')) == ctypes.sizeof(ServeArgs)
     for n in names:
         assert int(got[n]) == getattr(ServeArgs, n).offset, n
+
+
+def test_serve_entry_rejects_missing_arguments():
+    """The per-request serving call checks its arguments before touching the
+    device: no context or no argument block is an invalid-argument error."""
+    import ctypes
+    from gbkfit_b200 import _native
+    lib = _native.lib()
+    assert lib.gbkb200_serve_scube_chi2_f32(None, None) == 1
+    a = _native.ServeArgs()
+    assert lib.gbkb200_serve_scube_chi2_f32(None, ctypes.byref(a)) == 1
