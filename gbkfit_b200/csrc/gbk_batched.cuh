@@ -151,7 +151,9 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
         const long long zstride = (long long)P.Wy * P.pitch;
         float* dp = P.mplanes + ((long long)c * P.Nz * P.Wy + y) * P.pitch + x + zlo * zstride;
         unsigned mm = 0u;
-        int mz = zlo;     // lane (zo - mz) keeps the ballot of plane zo, flushed every 32 planes
+        // lane (zo - mz) keeps the ballot of plane zo; flushed at plane fl, every
+        // 32 planes and at the last one
+        int mz = zlo, own = zlo + lane, fl = min(zlo + 31, zhi);
         for (int zb = zlo; zb <= zhi; zb += KZ) {
 #pragma unroll
             for (int k = 0; k < KZ; ++k) {
@@ -169,14 +171,15 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
                 // zo in [olo, ohi] (false for a lane without a line: olo = INT_MAX, ohi = -1)
                 const unsigned m = __ballot_sync(0xffffffffu,
                                                  (unsigned)zo - (unsigned)olo <= olen);
-                if (lane == zo - mz) mm = m;
-                if (zo - mz == 31 || zo == zhi) {
-                    const int zz = mz + lane;
-                    if (zz <= zo)
-                        xr[zz] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
-                                       ((chunk * 32 + 31 - __clz(mm)) << 16))
-                                    : -1;
+                if (zo == own) mm = m;
+                if (zo == fl) {
+                    if (own <= zo)
+                        xr[own] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
+                                        ((chunk * 32 + 31 - __clz(mm)) << 16))
+                                     : -1;
                     mz = zo + 1;
+                    own = mz + lane;
+                    fl = min(mz + 31, zhi);
                 }
             }
         }
