@@ -120,13 +120,15 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
     // argument is >= -18.1 inside the +-5 sigma window, far from underflow)
     // (one unsigned compare for z in [lo, hi]; a lane without a line has
     // amp = 0 and rinv = 0, so its value is 0 whatever the compare says)
+    // zf: z as a float (exact: channel indices are far below 2^24)
     const unsigned wlen = (unsigned)hi - (unsigned)lo;
-    auto line = [&](int z) {
-        const float d = (z0 + z * dz) - v;
+    auto line_f = [&](int z, float zf) {
+        const float d = (z0 + zf * dz) - v;
         float e;
         asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-(d * d) * rinv));
         return (unsigned)z - (unsigned)lo <= wlen ? amp * e : 0.f;
     };
+    auto line = [&](int z) { return line_f(z, (float)z); };
     // the lane's and the warp's output channel ranges
     const bool lit = lo <= hi;
     const int olo = lit ? max(0, lo - KZ + 1) : INT_MAX, ohi = lit ? min(P.Nz - 1, hi) : -1;
@@ -154,12 +156,14 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
         // lane (zo - mz) keeps the ballot of plane zo; flushed at plane fl, every
         // 32 planes and at the last one
         int mz = zlo, own = zlo + lane, fl = min(zlo + 31, zhi);
+        float zf = (float)(zlo + KZ - 1);       // the newest window channel, counted in float
         for (int zb = zlo; zb <= zhi; zb += KZ) {
 #pragma unroll
             for (int k = 0; k < KZ; ++k) {
                 const int zo = zb + k;
                 if (zo > zhi) break;
-                w[(k + KZ - 1) % KZ] = line(zo + KZ - 1);
+                w[(k + KZ - 1) % KZ] = line_f(zo + KZ - 1, zf);
+                zf += 1.f;
                 // two independent accumulation chains (even and odd taps)
                 float acc0 = 0.f, acc1 = 0.f;
 #pragma unroll
