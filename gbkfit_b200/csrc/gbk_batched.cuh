@@ -215,7 +215,8 @@ __device__ __forceinline__ double sat_box(const double* T, int ld, int y0, int y
 // memory (box-relative row pitch; usually one pass):
 //   - the rows' nonzero segments are loaded from HBM (cp.async), the rest of
 //     the rows that the y FIR reads is zeroed;
-//   - x FIR in place, a warp per 1, 2 or 4 rows, 8 outputs per lane window;
+//   - x FIR in place, a warp per row, its lanes on consecutive (row, strip)
+//     pairs of its rows, 8 outputs per lane window;
 //   - y FIR in place, 8 x 4 outputs per item, ascending rounds of whole 8-row
 //     groups (an output row only overwrites an input row that no later output
 //     of the pass reads);
@@ -359,43 +360,51 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
         }
         cp_async_wait_all();
         __syncthreads();
-        // x FIR in place: S[y][xo] = sum_s vr[s] S[y][xo + s]; a warp owns rw
-        // whole rows (lane = strip * rw + row), loads before __syncwarp
+        // x FIR in place: S[y][xo] = sum_s vr[s] S[y][xo + s].  A warp owns whole
+        // rows (ly0 + warp, + NWARPS, ...); its lanes take consecutive (row,
+        // strip) pairs of those rows, 32 per pass.  Strip g writes columns
+        // [8g, 8g + 8) and reads columns >= 8g, so a row's strips in increasing
+        // order across passes, with loads before __syncwarp, never read a
+        // column that an earlier store of the row has overwritten.
         if (ly0 <= ly1) {
             float vr[K];
 #pragma unroll
             for (int s = 0; s < K; ++s) vr[s] = P.vr[s];
-            const int rw = ns8 >= 32 ? 1 : 32 / ns8;     // rows per warp
-            const int spw = 32 / rw;                    // strips per warp pass
-            const int r = lane % rw, sidx = lane / rw;
-            for (int ry = ly0 + warp * rw; ry <= ly1; ry += NWARPS * rw) {
-                const int y = ry + r;
-                float4* row = reinterpret_cast<float4*>(S) + (y - ys) * bp4;
-                for (int gs = 0; gs < ns8; gs += spw) {
-                    const int gi = gs + sidx;           // strip, box-relative
-                    const bool act = sidx < spw && gi < ns8 && y <= ly1;
-                    float w[4 * NW];
-                    if (act) {
+            const int nr = ly1 - ly0 + 1;
+            const int nri = warp < nr ? (nr - 1 - warp) / NWARPS + 1 : 0;   // rows of this warp
+            const int npairs = nri * ns8;
+            const int di = 32 / ns8, dg = 32 % ns8;
+            int ri = lane / ns8, gi = lane % ns8;       // the lane's pair: row index, strip
+            for (int q0 = 0; q0 < npairs; q0 += 32) {
+                const bool act = q0 + lane < npairs;
+                float4* row = reinterpret_cast<float4*>(S) + (ly0 + warp + NWARPS * ri - ys) * bp4;
+                float w[4 * NW];
+                if (act) {
 #pragma unroll
-                        for (int m = 0; m < NW; ++m) {
-                            const float4 f = row[2 * gi + m];
-                            w[4 * m] = f.x; w[4 * m + 1] = f.y; w[4 * m + 2] = f.z; w[4 * m + 3] = f.w;
-                        }
+                    for (int m = 0; m < NW; ++m) {
+                        const float4 f = row[2 * gi + m];
+                        w[4 * m] = f.x; w[4 * m + 1] = f.y; w[4 * m + 2] = f.z; w[4 * m + 3] = f.w;
                     }
-                    __syncwarp();
-                    if (act) {
-                        float o[8];
+                }
+                __syncwarp();
+                if (act) {
+                    float o[8];
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            float acc = 0.f;
+                    for (int q = 0; q < 8; ++q) {
+                        float acc = 0.f;
 #pragma unroll
-                            for (int s = 0; s < K; ++s) acc += vr[s] * w[q + s];
-                            o[q] = acc;
-                        }
-                        row[2 * gi] = make_float4(o[0], o[1], o[2], o[3]);
-                        row[2 * gi + 1] = make_float4(o[4], o[5], o[6], o[7]);
+                        for (int s = 0; s < K; ++s) acc += vr[s] * w[q + s];
+                        o[q] = acc;
                     }
-                    __syncwarp();
+                    row[2 * gi] = make_float4(o[0], o[1], o[2], o[3]);
+                    row[2 * gi + 1] = make_float4(o[4], o[5], o[6], o[7]);
+                }
+                __syncwarp();
+                ri += di;
+                gi += dg;
+                if (gi >= ns8) {
+                    gi -= ns8;
+                    ++ri;
                 }
             }
         }
