@@ -217,9 +217,9 @@ __device__ __forceinline__ double sat_box(const double* T, int ld, int y0, int y
 //     the rows that the y FIR reads is zeroed;
 //   - x FIR in place, a warp per row, its lanes on consecutive (row, strip)
 //     pairs of its rows, 8 outputs per lane window;
-//   - y FIR in place, 8 x 4 outputs per item, ascending rounds of whole 8-row
-//     groups (an output row only overwrites an input row that no later output
-//     of the pass reads);
+//   - y FIR in place, 8 x 4 outputs per item, ascending rounds of (8-row
+//     group, column) items (an output row only overwrites an input row that
+//     no later output of the pass reads);
 //   - crop, residual (objective.hpp:7-31) and r^2 streamed from shared memory
 //     against the data.
 // The zero-model residual outside the box comes from the summed-area table.
@@ -411,27 +411,28 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
         __syncthreads();
         // y FIR in place: model(yo, xo) = sum_t ur[t] S[yo + t][xo], written to S row yo.
         // Packed FP32 pairs (FFMA2: two lanes of fma, each rounded as fmaf),
-        // columns (x, x+1) and (x+2, x+3) of a float4 per instruction
+        // columns (x, x+1) and (x+2, x+3) of a float4 per instruction.  Items
+        // (8-row group, float4 column) in ascending order, KB_THREADS x KB_IT
+        // per round, loads before the round's barrier and stores after it: a
+        // column's group is written only after every lower group of that
+        // column, the only readers of its rows, has loaded them.
         {
             float2 u2[K];
 #pragma unroll
             for (int t = 0; t < K; ++t) u2[t] = make_float2(P.ur[t], P.ur[t]);
-            const int gmax = max(1, KB_THREADS * KB_IT / ns4);  // row groups per round at most
-            const int rounds = (ng + gmax - 1) / gmax;
-            const int gpr = (ng + rounds - 1) / rounds;         // balanced rounds
-            for (int gr0 = 0; gr0 < ng; gr0 += gpr) {
-                const int nitems = min(gpr, ng - gr0) * ns4;
+            const int nitems = ng * ns4;
+            for (int gr0 = 0; gr0 < nitems; gr0 += KB_THREADS * KB_IT) {
                 float2 acc[KB_IT][8][2];
 #pragma unroll
                 for (int it = 0; it < KB_IT; ++it) {
-                    const int item = threadIdx.x + it * KB_THREADS;
+                    const int item = gr0 + threadIdx.x + it * KB_THREADS;
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
                         acc[it][q][0] = make_float2(0.f, 0.f);
                         acc[it][q][1] = make_float2(0.f, 0.f);
                     }
                     if (item < nitems) {
-                        const int rb = 8 * (gr0 + item / ns4), s4 = item % ns4;
+                        const int rb = 8 * (item / ns4), s4 = item % ns4;
                         const float4* colp = reinterpret_cast<const float4*>(S) + rb * bp4 + s4;
 #pragma unroll
                         for (int m = 0; m < K + 7; ++m) {
@@ -451,9 +452,9 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
                 __syncthreads();
 #pragma unroll
                 for (int it = 0; it < KB_IT; ++it) {
-                    const int item = threadIdx.x + it * KB_THREADS;
+                    const int item = gr0 + threadIdx.x + it * KB_THREADS;
                     if (item < nitems) {
-                        const int rb = 8 * (gr0 + item / ns4), s4 = item % ns4;
+                        const int rb = 8 * (item / ns4), s4 = item % ns4;
 #pragma unroll
                         for (int q = 0; q < 8; ++q)
                             if (ys + rb + q < ye)
