@@ -188,3 +188,42 @@ def test_batched_nodewise_fast_path_matches_generic(gpu):
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
     assert np.array_equal(out[0][2], out[1][2]) and np.array_equal(out[0][0], out[0][2])
+
+
+@pytest.mark.parametrize('size,psf_fwhm,lsf_fwhm', [
+    ((37, 33, 20), 2.0, 1.0),       # odd width: the scalar residual path, short FIRs
+    ((90, 70, 40), 5.0, 3.0),       # long FIRs, boxes wider than 32 strips' worth of lanes
+    ((61, 128, 28), 3.0, 2.0),      # tall planes, many row groups per y-FIR round
+])
+def test_batched_direct_box_shapes(gpu, oracle_built, size, psf_fwhm, lsf_fwhm):
+    """Direct mode over box shapes that exercise the kernels' lane mappings
+    (x FIR (row, strip) pairs, y FIR (row group, column) rounds, odd widths):
+    model cube and chi^2 against the fp64 oracle."""
+    import torch
+    from oracle.oracle import chi2, scube_pipeline
+    from gbkfit_b200 import psflsf, workloads
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    nx, ny, nz = size
+    w = workloads.smdisk_batch128(nsets=3, size=size, nnodes=10)
+    w.geom = workloads.Geometry(size, w.geom.step, (0, 0, (nz - 1) / 2), (0, 0, 0),
+                                psflsf.PSFGauss(psflsf.gauss_fwhm_to_sigma(psf_fwhm)),
+                                psflsf.LSFGauss(psflsf.gauss_fwhm_to_sigma(lsf_fwhm * 10.0)))
+    w.params['xpos'] = np.array([nx / 2, nx / 3, 2 * nx / 3])
+    w.params['ypos'] = np.array([ny / 2, 2 * ny / 3, ny / 3])
+    w.extra['truth']['xpos'], w.extra['truth']['ypos'] = nx / 2, ny / 2
+    data, err, _ = synthetic_data(w)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=3, conv='direct')
+    assert ev.conv_mode == 'direct'
+    bufs = ev.alloc_inputs(3)
+    ev.upload(ev.pack(w.params, 3), bufs, 3)
+    model = torch.full((3,) + tuple(size[::-1]), 7.0, device='cuda')
+    got = ev.evaluate_device(bufs, 3, model=model).cpu().numpy()
+    model = model.cpu().numpy()
+    for i in range(3):
+        p = w.disk.pack(workloads.set_params(w, i))
+        ref = scube_pipeline(p, w.geom)
+        ref32 = scube_pipeline(p, w.geom, precision='f32')
+        assert rel_err(model[i], ref) <= max(1e-5, 1.5 * rel_err(ref32, ref)), i
+        assert not np.any(model[i] == 7.0), i
+        c_ref = chi2(ref, data, err)
+        assert abs(got[i] - c_ref) / c_ref < 1e-4, (i, got[i], c_ref)
