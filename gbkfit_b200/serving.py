@@ -107,7 +107,7 @@ class Request:
         self.arrival = arrival
         self.admit = self.done = None
         self.future = Future()
-        self.blob = self.layout = self.args = None
+        self.blob = self.layout = self.args = self.ds = None
 
     def prepare(self):
         """Pack the parameters (Disk.pack, and the cloud budget of mcdisk)
@@ -238,6 +238,8 @@ class ModelServer:
         return ds
 
     def unregister(self, key):
+        """Drop a dataset; requests already submitted against it still run
+        (each holds its dataset until it completes)."""
         with self._cv:
             ds = self.datasets.pop(key)
             self._resident -= ds.footprint
@@ -246,7 +248,8 @@ class ModelServer:
     def submit(self, request):
         """Queue a Request; returns its Future (result: dict(chi2=..., and
         model=(nz, ny, nx) array when want_model))."""
-        if request.dataset not in self.datasets:
+        ds = self.datasets.get(request.dataset)
+        if ds is None:
             raise KeyError(f"unknown dataset {request.dataset!r}")
         if request.arrival is None:
             request.arrival = time.perf_counter()
@@ -254,7 +257,10 @@ class ModelServer:
             request.prepare()
         if request.blob.size > _Slot.STAGE:
             raise ValueError("the request's parameter arrays exceed the staging buffer")
-        request.args = request.serve_args(self.datasets[request.dataset])
+        # the request holds its dataset: the native arguments point into the
+        # dataset's device buffers until the request completes
+        request.ds = ds
+        request.args = request.serve_args(ds)
         with self._cv:
             if self._error is not None:
                 raise RuntimeError("the serving loop stopped") from self._error
@@ -322,7 +328,7 @@ class ModelServer:
                             if not free or not self._queue:
                                 break
                             req = self._queue[0]
-                            need = self.datasets[req.dataset].request_footprint()
+                            need = req.ds.request_footprint()
                             if self._resident + self._inflight + need > self.budget and \
                                     self._inflight > 0:
                                 break
@@ -345,7 +351,7 @@ class ModelServer:
                     r.future.set_exception(e)
 
     def _launch(self, slot, req, need):
-        ds = self.datasets[req.dataset]
+        ds = req.ds
         req.admit = time.perf_counter()
         slot.req, slot.bytes = req, need
         lay, total = ds.request_layout()
@@ -370,8 +376,8 @@ class ModelServer:
         out = dict(chi2=float(slot.out[0]))
         if req.want_model:
             buf, o = slot.keep
-            n = int(np.prod(self.datasets[req.dataset].geom.size))
-            nx, ny, nz = self.datasets[req.dataset].geom.size
+            n = int(np.prod(req.ds.geom.size))
+            nx, ny, nz = req.ds.geom.size
             out['model'] = buf[o:o + 4 * n].view(torch.float32).reshape(nz, ny, nx).cpu().numpy()
         rc = 0
         if int(slot.status[0]):
@@ -379,6 +385,7 @@ class ModelServer:
             # uid): the context's synchronize reports and clears it
             rc = _lib.gbkb200_ctx_synchronize(slot.ctx.handle)
         req.done = time.perf_counter()
+        req.ds = req.args = None        # the dataset may go once no request holds it
         with self._cv:
             self._inflight -= slot.bytes
             slot.req, slot.keep, slot.bytes = None, None, 0

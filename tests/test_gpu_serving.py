@@ -97,3 +97,27 @@ def test_unknown_dataset_and_budget_errors(gpu):
             srv.register(d['key'], d['geom'], d['data'], d['error'])
         with pytest.raises(KeyError):
             srv.submit(Request(123, 'smdisk', d['smdisk'], stream.requests[0]['params']))
+
+
+def test_unregister_keeps_submitted_requests(gpu):
+    """Datasets dropped while their requests are queued or running: each
+    request holds its dataset's device buffers until it completes, and the
+    results equal those of the same requests run before."""
+    import gc
+    from gbkfit_b200.serving import ModelServer
+    stream = _small_stream(n=16, seed=13)
+    kinds = [q['kind'] for q in stream.requests][:10]
+    with ModelServer(slots=4) as srv:
+        _register(srv, stream)
+        ref = [f.result()['chi2'] for f in [srv.submit(r) for r in _requests(stream)[:10]]]
+        futs = [srv.submit(r) for r in _requests(stream)[:10]]
+        for d in stream.datasets:
+            srv.unregister(d['key'])
+        gc.collect()
+        got = [f.result()['chi2'] for f in futs]
+        assert srv.datasets == {}
+    for k, a, b in zip(kinds, ref, got):
+        if k == 'smdisk':
+            assert a == b
+        else:
+            assert abs(a - b) <= 1e-5 * abs(a)
