@@ -62,10 +62,25 @@ def direct_flops_per_eval(geom):
     return 2 * (kz * nz * wx * wy + kx * nz * wy * nx + ky * nz * ny * nx)
 
 
-# DRAM bytes (read + write) per evaluation of the direct-mode kernels
-# (ka_lines_lsf + k_xr_transpose + kb_psf_residual), from the ncu capture in
-# profiles/kernels_smdisk_batch128_direct.md (one 128-set launch each, / 128)
-DIRECT_TRAFFIC_PER_EVAL = 4.2e6
+# DRAM bytes (read + write) per parameter set of each direct-mode kernel, from
+# one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of a 128-set
+# wave of this workload, divided by 128; a launch of n sets moves about n times
+# this (the traffic grows with the sets processed).  Not measured by this run.
+NCU_DRAM_BYTES_PER_SET = {
+    'kb_psf_residual': 289.1e6 / 128,
+    'ka_lines_lsf': 211.5e6 / 128,
+    'k_xr_transpose': 36.5e6 / 128,
+}
+
+# FLOPs of one residual voxel computed from the model: (m - d), x w, r^2 sum
+RESIDUAL_FLOPS = 3
+
+
+def fp32_peak_tflops(clocks):
+    """Nominal FP32 CUDA-core peak at the sampled SM clock: 148 SMs x 128
+    lanes x 2 FLOP (one fused multiply-add) per clock."""
+    mhz = clocks.get('sm_mhz') or clocks.get('sm_max_mhz') or 1965.0
+    return 148 * 128 * 2 * mhz * 1e6 / 1e12, mhz
 
 
 class ClockSampler:
@@ -153,18 +168,96 @@ def barrier(world):
         dist.barrier()
 
 
-def fp32_roof(geom, nsets, ms_step, clocks, conv):
-    """Direct mode: dense FIR FLOPs per step over the nominal FP32 CUDA-core
-    peak at the sampled SM clock (148 SMs x 128 lanes x 2 FLOP)."""
-    if conv != 'direct':
-        return None
-    mhz = clocks.get('sm_mhz') or clocks.get('sm_max_mhz') or 1965.0
-    peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
-    ach = direct_flops_per_eval(geom) * nsets / (ms_step / 1e3) / 1e12
-    return dict(achieved=round(ach, 2), peak=round(peak, 1), unit='TFLOP/s',
-                frac=round(ach / peak, 3), peak_kind='nominal at the sampled SM clock',
-                basis='dense FIR FLOPs per evaluation (LSF + PSF x + PSF y), '
-                      f'{direct_flops_per_eval(geom)} per evaluation')
+def roofline_direct(kernels, counters, steps, nsets, clocks, geom, ms_step):
+    """Roofline of the dominant direct-mode kernel (the PSF FIR + residual
+    kernel): the FLOPs it executed (PSF x and y FIR multiply-adds and residual
+    voxels, counted inside the kernel over the timed launches) per launch,
+    divided by its average launch time (CUDA events on its stream), against
+    the FP32 CUDA-core peak at the sampled clock.  The kernel computes in
+    FP32 on CUDA cores and moves little DRAM traffic (see `hbm_view`)."""
+    peak, mhz = fp32_peak_tflops(clocks)
+    name = 'kb_psf_residual'
+    k = kernels[name]
+    launches = k['launches_per_step'] * steps
+    fl_kb = (2 * (counters['psf_x_fma'] + counters['psf_y_fma'])
+             + RESIDUAL_FLOPS * counters['residual_voxels']) / launches
+    ach = fl_kb / (k['ms_per_launch'] / 1e3) / 1e12
+    sets_per_launch = nsets / k['launches_per_step']
+    traffic = NCU_DRAM_BYTES_PER_SET[name] * sets_per_launch
+    ka = kernels.get('ka_lines_lsf')
+    ka_view = None
+    if ka:
+        fl_ka = 2 * counters['lsf_fma'] / (ka['launches_per_step'] * steps)
+        ka_view = dict(kernel='ka_lines_lsf', executed_flops_per_launch=int(fl_ka),
+                       lines_per_launch=int(counters['lines'] / (ka['launches_per_step'] * steps)),
+                       achieved=round(fl_ka / (ka['ms_per_launch'] / 1e3) / 1e12, 2),
+                       frac=round(fl_ka / (ka['ms_per_launch'] / 1e3) / 1e12 / peak, 3))
+    step_bytes = sum(NCU_DRAM_BYTES_PER_SET[n] * nsets for n in NCU_DRAM_BYTES_PER_SET
+                     if n in kernels)
+    hbm, hbm_kind = peaks()
+    return dict(
+        bound='fp32-issue', kernel=name, achieved=round(ach, 2), peak=round(peak, 1),
+        unit='TFLOP/s', frac=round(ach / peak, 3),
+        peak_kind=f'nominal FP32 CUDA-core peak at the sampled SM clock ({mhz:.0f} MHz): '
+                  '148 SMs x 128 lanes x 2 FLOP',
+        executed_flops_per_launch=int(fl_kb), ms_per_launch=k['ms_per_launch'],
+        sets_per_launch=sets_per_launch,
+        basis='PSF x and y FIR multiply-adds (2 FLOP each) and residual voxels (3 FLOP each) '
+              'executed by the kernel, counted in-kernel over the timed launches',
+        traffic=round(traffic), traffic_unit='DRAM bytes per launch',
+        traffic_source='ncu capture of a 128-set wave of this workload, scaled to the '
+                       'sets of one launch (not measured by this run)',
+        model_kernel=ka_view, kernels=kernels, dominant=name,
+        hbm_view=dict(dram_bytes_per_step=round(step_bytes),
+                      achieved=round(step_bytes / (ms_step / 1e3) / 1e9, 1), peak=hbm,
+                      unit='GB/s', frac=round(step_bytes / (ms_step / 1e3) / 1e9 / hbm, 3),
+                      peak_kind=hbm_kind),
+        staged_equivalent=dict(
+            bytes_per_eval=staged_bytes_per_eval(geom),
+            basis='staged FFT pipeline with the reference padding '
+                  f'{list(geom.size_hi)}; the direct path does not move these bytes',
+            equivalent_gbs=round(staged_bytes_per_eval(geom) * nsets / (ms_step / 1e3) / 1e9, 1)),
+        dense_fir_equivalent_tflops=round(direct_flops_per_eval(geom) * nsets
+                                          / (ms_step / 1e3) / 1e12, 2))
+
+
+def roofline_fft(kernels, nsets, geom, ms_step):
+    """FFT mode: staged algorithmic bytes with the reference padding over
+    the step time, against the measured HBM bandwidth."""
+    hbm, peak_kind = peaks()
+    b_eval = staged_bytes_per_eval(geom)
+    achieved = b_eval * nsets / (ms_step / 1e3) / 1e9
+    return dict(bound='hbm', achieved=round(achieved, 1), peak=hbm, unit='GB/s',
+                frac=round(achieved / hbm, 3), traffic=None, peak_kind=peak_kind,
+                basis=f'staged algorithmic bytes per evaluation ({b_eval} B, reference '
+                      f'padding {list(geom.size_hi)}) x {nsets} / step time',
+                kernels=kernels, dominant=max(kernels, key=lambda k: kernels[k]['share']),
+                fft_tflops=round(fft_flops_per_eval(geom) * nsets / (ms_step / 1e3) / 1e12, 2))
+
+
+def parity_sample(ev, w, bufs, nsets, data, err, sets=(0, 255, 511)):
+    """Sampled parity of the benchmarked evaluator: model cubes and chi^2 of a
+    few sets against the fp64 oracle chain (normwise relative errors)."""
+    import torch
+    from oracle import oracle
+    from oracle.oracle import chi2 as chi2_ref, scube_pipeline
+    from gbkfit_b200 import workloads
+    if not os.path.exists(oracle.ORACLE_LIB):
+        oracle.build()
+    sets = [i for i in sets if i < nsets]
+    nx, ny, nz = w.geom.size
+    model = torch.zeros((nsets, nz, ny, nx), device=ev.dev)
+    c = ev.evaluate_device(bufs, nsets, model=model).cpu().numpy()
+    cubes = {i: model[i].cpu().numpy().astype(np.float64) for i in sets}
+    del model
+    errs, cerrs = [], []
+    for i in sets:
+        ref = scube_pipeline(w.disk.pack(workloads.set_params(w, i)), w.geom, precision='f64')
+        errs.append(float(np.max(np.abs(cubes[i] - ref)) / np.max(np.abs(ref))))
+        cr = chi2_ref(ref, data, err)
+        cerrs.append(abs(float(c[i]) - cr) / cr)
+    return dict(sets=sets, model_max_rel_err=max(errs), chi2_max_rel_err=max(cerrs),
+                vs='fp64 oracle (smdisk on the padded grid, FFT convolution, crop, chi^2)')
 
 
 def autotune(w, data, err, nsets, budget_s=60.0):
@@ -235,12 +328,12 @@ def run_b200(args):
         flush.fill_(float(i))
         ev.evaluate_device(bufs, nsets)
     stages = ev.stage_times()
+    counters = ev.work_counters()
     ev.set_timing(False)
     total = sum(t for t, _ in stages.values())
     kernels = {k: dict(launches_per_step=n / args.steps, ms_per_step=round(t / args.steps, 4),
                        ms_per_launch=round(t / n, 5), share=round(t / total, 4))
                for k, (t, n) in stages.items()}
-    dominant = max(kernels, key=lambda k: kernels[k]['share'])
 
     # end to end through the public API: host dicts -> pinned H2D -> chi^2 D2H
     ev_api = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
@@ -260,14 +353,16 @@ def run_b200(args):
 
     out = None
     if rank == 0:
-        hbm, peak_kind = peaks()
-        b_eval = staged_bytes_per_eval(w.geom)
-        achieved = b_eval * nsets / (ms_step / 1e3) / 1e9
         n_chunks = (nsets + ev.chunk - 1) // ev.chunk
         per_chunk = 3 if ev.conv_mode == 'direct' else 5
         plain = plain_per_call(w, data, err) if args.plain else None
         serving = serving_run() if args.serving else None
         cpu = cpu_baseline(w, data, err) if args.cpu_baseline else None
+        parity = parity_sample(ev, w, bufs, nsets, data, err) if args.parity else None
+        if ev.conv_mode == 'direct':
+            roof = roofline_direct(kernels, counters, args.steps, nsets, clocks, w.geom, ms_step)
+        else:
+            roof = roofline_fft(kernels, nsets, w.geom, ms_step)
         out = dict(
             metric=METRIC, value=round(value, 1), unit=UNIT, n_gpus=world, steps=args.steps,
             warmup=args.warmup, ms_per_step=round(ms_step, 4), higher_is_better=True,
@@ -279,18 +374,8 @@ def run_b200(args):
                         tuned=cfg, cuda_graph=use_graph, l2='flushed between steps (256 MB write)',
                         parallelism=f'dp{world} (independent parameter sets per GPU)'),
             e2e=e2e,
-            roofline=dict(bound='hbm', achieved=round(achieved, 1), peak=hbm,
-                          unit='GB/s', frac=round(achieved / hbm, 3),
-                          traffic=DIRECT_TRAFFIC_PER_EVAL if ev.conv_mode == 'direct' else None,
-                          traffic_unit='DRAM bytes per evaluation (ncu, direct-mode kernels)',
-                          peak_kind=peak_kind,
-                          basis=f'staged algorithmic bytes per evaluation ({b_eval} B, '
-                                f'reference padding {list(w.geom.size_hi)}) x {nsets} / step time '
-                                '(all kernels of the step)',
-                          kernels=kernels, dominant=dominant,
-                          fft_equiv_tflops=round(fft_flops_per_eval(w.geom) * nsets
-                                                 / (ms_step / 1e3) / 1e12, 2),
-                          fp32=fp32_roof(w.geom, nsets, ms_step, clocks, ev.conv_mode)),
+            roofline=roof,
+            parity=parity,
             clocks=clocks,
             gpu_launches=args.steps * (per_chunk * n_chunks + 1),
             plain_per_call=plain,
@@ -670,6 +755,8 @@ def main():
     ap.add_argument('--no-plain', dest='plain', action='store_false')
     ap.add_argument('--no-serving', dest='serving', action='store_false')
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
+    ap.add_argument('--no-parity', dest='parity', action='store_false',
+                    help='skip the sampled parity check against the fp64 oracle')
     ap.add_argument('--conv', choices=['fft', 'direct'], default=None,
                     help='force the convolution mode (default: tuned)')
     ap.add_argument('--chunk', type=int, default=0, help='force the sets per wave (default: tuned)')

@@ -59,9 +59,15 @@ _lib.gbkb200_batch_set_timing.argtypes = [c_void_p, c_int]
 _lib.gbkb200_batch_set_timing.restype = c_int
 _lib.gbkb200_batch_timing.argtypes = [c_void_p, ctypes.c_double * 6, c_int * 6]
 _lib.gbkb200_batch_timing.restype = c_int
+_lib.gbkb200_batch_counters.argtypes = [c_void_p, ctypes.c_ulonglong * 8]
+_lib.gbkb200_batch_counters.restype = c_int
 
 BATCH_EXPORTED = ['gbkb200_batch_create', 'gbkb200_batch_evaluate', 'gbkb200_batch_info',
-                  'gbkb200_batch_destroy', 'gbkb200_batch_set_timing', 'gbkb200_batch_timing']
+                  'gbkb200_batch_destroy', 'gbkb200_batch_set_timing', 'gbkb200_batch_timing',
+                  'gbkb200_batch_counters']
+
+# slots of gbkb200_batch_counters
+COUNTERS = ('lsf_fma', 'lines', 'psf_x_fma', 'psf_y_fma', 'residual_voxels', 'spaxels')
 
 # per-stage kernel names of gbkb200_batch_timing, by convolution mode
 STAGE_KERNELS = {
@@ -317,6 +323,13 @@ class BatchedSMDisk:
         check(_lib.gbkb200_batch_timing(self.handle, ms, n), 'batch_timing')
         names = STAGE_KERNELS[self.conv_mode]
         return {names[i]: (ms[i], n[i]) for i in range(6) if n[i]}
+
+    def work_counters(self):
+        """{counter: executed work} of the direct-mode kernels since the last
+        call, counted while timing is enabled (synchronises)."""
+        out = (ctypes.c_ulonglong * 8)()
+        check(_lib.gbkb200_batch_counters(self.handle, out), 'batch_counters')
+        return {n: int(out[i]) for i, n in enumerate(COUNTERS)}
 
     def close(self):
         if getattr(self, 'handle', None):

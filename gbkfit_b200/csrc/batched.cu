@@ -362,6 +362,7 @@ struct gbkb200_batch {
     void (*ka)(BatchKernelArgs, int*) = nullptr;
     // per-stage timing: event pairs recorded around launches while enabled
     int timing = 0;
+    unsigned long long* counters = nullptr;   // device, GBK_CTR_N (direct mode, timing on)
     std::vector<cudaEvent_t> ev;      // 2 per record
     std::vector<int> ev_stage;
     size_t ev_used = 0;
@@ -573,6 +574,7 @@ extern "C" int gbkb200_batch_destroy(gbkb200_batch* bt)
     cudaFree(bt->xrt);
     cudaFree(bt->sat);
     cudaFree(bt->iw);
+    cudaFree(bt->counters);
     for (cudaEvent_t e : bt->ev) cudaEventDestroy(e);
     delete bt;
     return GBKB200_OK;
@@ -778,6 +780,7 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
     }
     P.model = model;
     P.lim_model = model ? (long long)nsets * P.Nz * P.Ny * P.Nx : 0;
+    P.counters = bt->timing ? bt->counters : nullptr;
     const long long set_stride = (long long)P.Wz * P.Py * P.hx;
     const long long lim_spec = (long long)P.Pz * P.Py * P.hx;
     const int tiles = (P.hx + BLT - 1) / BLT;
@@ -845,6 +848,11 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
 extern "C" int gbkb200_batch_set_timing(gbkb200_batch* bt, int enable)
 {
     if (!bt) return GBKB200_ERR_INVALID_ARG;
+    if (enable && !bt->counters) {
+        if (cudaMalloc(&bt->counters, GBK_CTR_N * sizeof(unsigned long long)) != cudaSuccess)
+            return GBKB200_ERR_OOM;
+        GBK_CUDA_TRY(cudaMemset(bt->counters, 0, GBK_CTR_N * sizeof(unsigned long long)));
+    }
     bt->timing = enable ? 1 : 0;
     bt->ev_used = 0;
     bt->ev_error = 0;
@@ -870,4 +878,17 @@ extern "C" int gbkb200_batch_timing(gbkb200_batch* bt, double ms[GBKB200_BATCH_S
     bt->ev_used = 0;
     bt->ev_error = 0;
     return failed ? GBKB200_ERR_OOM : GBKB200_OK;
+}
+
+extern "C" int gbkb200_batch_counters(gbkb200_batch* bt, unsigned long long out[GBKB200_BATCH_COUNTERS])
+{
+    if (!bt || !out) return GBKB200_ERR_INVALID_ARG;
+    static_assert(GBK_CTR_N == GBKB200_BATCH_COUNTERS, "counter slots");
+    for (int i = 0; i < GBKB200_BATCH_COUNTERS; ++i) out[i] = 0;
+    if (!bt->counters) return GBKB200_OK;
+    GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
+    GBK_CUDA_TRY(cudaMemcpy(out, bt->counters, GBK_CTR_N * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost));
+    GBK_CUDA_TRY(cudaMemset(bt->counters, 0, GBK_CTR_N * sizeof(unsigned long long)));
+    return GBKB200_OK;
 }

@@ -47,6 +47,20 @@ struct BatchKernelArgs {
                           // each plane row chunk (4-aligned around it is written), or -1
     int* xrt;             // (chunk, Nz, Wy, nch): the same, plane-major (read by the PSF kernel)
     const double* sat;    // (Nz, Ny + 1, Nx + 1): summed-area table of the zero-model r^2
+    // executed-work counters (null unless enabled): what the direct-mode kernels
+    // actually compute, for the roofline of the measured launches
+    unsigned long long* counters;   // [GBK_CTR_*]
+};
+
+// counters[] slots (FMA = one fused multiply-add of one lane)
+enum {
+    GBK_CTR_KA_FMA = 0,     // LSF FIR taps of the model kernel
+    GBK_CTR_KA_LINE = 1,    // line values (one exp each) of the model kernel
+    GBK_CTR_KB_XFMA = 2,    // PSF x FIR taps
+    GBK_CTR_KB_YFMA = 3,    // PSF y FIR taps
+    GBK_CTR_KB_VOX = 4,     // residual voxels computed from the model box
+    GBK_CTR_KA_SPAXEL = 5,  // spaxel evaluations
+    GBK_CTR_N = 8
 };
 
 // set b's per-set inputs: pointers offset from set 0 by the strides
@@ -188,6 +202,14 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
             }
         }
     }
+    if (P.counters && lane == 0) {
+        atomicAdd(&P.counters[GBK_CTR_KA_SPAXEL], 32ull);
+        if (zlo <= zhi) {
+            const unsigned long long n = (unsigned long long)(zhi - zlo + 1) * 32;
+            atomicAdd(&P.counters[GBK_CTR_KA_FMA], n * KZ);
+            atomicAdd(&P.counters[GBK_CTR_KA_LINE], n + (KZ - 1) * 32ull);
+        }
+    }
     if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
 }
 
@@ -321,11 +343,17 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
     const float4* src = reinterpret_cast<const float4*>(P.mplanes + prow * P.pitch);
     const int pbase = zo * P.Ny * P.Nx;       // the data cube has < 2^31 voxels
     float sum = 0.f;
+    unsigned long long c_x = 0, c_y = 0, c_v = 0;    // executed work (thread 0)
     for (int ys = yo_lo; ys < yb_end; ys += bo) {
         const int ye = min(yb_end, ys + bo);                 // outputs [ys, ye)
         const int ng = (ye - ys + 7) / 8;
         const int rend = ys + 8 * ng + K - 1;                // rows [ys, rend) are read
         const int ly0 = max(y0, ys), ly1 = min(y1, rend - 1);
+        if (P.counters && threadIdx.x == 0) {
+            if (ly0 <= ly1) c_x += (unsigned long long)(ly1 - ly0 + 1) * ns8 * 8 * K;
+            c_y += (unsigned long long)ng * ns4 * 32 * K;
+            c_v += (unsigned long long)(ye - ys) * (xb_end - xb0);
+        }
         // load rows [ly0, ly1]: each row chunk's nonzero range, zeros elsewhere
         if (ly0 <= ly1) {
             const int tc = min(nsl, KB_THREADS), tr = KB_THREADS / tc;
@@ -532,6 +560,11 @@ __global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs
         float s = 0.f;
         for (int w = 0; w < NWARPS; ++w) s += warp_part[w];
         P.partials[part] = (double)s + outside;
+        if (P.counters) {
+            atomicAdd(&P.counters[GBK_CTR_KB_XFMA], c_x);
+            atomicAdd(&P.counters[GBK_CTR_KB_YFMA], c_y);
+            atomicAdd(&P.counters[GBK_CTR_KB_VOX], c_v);
+        }
     }
 }
 

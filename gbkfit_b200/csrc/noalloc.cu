@@ -20,6 +20,8 @@
 // by the caller.
 #include "gbk_common.cuh"
 
+#include <cuda.h>
+
 #include <mutex>
 
 namespace {
@@ -33,10 +35,42 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_PARTIALS];
 
 // Device address of g_noalloc_partials per device, looked up once per device
-// (cudaGetSymbolAddress with that device current).  The name of the array is
-// only a host-side stand-in in host code; kernels get this address.
-double* g_partials_addr[NOALLOC_MAX_DEVICES] = {};
+// and context (cudaGetSymbolAddress with that device current).  The name of
+// the array is only a host-side stand-in in host code; kernels get this
+// address.  The context it was looked up in is kept beside it: when the
+// device's context is re-created (after cudaDeviceReset) the address is
+// looked up again instead of pointing into the old context.
+struct PartialsAddr {
+    CUcontext ctx;
+    double* addr;
+};
+PartialsAddr g_partials_addr[NOALLOC_MAX_DEVICES] = {};
 std::mutex g_setup_mutex;
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link-time
+// dependency on the driver library); null where it cannot be resolved
+CtxGetCurrentFn ctx_get_current()
+{
+    static const CtxGetCurrentFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return static_cast<CtxGetCurrentFn>(nullptr);
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    return fn;
+}
+
+CUcontext current_context()
+{
+    CUcontext c = nullptr;
+    const CtxGetCurrentFn fn = ctx_get_current();
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
 
 __device__ __forceinline__ float warp_sum(float v)
 {
@@ -87,12 +121,14 @@ int partials_address(double** out)
     GBK_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return GBKB200_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials_addr[dev]) {
+    PartialsAddr& e = g_partials_addr[dev];
+    if (!e.addr || current_context() != e.ctx) {
         void* p = nullptr;
-        GBK_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_partials));
-        g_partials_addr[dev] = static_cast<double*>(p);
+        GBK_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_partials));   // makes the context current
+        e.ctx = current_context();
+        e.addr = static_cast<double*>(p);
     }
-    *out = g_partials_addr[dev];
+    *out = e.addr;
     return GBKB200_OK;
 }
 

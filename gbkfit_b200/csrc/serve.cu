@@ -79,6 +79,10 @@ extern "C" int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serv
         if (a->size_hi[k] < 1 || a->size[k] < 1 || a->edge[k] < 0 ||
             a->edge[k] + a->size[k] > a->size_hi[k])
             return GBKB200_ERR_INVALID_ARG;
+    // sizes are checked before anything is enqueued on the stream
+    const long long vhi = (long long)a->size_hi[0] * a->size_hi[1] * a->size_hi[2];
+    if ((long long)a->size[0] * a->size[1] * a->size[2] >= (1ll << 31) || vhi >= (1ll << 31))
+        return GBKB200_ERR_TOO_LARGE;
     char* base = static_cast<char*>(a->blob_dev);
     auto at = [&](long long off) -> char* { return off < 0 ? nullptr : base + off; };
     const cudaStream_t st = ctx->stream;
@@ -87,7 +91,6 @@ extern "C" int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serv
         GBK_CUDA_TRY(cudaMemcpyAsync(a->blob_dev, a->blob_host, (size_t)a->blob_bytes,
                                      cudaMemcpyHostToDevice, st));
     }
-    const long long vhi = (long long)a->size_hi[0] * a->size_hi[1] * a->size_hi[2];
     GBK_CUDA_TRY(cudaMemsetAsync(a->scube, 0, (size_t)vhi * sizeof(float), st));
 #define GBK_T(k)                                                                                 \
     reinterpret_cast<const int*>(at(a->off_uids[k])),                                            \
@@ -127,7 +130,6 @@ extern "C" int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serv
     double* part = static_cast<double*>(ctx->serve_scratch);
     unsigned* counter = reinterpret_cast<unsigned*>(part + TAIL_BLOCKS);
     const long long n = (long long)a->size[0] * a->size[1] * a->size[2];
-    if (n >= (1ll << 31) || vhi >= (1ll << 31)) return GBKB200_ERR_TOO_LARGE;
     int blocks = (int)std::min<long long>(TAIL_BLOCKS, (n + 4 * TAIL_THREADS - 1) / (4 * TAIL_THREADS));
     serve_tail_kernel<<<blocks, TAIL_THREADS, 0, st>>>(
         a->scube, a->size_hi[0], a->size_hi[1], a->edge[0], a->edge[1], a->edge[2], a->size[0],

@@ -72,6 +72,8 @@ class Dataset:
                                            _ptr(self.spectrum)), 'fft_r2c')
         stream.synchronize()
         self.footprint = self.spectrum.numel() * 4 + 2 * 4 * int(np.prod(geom.size))
+        self.holders = 0        # submitted requests that have not completed
+        self.released = False   # unregistered
 
     def request_layout(self):
         """Byte offsets of one in-flight request's device buffers (padded
@@ -239,10 +241,13 @@ class ModelServer:
 
     def unregister(self, key):
         """Drop a dataset; requests already submitted against it still run
-        (each holds its dataset until it completes)."""
+        (each holds its dataset until it completes).  Its device bytes stay
+        counted against the budget until the last of them completes."""
         with self._cv:
             ds = self.datasets.pop(key)
-            self._resident -= ds.footprint
+            ds.released = True
+            if ds.holders == 0:
+                self._resident -= ds.footprint
 
     # ---- requests --------------------------------------------------------------
     def submit(self, request):
@@ -264,6 +269,9 @@ class ModelServer:
         with self._cv:
             if self._error is not None:
                 raise RuntimeError("the serving loop stopped") from self._error
+            if self.datasets.get(request.dataset) is not ds:
+                raise KeyError(f"dataset {request.dataset!r} was unregistered")
+            ds.holders += 1
             self._queue.append(request)
             self._cv.notify()
         return request.future
@@ -385,8 +393,12 @@ class ModelServer:
             # uid): the context's synchronize reports and clears it
             rc = _lib.gbkb200_ctx_synchronize(slot.ctx.handle)
         req.done = time.perf_counter()
+        ds = req.ds
         req.ds = req.args = None        # the dataset may go once no request holds it
         with self._cv:
+            ds.holders -= 1
+            if ds.released and ds.holders == 0:
+                self._resident -= ds.footprint
             self._inflight -= slot.bytes
             slot.req, slot.keep, slot.bytes = None, None, 0
             self._done.append(req)

@@ -191,8 +191,10 @@ int gbkb200_objective_residual_sum_f32(gbkb200_ctx* ctx, const float* residual, 
  * default stream) on the current device; sum (one device float) is ready
  * when the stream reaches that point.  The first call on a device looks up
  * the array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race and must be ordered by the caller. */
+ * before any stream capture.  After the device's context is re-created
+ * (cudaDeviceReset) the next call looks the address up again, so that
+ * call also belongs outside any capture.  All calls share the array: calls
+ * that overlap on the GPU race and must be ordered by the caller. */
 int gbkb200_objective_residual_sum_noalloc_f32(const float* residual, int size, int squared,
                                                float* sum, void* stream);
 
@@ -368,6 +370,16 @@ int gbkb200_batch_destroy(gbkb200_batch* b);
 int gbkb200_batch_set_timing(gbkb200_batch* b, int enable);
 int gbkb200_batch_timing(gbkb200_batch* b, double ms[GBKB200_BATCH_STAGES],
                          int launches[GBKB200_BATCH_STAGES]);
+/* Executed-work counters of the direct-mode kernels (no reference
+ * counterpart; a measurement aid), counted while timing is enabled:
+ * [0] LSF FIR multiply-adds, [1] line values (one exponential each),
+ * [2] PSF x FIR multiply-adds, [3] PSF y FIR multiply-adds, [4] residual
+ * voxels computed from the model box, [5] spaxel evaluations (one
+ * multiply-add is one lane's fused multiply-add).  Synchronizes the stream,
+ * returns the sums since the last call and resets them; all zero in FFT
+ * mode. */
+#define GBKB200_BATCH_COUNTERS 8
+int gbkb200_batch_counters(gbkb200_batch* b, unsigned long long out[GBKB200_BATCH_COUNTERS]);
 
 #ifdef __cplusplus
 }

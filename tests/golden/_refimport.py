@@ -2,11 +2,19 @@
 generation, with stand-ins for the modules it imports but the model path does
 not use (astropy, ruamel.yaml, pandas) and for its generated version file."""
 
+import os
 import sys
 import types
 
 
-def import_reference(src='/root/reference/src'):
+def reference_src():
+    """src/ of the GBKFIT checkout the fixtures are generated from:
+    $GBKFIT_REFERENCE/src, else the checkout of the build container."""
+    return os.path.join(os.environ.get('GBKFIT_REFERENCE', '/root/reference'), 'src')
+
+
+def import_reference(src=None):
+    src = src or reference_src()
     if src not in sys.path:
         sys.path.insert(0, src)
 

@@ -156,7 +156,7 @@ def capture(D, T, name, kw, rn, params, loose, tilted, mc=False):
     return out
 
 
-def main(src='/root/reference/src'):
+def main(src=None):
     from _refimport import import_reference
     import_reference(src)
     import gbkfit.model.gmodels._disk as D
