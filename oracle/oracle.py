@@ -206,6 +206,11 @@ class Reference(_Lib):
     def num_threads(self):
         return self.lib.ref_num_threads()
 
+    def set_num_threads(self, n):
+        """OpenMP threads of the following calls (one thread: the reference's
+        mcdisk draws all clouds from one mt19937 stream seeded 42)."""
+        self.lib.ref_set_num_threads(int(n))
+
     def smdisk_evaluate(self, packed, geom, outs):
         args, keep = disk_arglist(packed, geom, outs, np.float32)
         self.lib.ref_smdisk_evaluate_f32(*args)

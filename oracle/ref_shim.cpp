@@ -189,5 +189,8 @@ void ref_wcube_evaluate_f32(int sx, int sy, int sz, int spec_z, const float* spa
 }
 
 int ref_num_threads(void) { return omp_get_max_threads(); }
+// threads of the following calls (1: the reference's mcdisk draws every cloud
+// from one mt19937 stream seeded 42, host/kernels.hpp:239-242)
+void ref_set_num_threads(int n) { omp_set_num_threads(n); }
 
 }  // extern "C"

@@ -267,8 +267,16 @@ def test_mcdisk_flux_and_clouds(be, oracle_built):
     assert n_gpu > 0.5 * nclouds
     assert abs(n_gpu - n_orc) <= 1e-4 * nclouds
     diff = np.abs(rd - oh['rdata'])
-    assert np.sum(diff > 0.5 * per_cloud) <= 1e-3 * nclouds
-    assert rel_err(outs['scube'].cpu().numpy(), oh['scube']) < 1e-2
+    moved = int(np.sum(diff > 0.5 * per_cloud))       # ~2 voxels per cloud that moved
+    assert moved <= 1e-3 * nclouds
+    # scube: a cloud that landed in another spaxel moves its whole line (its
+    # spectral sum is at most 1.5 x per_cloud / dz for these line widths);
+    # every other cloud differs by fp32 rounding of its line only
+    sg = outs['scube'].cpu().numpy().astype(np.float64)
+    so = oh['scube'].astype(np.float64)
+    line_sum = 1.5 * per_cloud / g['spec_step']
+    assert np.abs(sg - so).sum() <= moved * line_sum + 1e-5 * np.abs(so).sum()
+    assert abs(sg.sum() - so.sum()) <= moved * line_sum + 1e-5 * abs(so.sum())
 
 
 def test_mcdisk_deterministic_mode(be, oracle_built):
