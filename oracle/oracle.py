@@ -428,3 +428,46 @@ def chi2_gradient_f64(packed, geom, data, error, scale):
     grad[g0 + 3] = np.deg2rad(np.sum(np.where(on, dphi, 0.0)))
     grad[g0 + 4] = np.deg2rad(np.sum(np.where(on, di, 0.0)))
     return chi2, grad, dscale
+
+
+def dcube_pipeline(packed, size, step, rpix, rval, scale, psf, lsf, precision='f64',
+                   mask_cutoff=None, mask_apply=False, thick=False):
+    """The reference's DCube chain with supersampling and masking
+    (_dcube.py:128-313): the padded high-resolution grid (size x scale +
+    kernel - 1, padded by backend.py:51-66), smdisk on it, FFT convolution
+    with the rolled PSF x LSF cube sampled at the high-resolution step, the
+    downscale of the crop (dmodels.hpp:8-46, host/kernels.hpp:55-80) and the
+    mask (dmodels.hpp:49-74).  psf/lsf are gbkfit_b200.psflsf objects (their
+    arrays are pinned to the reference's by the golden fixtures).  Returns
+    (dcube_lo, mcube_lo or None)."""
+    from gbkfit_b200.workloads import dcube_geometry
+    o = Oracle(precision)
+    real = o.real
+    zero, size_hi, step_hi, zero_hi, edge, ksize = dcube_geometry(size, step, rpix, rval, scale,
+                                                                  psf, lsf)
+    sx, sy, sz = size_hi
+    if thick:
+        i = int(sx < sy)
+        spat = ((sx, sy, (sx, sy)[i]), (step_hi[0], step_hi[1], step_hi[i]),
+                (zero_hi[0], zero_hi[1], -((sx, sy)[i] / 2 - 0.5) * step_hi[i]))
+    else:
+        spat = ((sx, sy, 1), (step_hi[0], step_hi[1], 0.0), (zero_hi[0], zero_hi[1], 0.0))
+    g = dict(loose=False, tilted=False, spat_size=spat[0], spat_step=spat[1],
+             spat_zero=spat[2], spec_size=sz, spec_step=step_hi[2], spec_zero=zero_hi[2],
+             opacity=None)
+    cube = np.zeros((sz, sy, sx), real)
+    o.smdisk_evaluate(packed, g, dict(scube=cube))
+    if psf is not None or lsf is not None:
+        from gbkfit_b200 import psflsf as P
+        off = [(n % 2) - 1 for n in size_hi]
+        p = (psf or P.PSFPoint()).asarray(step_hi[:2], (sx, sy), (off[0], off[1]))
+        l_ = (lsf or P.LSFPoint()).asarray(step_hi[2], sz, off[2])
+        pc = (p * l_[:, None, None]).astype(real)
+        pc = np.roll(pc, np.array(pc.shape) // 2 + 1, axis=(0, 1, 2))
+        cube = fft_convolve_cached(cube, pc).astype(real)
+    nx, ny, nz = size
+    lo = o.dcube_downscale(scale, edge, cube, (nz, ny, nx))
+    mcube = None
+    if mask_cutoff is not None:
+        lo, mcube = o.dcube_mask(mask_cutoff, mask_apply, lo)
+    return lo, mcube

@@ -1,0 +1,136 @@
+"""GPU smdisk over the whole trait catalogue and the disk branches the
+configurations do not reach, through the drop-in gmodel backend (C ABI):
+
+* every trait uid of every kind (tests/trait_catalogue.py), thin and thick,
+  against the fp64 oracle and the fp32 restatement (which the catalogue test
+  on the CPU pins to the compiled reference);
+* loose and tilted disks (ring_info, gmodels.hpp:218-323), thick disks with
+  truncated node-wise heights and two-trait harmonic disks with a selection
+  trait, against the reference's own outputs (tests/golden/cubes.npz);
+* opacity: the emission of a thick disk attenuated by an opacity cube
+  (gmodels.hpp:933-937).
+
+Tolerances as in test_gpu_parity: GPU error against fp64 <= max(1e-5, 1.5 x
+the fp32 CPU path's own error), GPU against the fp32 path within the sum of
+both errors; velocity and dispersion maps where both are finite."""
+
+import os
+
+import numpy as np
+import pytest
+
+from tests import trait_catalogue as C
+from tests.helpers import gpu_smdisk, rel_err, upload
+
+pytestmark = pytest.mark.gpu
+
+CASES = C.cases()
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+
+
+@pytest.fixture(scope='module')
+def gm(gpu):
+    from gbkfit_b200.driver import DriverB200
+    return DriverB200(0).backends().gmodel(np.float32)
+
+
+def _gpu_outputs(gm, packed, geo, opacity=None):
+    import torch
+    h = C.host_outputs(geo, np.float32)
+    d = {k: torch.from_numpy(v).cuda() for k, v in h.items()}
+    g = dict(geo)
+    if opacity is not None:
+        g['opacity'] = torch.from_numpy(opacity).cuda()
+    gpu_smdisk(gm, upload(packed, 'cuda'), g, d)
+    return {k: v.cpu().numpy() for k, v in d.items()}
+
+
+def _check(gpu, o64, o32, name):
+    for k in C.OUTS:
+        x = np.asarray(gpu[k], np.float64)
+        y = np.asarray(o64[k], np.float64)
+        z = np.asarray(o32[k], np.float64)
+        fx, fy = np.isfinite(x), np.isfinite(y)
+        if name in C.STUB_HEIGHTS:
+            assert np.array_equal(fx, np.isfinite(z)), (name, k)
+            assert np.array_equal(x[fx] == 0, z[fx] == 0), (name, k)
+            continue
+        assert np.array_equal(fx, fy), (name, k)
+        m = fx & fy
+        e64, e32, cpu = rel_err(x[m], y[m]), rel_err(x[m], z[m]), rel_err(z[m], y[m])
+        assert e64 <= max(1e-5, 1.5 * cpu), (name, k, e64, cpu)
+        assert e32 <= max(1e-5, e64 + cpu + 1e-6), (name, k, e32, e64, cpu)
+
+
+@pytest.mark.parametrize('case', CASES, ids=[c[0] for c in CASES])
+def test_gpu_catalogue(gm, oracle_built, case):
+    from oracle.oracle import Oracle
+    name, traits, params, thick = case
+    geo = C.geometry(thick)
+    packed = C.disk_of(case).pack(params)
+    got = _gpu_outputs(gm, packed, geo)
+    o64 = C.host_outputs(geo, np.float64)
+    o32 = C.host_outputs(geo, np.float32)
+    Oracle('f64').smdisk_evaluate(packed, geo, o64)
+    Oracle('f32').smdisk_evaluate(packed, geo, o32)
+    if name not in C.STUB_HEIGHTS:
+        assert np.max(o64['scube']) > 0
+    _check(got, o64, o32, name)
+
+
+def _golden_cases():
+    from tests.test_golden import _cases
+    return [c for c in _cases()]
+
+
+@pytest.mark.parametrize('case', [c[0] for c in _golden_cases()])
+def test_gpu_golden_cases_vs_reference_outputs(gm, oracle_built, case):
+    """Loose/tilted, thick (sech2; gauss with truncated node-wise heights) and
+    multi-trait disks against the compiled reference's own fixtures."""
+    from oracle.oracle import Oracle
+    from tests.test_golden import _GEOMS, _disk
+    cubes = dict(np.load(os.path.join(GOLDEN, 'cubes.npz')))
+    name, traits, params, loose, tilted = [c for c in _golden_cases() if c[0] == case][0]
+    thick = name.startswith('thick')
+    geo = dict(_GEOMS['thick' if thick else 'thin'], loose=loose, tilted=tilted, opacity=None)
+    packed = _disk(traits, loose, tilted).pack(params)
+    got = _gpu_outputs(gm, packed, geo)
+    o64 = C.host_outputs(geo, np.float64)
+    Oracle('f64').smdisk_evaluate(packed, geo, o64)
+    for k in ('scube', 'rdata'):
+        ref = cubes[f'{name}/{k}'].astype(np.float64)
+        cpu = rel_err(ref, o64[k])        # the reference's own fp32 error
+        assert ref.max() > 0
+        assert rel_err(got[k], o64[k]) <= max(1e-5, 1.5 * cpu), (name, k)
+        assert rel_err(got[k], ref) <= max(1e-5, 2.5 * cpu + 1e-6), (name, k)
+    for k in ('vdata_cmp', 'ddata_cmp'):
+        ref = cubes[f'{name}/{k}']
+        m = np.isfinite(ref)
+        assert np.array_equal(m, np.isfinite(got[k])), (name, k)
+        assert rel_err(got[k][m], ref[m]) <= 1e-5, (name, k)
+
+
+def test_gpu_opacity(gm, oracle_built):
+    """A thick disk's emission attenuated by an opacity cube: every spaxel's
+    flux is multiplied by (1 - opacity) of each voxel in front of it."""
+    from oracle.oracle import Oracle
+    from gbkfit_b200 import traits as T
+    from gbkfit_b200.disk import Disk
+    traits = dict(rpt=[T.bpt('exponential')], rht=[T.bht('sech2')], vpt=[T.vpt('tan_arctan')],
+                  vht=[T.vht_one()], dpt=[T.dpt('uniform')], dht=[T.dht_one()])
+    d = Disk(False, False, C.RNODES, traits=traits)
+    params = dict(C.BASE, bpt_a=1.0, bpt_s=8.0, bht_s=1.5, vpt_rt=4.0, vpt_vt=200.0, dpt_a=20.0)
+    geo = C.geometry(True)
+    sx, sy, sz = geo['spat_size']
+    rng = np.random.default_rng(4)
+    opacity = (0.3 * rng.random((sz, sy, sx))).astype(np.float32)
+    packed = d.pack(params)
+    got = _gpu_outputs(gm, packed, geo, opacity)
+    plain = _gpu_outputs(gm, packed, geo)
+    o64 = C.host_outputs(geo, np.float64)
+    o32 = C.host_outputs(geo, np.float32)
+    Oracle('f64').smdisk_evaluate(packed, dict(geo, opacity=opacity.astype(np.float64)), o64)
+    Oracle('f32').smdisk_evaluate(packed, dict(geo, opacity=opacity), o32)
+    _check(got, o64, o32, 'opacity')
+    # the attenuation is visible: less flux than without opacity
+    assert got['scube'].sum() < 0.9 * plain['scube'].sum()
