@@ -272,9 +272,15 @@ def run_b200(args):
     import torch
     from gbkfit_b200 import workloads
     from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    from gbkfit_b200.sharded import ShardedEvaluator, shard_sets, slice_sets
     rank, world, local = setup_dist(args)
     nsets = args.nsets
-    w = workloads.smdisk_batch128(nsets=nsets, seed=1234 + rank)
+    # one batch of nsets x world sets (the same seeded draw on every rank);
+    # rank r evaluates its contiguous share of nsets sets
+    total = nsets * world
+    w = workloads.smdisk_batch128(nsets=total, seed=1234)
+    lo, hi = shard_sets(total, rank, world)
+    mine = slice_sets(w.params, total, lo, hi)
     data, err, _ = synthetic_data(w, device=local)
     cfg = autotune(w, data, err, nsets, budget_s=args.tune_budget) if args.tune else {}
     if args.conv:
@@ -287,7 +293,7 @@ def run_b200(args):
         cfg['band'] = args.band
     ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
     bufs = ev.alloc_inputs(nsets)
-    ev.upload(ev.pack(w.params, nsets), bufs, nsets)
+    ev.upload(ev.pack(mine, nsets), bufs, nsets)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
     use_graph = not args.no_graph
@@ -335,21 +341,29 @@ def run_b200(args):
                        ms_per_launch=round(t / n, 5), share=round(t / total, 4))
                for k, (t, n) in stages.items()}
 
-    # end to end through the public API: host dicts -> pinned H2D -> chi^2 D2H
+    # end to end through the public API: every rank takes the whole batch of
+    # host parameter dicts, packs and copies its share (pinned H2D), evaluates
+    # it, reads its chi^2 back (D2H) and gathers all chi^2 values (NCCL
+    # all_gather across the ranks)
     ev_api = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
+    sharded = ShardedEvaluator(ev_api)
     d2h = nsets * 4
     for _ in range(max(1, args.warmup)):
-        ev_api.evaluate(w.params, nsets)
+        sharded.evaluate(w.params, total)
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        ev_api.evaluate(w.params, nsets)
+        chi2_all = sharded.evaluate(w.params, total)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, world)
+    assert len(chi2_all) == total and np.all(np.isfinite(chi2_all))
     h2d = int(ev_api.last_h2d_bytes)     # pinned input pieces copied per call
-    e2e = dict(value=world * nsets / e2e_s, unit=UNIT, h2d_bytes_per_step=h2d,
-               d2h_bytes_per_step=d2h, ms_per_step=e2e_s * 1e3)
+    e2e = dict(value=total / e2e_s, unit=UNIT, h2d_bytes_per_step=h2d,
+               d2h_bytes_per_step=d2h, ms_per_step=e2e_s * 1e3,
+               gather_bytes_per_step=sharded.last_gather_bytes,
+               path='ShardedEvaluator(BatchedSMDisk).evaluate: host parameter dicts of all '
+                    f'{total} sets in, chi^2 of all sets out on every rank')
 
     out = None
     if rank == 0:
@@ -372,7 +386,8 @@ def run_b200(args):
                         nsets_per_gpu=nsets, conv=ev.conv_mode, psf_rank=ev.psf_rank,
                         fft_grid=list(ev.fft_size), chunk=ev.chunk,
                         tuned=cfg, cuda_graph=use_graph, l2='flushed between steps (256 MB write)',
-                        parallelism=f'dp{world} (independent parameter sets per GPU)'),
+                        parallelism=f'dp{world} (parameter sets sharded across GPUs, '
+                                    'chi^2 all_gather)'),
             e2e=e2e,
             roofline=roof,
             parity=parity,

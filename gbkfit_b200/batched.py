@@ -77,12 +77,7 @@ STAGE_KERNELS = {
 }
 
 
-def shard_sets(nsets, rank, world):
-    """Contiguous [lo, hi) share of nsets parameter sets for one rank (the
-    multi-GPU path evaluates independent sets per GPU, no data exchange)."""
-    base, extra = divmod(int(nsets), int(world))
-    lo = rank * base + min(rank, extra)
-    return lo, lo + base + (1 if rank < extra else 0)
+from .sharded import shard_sets  # noqa: E402,F401  (the per-rank share; see sharded.py)
 
 
 def kernel_boxes(geom):

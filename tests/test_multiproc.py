@@ -1,15 +1,23 @@
-"""Multi-process (gloo, world size 2, CPU) tests of the sharded objective:
-parameter sets are split across ranks with shard_sets, every rank scores its
-own sets (the oracle stands in for the GPU here), and gathering the chi^2
-values reproduces the single-process result exactly.  A rank that fails
-before joining the gather is detected by the others through the process
-group's timeout."""
+"""Multi-process (gloo, world size 2, CPU) tests of the sharded objective
+(gbkfit_b200.sharded.ShardedEvaluator): every rank evaluates its share of
+the parameter sets and the chi^2 of all sets is gathered to every rank.  On
+the CPU an oracle-backed evaluator stands in for each rank's GPU evaluator
+(the same interface as BatchedSMDisk: evaluate(params, nsets), max_sets);
+the sharding, the slicing of the per-set parameters, the padding and the
+gather are the product's.
+
+* sharded chi^2 == the single-process chi^2, exactly, for uneven shares and
+  batches larger than one rank's max_sets;
+* emcee's vectorised log-probability (fitting.BatchedLogProbability) on top of
+  the sharded evaluator gives every rank the same values;
+* parameters held by one rank reach the others (broadcast_theta);
+* a rank that fails before the gather is detected by the others through the
+  process group's timeout."""
 
 import os
 import socket
 
 import numpy as np
-import pytest
 
 
 def _free_port():
@@ -20,40 +28,67 @@ def _free_port():
     return p
 
 
-def _chi2_of_sets(lo, hi):
-    from oracle.oracle import chi2, scube_pipeline
+def _problem():
+    from oracle.oracle import scube_pipeline
     from gbkfit_b200 import workloads
-    w = workloads.smdisk_batch128(nsets=6, size=(24, 20, 16), nnodes=8)
+    w = workloads.smdisk_batch128(nsets=7, size=(24, 20, 16), nnodes=8)
     truth = w.disk.pack(w.extra['truth'])
     m = scube_pipeline(truth, w.geom)
     rng = np.random.default_rng(w.extra['noise_seed'])
     sigma = 0.02 * float(np.max(m))
     data = m + rng.normal(0, sigma, m.shape)
     err = np.full(m.shape, sigma)
-    return [chi2(scube_pipeline(w.disk.pack(workloads.set_params(w, i)), w.geom), data, err)
-            for i in range(lo, hi)]
+    return w, data, err
+
+
+class OracleEvaluator:
+    """The per-rank evaluator interface of BatchedSMDisk, scored by the fp64
+    oracle (test stand-in for a rank's GPU)."""
+
+    def __init__(self, w, data, err, max_sets=2):
+        self.w, self.data, self.err, self.max_sets = w, data, err, max_sets
+        self.calls = []
+
+    def evaluate(self, params, nsets):
+        from oracle.oracle import chi2, scube_pipeline
+        assert nsets <= self.max_sets
+        self.calls.append(nsets)
+        out = []
+        for i in range(nsets):
+            p = {k: (np.asarray(v)[i] if np.ndim(v) and np.shape(v)[0] == nsets else v)
+                 for k, v in params.items()}
+            out.append(chi2(scube_pipeline(self.w.disk.pack(p), self.w.geom), self.data,
+                            self.err))
+        return np.array(out)
 
 
 def _worker(rank, world, port, out, fail_rank):
-    import torch
-    import torch.distributed as dist
     import datetime
-    from gbkfit_b200.batched import shard_sets
+    import torch.distributed as dist
+    from gbkfit_b200 import fitting
+    from gbkfit_b200.sharded import ShardedEvaluator, broadcast_theta
     os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port))
     dist.init_process_group('gloo', rank=rank, world_size=world,
                             timeout=datetime.timedelta(seconds=20))
     try:
         if rank == fail_rank:
             raise RuntimeError('injected failure before the gather')
-        lo, hi = shard_sets(6, rank, world)
-        mine = torch.tensor(_chi2_of_sets(lo, hi) + [0.0] * (3 - (hi - lo)), dtype=torch.float64)
-        parts = [torch.zeros(3, dtype=torch.float64) for _ in range(world)]
-        dist.all_gather(parts, mine)
-        vals = []
-        for r in range(world):
-            a, b = shard_sets(6, r, world)
-            vals += parts[r][:b - a].tolist()
-        out.put((rank, 'ok', vals))
+        w, data, err = _problem()
+        local = OracleEvaluator(w, data, err, max_sets=2)
+        sh = ShardedEvaluator(local)
+        chi2 = sh.evaluate(w.params, 7)
+        # the sampler-side objective over the sharded evaluator: theta held by
+        # rank 0 only, broadcast to the others
+        template = {k: (np.asarray(v)[0] if np.ndim(v) and np.shape(v)[0] == 7 else v)
+                    for k, v in w.params.items()}
+        fp = fitting.FreeParams(template, {'incl': fitting.PriorUniform(10, 85),
+                                           'vpt_vt[3]': fitting.PriorUniform(0, 400)})
+        theta = np.stack([w.params['incl'], w.params['vpt_vt'][:, 3]], axis=1) \
+            if rank == 0 else None
+        theta = broadcast_theta(theta, src=0, ndim=2)
+        post, blobs = fitting.BatchedLogProbability(sh, fp)(theta)
+        out.put((rank, 'ok', dict(chi2=chi2.tolist(), post=post.tolist(), calls=local.calls,
+                                  share=sh.share(7), theta=theta.tolist())))
     except Exception as e:
         out.put((rank, 'error', type(e).__name__))
     finally:
@@ -74,15 +109,32 @@ def _run(world, fail_rank=-1):
     res = [q.get(timeout=180) for _ in ps]
     for p in ps:
         p.join(timeout=60)
-    return sorted(res)
+    return sorted(res, key=lambda r: r[0])
 
 
 def test_sharded_chi2_equals_single_process(oracle_built):
+    from gbkfit_b200 import fitting
+    from gbkfit_b200.sharded import ShardedEvaluator
+    w, data, err = _problem()
+    single_ev = OracleEvaluator(w, data, err, max_sets=7)
+    single = ShardedEvaluator(single_ev).evaluate(w.params, 7)     # world 1: no gather
     res = _run(2)
-    single = _chi2_of_sets(0, 6)
-    for rank, status, vals in res:
-        assert status == 'ok'
-        assert np.allclose(vals, single, rtol=0, atol=0)
+    for rank, status, got in res:
+        assert status == 'ok', got
+        assert np.array_equal(np.array(got['chi2']), single)
+        assert got['share'] == [(0, 4), (4, 7)][rank]
+        # shares of 4 and 3 sets, in calls of at most max_sets = 2
+        assert got['calls'][:2] == ([2, 2] if rank == 0 else [2, 1])
+    theta = np.stack([w.params['incl'], w.params['vpt_vt'][:, 3]], axis=1)
+    assert np.array_equal(np.array(res[1][2]['theta']), theta)
+    template = {k: (np.asarray(v)[0] if np.ndim(v) and np.shape(v)[0] == 7 else v)
+                for k, v in w.params.items()}
+    fp = fitting.FreeParams(template, {'incl': fitting.PriorUniform(10, 85),
+                                       'vpt_vt[3]': fitting.PriorUniform(0, 400)})
+    post_single, _ = fitting.BatchedLogProbability(single_ev, fp)(theta)
+    for rank, status, got in res:
+        assert np.allclose(got['post'], post_single, rtol=1e-12, atol=0)
+    assert res[0][2]['post'] == res[1][2]['post']
 
 
 def test_failed_rank_is_detected(oracle_built):
