@@ -404,29 +404,28 @@ def run_b200(args):
     return out
 
 
-def serving_run(nrequests=10000, slots=8, load=0.8):
+def serving_run(nrequests=10000, slots=8, load=0.8, batch_sets=16):
     """The serving stream (workloads.serving_stream: 64 datasets, 70 % smdisk /
     30 % mcdisk, sides 32-256 px, 32-192 channels, 1e5-1e7 clouds): capacity
-    with every request queued at once, then Poisson arrivals at `load` x
-    capacity; latency = completion - scheduled arrival."""
+    with every request submitted at once, then Poisson arrivals at `load` x
+    capacity; latency = completion - scheduled arrival, and includes the
+    packing of the request's parameters (in submit).  Every dataset is
+    registered with its smdisk disk, so its smdisk requests are coalesced
+    into batched launches (direct separable convolution, up to batch_sets
+    sets each)."""
     import torch
     from gbkfit_b200 import workloads
     from gbkfit_b200.serving import ModelServer, Request
     st = workloads.serving_stream(nrequests=nrequests, ndatasets=64, rate=1.0, seed=7)
 
     def reqs():
-        out = []
-        for q in st.requests:
-            d = st.datasets[q['dataset']]
-            r = Request(q['dataset'], q['kind'], d[q['kind']], q['params'], cflux=q['cflux'],
-                        thick=q['thick'])
-            r.prepare()
-            out.append(r)
-        return out
+        return [Request(q['dataset'], q['kind'], st.datasets[q['dataset']][q['kind']],
+                        q['params'], cflux=q['cflux'], thick=q['thick']) for q in st.requests]
 
     with ModelServer(slots=slots, hbm_budget=40 << 30) as srv:
         for d in st.datasets:
-            srv.register(d['key'], d['geom'], d['data'], d['error'])
+            srv.register(d['key'], d['geom'], d['data'], d['error'], smdisk=d['smdisk'],
+                         batch_sets=batch_sets)
         [f.result() for f in [srv.submit(r) for r in reqs()[:300]]]     # plans, allocator
         srv.stats(reset=True)
         [f.result() for f in [srv.submit(r) for r in reqs()]]
@@ -445,10 +444,12 @@ def serving_run(nrequests=10000, slots=8, load=0.8):
         [f.result() for f in futs]
         s = srv.stats(reset=True)
         resident = srv._resident
-    return dict(requests=nrequests, slots=slots, capacity_evals_per_s=round(cap, 1),
+    return dict(requests=nrequests, slots=slots, batch_sets=batch_sets,
+                max_group=s.get('max_group'), capacity_evals_per_s=round(cap, 1),
                 offered_evals_per_s=round(rate, 1), evals_per_s=round(s['evals_per_s'], 1),
                 p50_ms=round(s['p50_ms'], 3), p99_ms=round(s['p99_ms'], 3),
                 max_ms=round(s['max_ms'], 3), resident_gb=round(resident / 1e9, 3),
+                latency='completion - arrival, parameter packing included',
                 workload='serving_stream: 64 datasets (sides log-U 32-256 px, channels '
                          'log-U 32-192, PSF FWHM U(1.5,4) px, LSF FWHM U(1,3) ch), '
                          '70% smdisk / 30% mcdisk (1e5-1e7 clouds), chi^2 per request')
@@ -669,9 +670,33 @@ def run_mcdisk(args):
                 cpu_baseline=cpu)
 
 
+def _c0_reference_eval(ref, w0, pcube, workers):
+    """One plain smdisk evaluation with the reference's own CPU code: smdisk
+    (oracle/_ref, OpenMP) on the padded 96^3 grid, the FFT convolution with
+    scipy (standing in for FFTW, which is not installed), the crop and the
+    moment maps 0/1/2 (oracle/_ref).  Returns (maps, cube)."""
+    from oracle.oracle import fft_convolve_cached
+    g = w0.geom
+    ga = w0.geometry_args()
+    hh = np.zeros((ga['spec_size'], ga['spat_size'][1], ga['spat_size'][0]), np.float32)
+    ref.smdisk_evaluate(w0.disk.pack(w0.params), ga, dict(scube=hh))
+    conv = fft_convolve_cached(hh, pcube, dtype=np.float32, workers=workers)
+    ex, ey, ez = g.edge
+    nx, ny, nz = g.size
+    cube = np.ascontiguousarray(conv[ez:ez + nz, ey:ey + ny, ex:ex + nx], np.float32)
+    zero = (0.0, 0.0, -(nz - 1) / 2 * g.step[2])
+    maps = ref.mmaps_moments(g.size, g.step, zero, cube, None, 1e-6, np.array([0, 1, 2], np.int32))
+    return maps, cube
+
+
 def run_smdisk64(args):
-    """smdisk_cube64: the reference-style per-call drop-in path (DModelSCube
-    + smdisk, one synchronous call chain) on a 64^3 cube."""
+    """smdisk_cube64, the plain configuration end to end: thin smdisk on the
+    64^3 cube -> PSF x LSF FFT convolution on the padded 96^3 grid -> crop ->
+    moment maps 0, 1, 2 and the full cube, through the drop-in DModelMMaps
+    (one synchronous call chain per evaluation, the reference's semantics),
+    host parameters in, host maps and cube out.  The reference's CPU code for
+    the same chain (OpenMP smdisk and moments from oracle/_ref, scipy's FFT
+    standing in for FFTW) is timed beside it on the host cores."""
     import torch
     from gbkfit_b200 import model as M, workloads
     from gbkfit_b200.driver import DriverB200
@@ -680,39 +705,61 @@ def run_smdisk64(args):
     comp = M.SpectralSMDisk2D(False, False, w0.disk.traits['rpt'], w0.disk.traits['vpt'],
                               w0.disk.traits['dpt'], rnodes=w0.disk.rnodes)
     g0 = w0.geom
-    dm = M.DModelSCube(g0.size, g0.step, rpix=(0, 0, (g0.size[2] - 1) / 2), rval=(0, 0, 0),
-                       psf=g0.psf, lsf=g0.lsf)
+    dm = M.DModelMMaps(g0.size, g0.step, rpix=(0, 0, (g0.size[2] - 1) / 2), rval=(0, 0, 0),
+                       psf=g0.psf, lsf=g0.lsf, orders=(0, 1, 2))
     mdl = M.Model(drv, dm, M.GModelKinematics2D([comp]))
+
+    def call():
+        out = mdl.evaluate_d(w0.params)
+        maps = [out[f'mmap{o}']['d'].cpu().numpy() for o in (0, 1, 2)]
+        cube = dm.dcube().dcube().cpu().numpy()
+        return maps, cube
+
     for _ in range(args.warmup):
-        mdl.evaluate_d(w0.params)
+        call()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        mdl.evaluate_d(w0.params)
-    torch.cuda.synchronize()
+        maps, cube = call()
     ms = (time.perf_counter() - t0) / args.steps * 1e3
+    # device time of the same chain (CUDA events around the call, L2 flushed)
+    dev_ms = _events_ms(lambda: mdl.evaluate_d(w0.params), args.steps, args.warmup)
     cpu = None
+    parity = None
     if args.cpu_baseline:
         from oracle.oracle import Reference, build
         if not Reference.available():
             build()
         ref = Reference()
-        ga = w0.geometry_args()
-        hh = np.zeros((ga['spec_size'], ga['spat_size'][1], ga['spat_size'][0]), np.float32)
+        workers = os.cpu_count()
+        pcube = g0.pcube(np.float32)
+        (rd, _, _), rcube = _c0_reference_eval(ref, w0, pcube, workers)
+        n = max(3, args.steps)
         t0 = time.perf_counter()
-        for _ in range(5):
-            hh[:] = 0
-            ref.smdisk_evaluate(w0.disk.pack(w0.params), ga, dict(scube=hh))
-        cpu = dict(value=round(5 / (time.perf_counter() - t0), 2), unit='evals/s',
-                   cores=ref.num_threads(), kind='reference',
-                   sample='5 smdisk calls into the 96^3 padded cube (model stage only)')
-    return dict(metric='smdisk_cube64 drop-in model evaluations/s (per call, synchronous)',
+        for _ in range(n):
+            _c0_reference_eval(ref, w0, pcube, workers)
+        dt = (time.perf_counter() - t0) / n
+        cpu = dict(value=round(1 / dt, 2), unit='evals/s', cores=ref.num_threads(),
+                   kind='reference', ms_per_eval=round(dt * 1e3, 3),
+                   sample=f'{n} evaluations of the same chain: smdisk + moments from the '
+                          'reference templates (OpenMP), scipy.fft (all cores) for the FFT')
+        v = np.isfinite(rd[0])
+        parity = dict(vs='the reference CPU chain (fp32)',
+                      cube_rel_err=float(np.max(np.abs(cube - rcube)) / np.max(np.abs(rcube))),
+                      map_rel_err=[float(np.max(np.abs(maps[i][v] - rd[i][v]))
+                                         / np.max(np.abs(rd[i][v]))) for i in range(3)])
+    return dict(metric='smdisk_cube64 evaluations/s (smdisk -> PSF/LSF FFT -> moments 0/1/2 '
+                       '+ cube, per call, synchronous)',
                 value=round(1e3 / ms, 1), unit='evals/s', n_gpus=1, steps=args.steps,
-                warmup=args.warmup, ms_per_step=round(ms, 4), higher_is_better=True,
-                dtype='f32', data='synthetic',
-                config=dict(workload='smdisk_cube64: 64^3 cube, 20 nodes, Gaussian PSF x LSF, '
-                                     'padded 96^3', path='Model.evaluate_d (DModelSCube)'),
-                cpu_baseline=cpu)
+                warmup=args.warmup, ms_per_step=round(ms, 4), device_ms=round(dev_ms, 4),
+                higher_is_better=True, dtype='f32', data='synthetic',
+                config=dict(workload='smdisk_cube64: 64^3 cube, 20 nodes, Gaussian PSF FWHM 2.5 px '
+                                     'x LSF FWHM 2 ch, padded 96^3, moments 0/1/2',
+                            path='Model.evaluate_d (DModelMMaps), host maps + cube out'),
+                e2e=dict(value=round(1e3 / ms, 1), unit='evals/s',
+                         h2d_bytes_per_step=None,
+                         d2h_bytes_per_step=int(3 * 64 * 64 * 4 + 64 ** 3 * 4)),
+                cpu_baseline=cpu, parity=parity)
 
 
 def run_grad96(args):

@@ -288,6 +288,37 @@ class BatchedSMDisk:
         self._e2e = st
         return st
 
+    # ---- asynchronous groups (serving) ----------------------------------------
+    def pack_one(self, params):
+        """One parameter set (host dict) -> {name: float32 row} in the layout
+        of the evaluator's inputs (what pack() gives for one set)."""
+        one = {k: np.asarray(v)[None] for k, v in params.items()}
+        return {k: v[0] for k, v in self.pack(one, 1).items() if v.size}
+
+    def submit_rows(self, rows):
+        """Enqueue one evaluation of len(rows) parameter sets (rows from
+        pack_one) on the evaluator's stream: the rows are gathered into a
+        pinned buffer, copied to the device in one transfer, evaluated, and
+        chi^2 is copied back to pinned memory.  Returns (event, chi2 host
+        tensor view); chi2 is valid once the event has completed.  One
+        submission may be in flight per evaluator (the next one reuses its
+        buffers): the caller waits for the event before submitting again."""
+        n = len(rows)
+        if not 0 < n <= self.max_sets:
+            raise ValueError(f"a group of {n} sets (max_sets {self.max_sets})")
+        st = self._e2e_buffers(self.max_sets, 1)
+        hv, hflat, dflat, dv = st['pieces'][0]
+        for name, arr in hv.items():
+            arr[:n] = np.stack([r[name] for r in rows])
+        with torch.cuda.stream(self.stream):
+            dflat.copy_(hflat, non_blocking=True)
+            self.evaluate_device(dv, n)
+            out = st['chi2'][:n]
+            out.copy_(self.chi2[:n], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+        return ev, out
+
     def capture(self, bufs, nsets):
         """Capture one evaluate_device call for nsets sets in a CUDA graph."""
         s = torch.cuda.Stream(self.dev)

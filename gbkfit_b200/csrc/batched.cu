@@ -444,7 +444,7 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     P.disk.zy = d->spat_zero[1] + ty * d->spat_step[1];
     P.disk.spec_zero = d->spec_zero + tz * d->spec_step;
     P.K = std::max(KB_KMIN, std::max(P.Kx, P.Ky) | 1);
-    if (P.K > KB_KMAX || P.Kz > KA_KMAX || P.Nx > 4 * KB_THREADS * KB_IT || P.Wx > 1024 ||
+    if (P.K > KB_KMAX || P.Kz > KA_KMAX || P.Nx > KB_NX_MAX || P.Wx > 1024 ||
         (long long)P.Nx * P.Ny * P.Nz >= (1LL << 31))
         return GBKB200_ERR_UNSUPPORTED;
     const int NW = (P.K + 7 + 3) / 4;
@@ -492,6 +492,7 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
         P.vr[i] = i < P.K ? vr[i] : 0.f;
         P.ur[i] = i < P.K ? ur[i] : 0.f;
         P.lsfr[i] = i < P.Kz ? lr[i] : 0.f;
+        P.ur2[i] = make_float2(P.ur[i], P.ur[i]);
     }
     if (cudaMalloc(&bt->mplanes, nrows * P.pitch * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&bt->xr, nrows * P.nch * sizeof(int)) != cudaSuccess ||
@@ -755,8 +756,22 @@ extern "C" int gbkb200_batch_info(const gbkb200_batch* bt, int fft_size[3], int*
         fft_size[0] = bt->P.Px; fft_size[1] = bt->P.Py; fft_size[2] = bt->P.Pz;
     }
     if (chunk) *chunk = bt->chunk;
-    if (work_bytes)
-        *work_bytes = (size_t)bt->chunk * bt->P.Wz * bt->P.Py * bt->P.hx * sizeof(float2);
+    if (work_bytes) {
+        // device bytes the evaluator holds (its scratch, tables and partials)
+        const BatchKernelArgs& P = bt->P;
+        size_t b = (size_t)bt->max_sets * bt->nper * sizeof(double);
+        if (bt->direct) {
+            const size_t nrows = (size_t)bt->chunk * P.Nz * P.Wy;
+            b += nrows * P.pitch * sizeof(float) + 2 * nrows * P.nch * sizeof(int) +
+                 (size_t)P.Nz * (P.Ny + 1) * (P.Nx + 1) * sizeof(double) +
+                 (size_t)P.Nz * P.Ny * P.Nx * sizeof(float);
+        } else {
+            b += (size_t)bt->chunk * P.Wz * P.Py * P.hx * sizeof(float2) +
+                 (size_t)P.Pz * P.Py * P.hx * sizeof(float2) +
+                 (size_t)(P.Px / 2 + P.Py + P.Pz + P.hx) * sizeof(float2);
+        }
+        *work_bytes = b;
+    }
     return GBKB200_OK;
 }
 

@@ -46,10 +46,18 @@ __global__ void mask_kernel(float cutoff, int apply, long long n, float* d, floa
 }
 
 // dmodels.hpp:76-228, one thread per (x, y) pixel; adjacent threads read
-// adjacent x, so every spectral step is a coalesced row read.  The sums are
-// accumulated in the reference's order (channel 0 upwards, fp32, with the
-// second and higher moments' terms promoted to double as std::pow(T, int)
-// does there).  mm receives the mask map, mw the weight map.
+// adjacent x, so every spectral step is a coalesced row read, and orders 0-2
+// (and the weight map) read the column once:
+// * m0 = sum d dz in fp32, channel 0 upwards, as the reference sums it (the
+//   mask |m0| > cutoff and the m0 map are the reference's, bit for bit);
+// * fp64 running sums S0 = sum d dz, S1 = sum d v dz, S2 = sum d v^2 dz and
+//   SW = sum w d dz give m1 = S1 / S0, m2 = sqrt(S2 / S0 - m1^2) (the centred
+//   second moment, exact in fp64 for these magnitudes) and the weight map
+//   SW / m0; the reference's fp32 sums round at ~1e-7 relative, these at
+//   ~1e-16;
+// * orders >= 3 take a second pass over the column with (v - m1)^k in fp64,
+//   without dz, divided by m0, as the reference does.
+// mm receives the mask map, mw the weight map.
 __global__ void moments_kernel(int nx, int ny, int nz, float stz, float zz, const float* d,
                                const float* w, float cutoff, int norders, const int* orders,
                                float* md, float* mm, float* mw)
@@ -59,37 +67,46 @@ __global__ void moments_kernel(int nx, int ny, int nz, float stz, float zz, cons
     if (x >= nx) return;
     const long long i2 = x + (long long)nx * y, sxy = (long long)nx * ny;
     const int maxo = orders[norders - 1];
-    int m = 0;
     float m0s = 0;
-    for (int z = 0; z < nz; ++z) m0s += d[i2 + sxy * z] * stz;
+    double s0 = 0, s1 = 0, s2 = 0, sw = 0;
+    const float* dp = d + i2;
+    const float* wp = w ? w + i2 : nullptr;
+#pragma unroll 4
+    for (int z = 0; z < nz; ++z) {
+        const float dv = dp[sxy * z];
+        const float ddz = dv * stz;
+        m0s += ddz;
+        const double v = (double)(zz + z * stz);
+        const double a = (double)ddz;
+        s0 += a;
+        s1 += a * v;
+        s2 += a * v * v;
+        if (wp) sw += (double)wp[sxy * z] * a;
+    }
     const bool valid = fabsf(m0s) > cutoff;
     mm[i2] = valid ? 1.f : 0.f;
     const float m0 = valid ? m0s : NAN;
+    if (w) mw[i2] = valid ? (float)(sw / (double)m0s) : NAN;
+    int m = 0;
     if (orders[m] == 0) { md[i2 + sxy * m] = m0; m++; }
-    if (w) {
-        float ws = 0;
-        for (int z = 0; valid && z < nz; ++z) ws += w[i2 + sxy * z] * d[i2 + sxy * z] * stz / m0;
-        mw[i2] = valid ? ws : NAN;
-    }
     if (maxo == 0) return;
-    float m1s = 0;
-    for (int z = 0; valid && z < nz; ++z) m1s += d[i2 + sxy * z] * (zz + z * stz) * stz;
-    const float m1 = valid ? m1s / m0 : NAN;
-    if (orders[m] == 1) { md[i2 + sxy * m] = m1; m++; }
+    const double m1d = s1 / s0;
+    const float m1 = valid ? (float)m1d : NAN;
+    if (m < norders && orders[m] == 1) { md[i2 + sxy * m] = m1; m++; }
     if (maxo == 1) return;
-    float m2s = 0;
-    for (int z = 0; valid && z < nz; ++z) {
-        double dv = (double)((zz + z * stz) - m1);
-        m2s = (float)((double)m2s + (double)d[i2 + sxy * z] * (dv * dv) * (double)stz);
-    }
-    const float m2 = valid ? sqrtf(m2s / m0) : NAN;
-    if (orders[m] == 2) { md[i2 + sxy * m] = m2; m++; }
+    const double var = fmax(s2 / s0 - m1d * m1d, 0.0);
+    const float m2 = valid ? (float)sqrt(var) : NAN;
+    if (m < norders && orders[m] == 2) { md[i2 + sxy * m] = m2; m++; }
     for (; m < norders; ++m) {
-        float mns = 0;
-        for (int z = 0; valid && z < nz; ++z)
-            mns = (float)((double)mns +
-                          (double)d[i2 + sxy * z] * pow((double)((zz + z * stz) - m1), orders[m]));
-        md[i2 + sxy * m] = valid ? mns / m0 : NAN;
+        double mns = 0;
+        const int k = orders[m];
+        for (int z = 0; valid && z < nz; ++z) {
+            const double t = (double)((zz + z * stz) - m1);
+            double p = t;
+            for (int e = 1; e < k; ++e) p *= t;
+            mns += (double)dp[sxy * z] * p;
+        }
+        md[i2 + sxy * m] = valid ? (float)(mns / (double)m0s) : NAN;
     }
 }
 

@@ -24,8 +24,17 @@ optionally, its model cube).
   copies of chi^2 and the kernel status word to pinned host memory; the
   argument block is filled in the submitting thread, so the scheduler only
   sets the slot's buffers and makes the call.
+* Coalescing: a dataset registered with its smdisk disk and a separable
+  (rank-1) PSF keeps a batched evaluator of that disk (direct separable
+  convolution, gbkb200_batch_*).  Its queued smdisk requests are packed into
+  per-set parameter rows when they are submitted and started together, up
+  to the evaluator's batch, whenever the evaluator is idle: one H2D copy of
+  the rows, one batched evaluation, one D2H copy of chi^2 on the dataset's
+  own stream.  Each request's chi^2 does not depend on the others of its
+  launch (per-set partial sums in a fixed order).
 * Latency: completion minus arrival (the submit time, or the arrival time a
-  caller passes).  ``ModelServer.stats()`` gives p50/p99 and throughput.
+  caller passes); the packing of the parameters happens in submit, after
+  the arrival.  ``ModelServer.stats()`` gives p50/p99 and throughput.
 """
 
 import collections
@@ -56,9 +65,16 @@ def _cbytes(size_hi):
 class Dataset:
     """A registered dataset: geometry (workloads.Geometry, with PSF/LSF),
     data and error cubes (nz, ny, nx); resident on the device with the
-    PSF x LSF spectrum of its FFT grid."""
+    PSF x LSF spectrum of its FFT grid.
 
-    def __init__(self, key, geom, data, error, ctx, dev, stream):
+    smdisk: optionally, the thin smooth disk (gbkfit_b200.disk.Disk) that
+    smdisk requests against this dataset use; when its PSF is separable
+    (rank 1, e.g. a circular Gaussian) the dataset keeps a batched evaluator
+    of that disk (direct separable convolution, batch_sets sets per launch,
+    its own stream) and queued smdisk requests of that disk are coalesced
+    into its launches."""
+
+    def __init__(self, key, geom, data, error, ctx, dev, stream, smdisk=None, batch_sets=16):
         self.key, self.geom = key, geom
         f32 = lambda a: None if a is None else torch.as_tensor(
             np.ascontiguousarray(a, np.float32)).to(dev)
@@ -74,6 +90,16 @@ class Dataset:
         self.footprint = self.spectrum.numel() * 4 + 2 * 4 * int(np.prod(geom.size))
         self.holders = 0        # submitted requests that have not completed
         self.released = False   # unregistered
+        self.smdisk, self.batched = smdisk, None
+        self.group = None       # (event, chi2 host view, requests) of the launch in flight
+        if smdisk is not None and not smdisk.traits['rht'] and batch_sets > 0:
+            from .batched import BatchedSMDisk, kernel_boxes, separable_factors
+            if separable_factors(kernel_boxes(geom)[0])[0] == 1:
+                self.batched = BatchedSMDisk(
+                    smdisk, geom, self.obs, self.err, max_sets=int(batch_sets),
+                    chunk=int(batch_sets), conv='direct', device=dev.index,
+                    stream=torch.cuda.Stream(dev))
+                self.footprint += self.batched.work_bytes + 4 * self.batched.max_sets
 
     def request_layout(self):
         """Byte offsets of one in-flight request's device buffers (padded
@@ -110,6 +136,7 @@ class Request:
         self.admit = self.done = None
         self.future = Future()
         self.blob = self.layout = self.args = self.ds = None
+        self.rows = None        # packed parameter row of a coalesced smdisk request
 
     def prepare(self):
         """Pack the parameters (Disk.pack, and the cloud budget of mcdisk)
@@ -220,16 +247,21 @@ class ModelServer:
         self._inflight = 0          # in-flight request bytes
         self.max_inflight_bytes = 0
         self.max_inflight = 0
+        self.max_group = 0          # largest coalesced launch
+        self._group_ds = []         # datasets with a batched evaluator
         self._done = []
         self._error = None
         self._thread = threading.Thread(target=self._run, name='gbkb200-serving', daemon=True)
         self._thread.start()
 
     # ---- datasets --------------------------------------------------------------
-    def register(self, key, geom, data, error=None):
-        """Make a dataset resident (its spectrum is computed now)."""
+    def register(self, key, geom, data, error=None, smdisk=None, batch_sets=16):
+        """Make a dataset resident (its spectrum is computed now).  smdisk:
+        the thin disk of its smdisk requests, whose requests are then
+        coalesced into batched launches (see Dataset)."""
         with torch.cuda.device(self.dev):
-            ds = Dataset(key, geom, data, error, self._setup_ctx, self.dev, self._setup_stream)
+            ds = Dataset(key, geom, data, error, self._setup_ctx, self.dev, self._setup_stream,
+                         smdisk=smdisk, batch_sets=batch_sets)
         with self._cv:
             if key in self.datasets:
                 raise KeyError(f"dataset {key!r} is already registered")
@@ -237,6 +269,8 @@ class ModelServer:
                 raise MemoryError(f"dataset {key!r} does not fit the HBM budget")
             self.datasets[key] = ds
             self._resident += ds.footprint
+            if ds.batched is not None:
+                self._group_ds.append(ds)
         return ds
 
     def unregister(self, key):
@@ -247,7 +281,17 @@ class ModelServer:
             ds = self.datasets.pop(key)
             ds.released = True
             if ds.holders == 0:
-                self._resident -= ds.footprint
+                self._release(ds)
+
+    def _release(self, ds):
+        """An unregistered dataset that no request holds any more (call with
+        the lock held): its bytes leave the budget, its evaluator goes."""
+        self._resident -= ds.footprint
+        if ds in self._group_ds:
+            self._group_ds.remove(ds)
+        if ds.batched is not None:
+            ds.batched.stream.synchronize()
+            ds.batched.close()
 
     # ---- requests --------------------------------------------------------------
     def submit(self, request):
@@ -258,14 +302,19 @@ class ModelServer:
             raise KeyError(f"unknown dataset {request.dataset!r}")
         if request.arrival is None:
             request.arrival = time.perf_counter()
-        if request.blob is None:
-            request.prepare()
-        if request.blob.size > _Slot.STAGE:
-            raise ValueError("the request's parameter arrays exceed the staging buffer")
-        # the request holds its dataset: the native arguments point into the
-        # dataset's device buffers until the request completes
+        # packing happens here, in the caller's thread, after the arrival time
         request.ds = ds
-        request.args = request.serve_args(ds)
+        if (ds.batched is not None and request.kind == 'smdisk' and request.disk is ds.smdisk
+                and not request.want_model and not request.thick):
+            request.rows = ds.batched.pack_one(request.params)
+        else:
+            if request.blob is None:
+                request.prepare()
+            if request.blob.size > _Slot.STAGE:
+                raise ValueError("the request's parameter arrays exceed the staging buffer")
+            # the request holds its dataset: the native arguments point into the
+            # dataset's device buffers until the request completes
+            request.args = request.serve_args(ds)
         with self._cv:
             if self._error is not None:
                 raise RuntimeError("the serving loop stopped") from self._error
@@ -288,6 +337,10 @@ class ModelServer:
         for s in self._slots:
             s.stream.synchronize()
             s.ctx.close()
+        for ds in self.datasets.values():
+            if ds.batched is not None:
+                ds.batched.stream.synchronize()
+                ds.batched.close()
         self._setup_ctx.close()
 
     def __enter__(self):
@@ -311,18 +364,22 @@ class ModelServer:
         return dict(requests=len(done), p50_ms=float(np.percentile(lat, 50)),
                     p99_ms=float(np.percentile(lat, 99)), mean_ms=float(lat.mean()),
                     max_ms=float(lat.max()), evals_per_s=len(done) / max(t1 - t0, 1e-9),
-                    max_inflight=self.max_inflight, max_inflight_bytes=self.max_inflight_bytes)
+                    max_inflight=self.max_inflight, max_inflight_bytes=self.max_inflight_bytes,
+                    max_group=self.max_group)
 
     # ---- scheduler -------------------------------------------------------------
+    SCAN = 64   # queued requests the scheduler looks at per pass
+
     def _run(self):
         try:
             with torch.cuda.device(self.dev):
                 while True:
                     with self._cv:
                         busy = [s for s in self._slots if s.req is not None]
-                        if self._stop and not busy and not self._queue:
+                        groups = [d for d in self._group_ds if d.group is not None]
+                        if self._stop and not busy and not groups and not self._queue:
                             return
-                        if not busy and not self._queue:
+                        if not busy and not groups and not self._queue:
                             self._cv.wait()
                             continue
                     progressed = False
@@ -330,33 +387,98 @@ class ModelServer:
                         if s.event.query():
                             self._complete(s)
                             progressed = True
-                    while True:
-                        with self._cv:
-                            free = [s for s in self._slots if s.req is None]
-                            if not free or not self._queue:
-                                break
-                            req = self._queue[0]
-                            need = req.ds.request_footprint()
-                            if self._resident + self._inflight + need > self.budget and \
-                                    self._inflight > 0:
-                                break
-                            self._queue.popleft()
-                            self._inflight += need
-                            nbusy = len(self._slots) - len(free) + 1
-                            self.max_inflight = max(self.max_inflight, nbusy)
-                            self.max_inflight_bytes = max(self.max_inflight_bytes, self._inflight)
-                        self._launch(free[0], req, need)
-                        progressed = True
+                    for d in groups:
+                        if d.group[0].query():
+                            self._complete_group(d)
+                            progressed = True
+                    progressed |= self._admit()
                     if not progressed:
                         time.sleep(2e-5)
         except BaseException as e:      # fail every pending future, not the process
             with self._cv:
                 self._error = e
                 pending = list(self._queue) + [s.req for s in self._slots if s.req is not None]
+                for d in self._group_ds:
+                    if d.group is not None:
+                        pending += d.group[2]
                 self._queue.clear()
             for r in pending:
                 if not r.future.done():
                     r.future.set_exception(e)
+
+    def _admit(self):
+        """Starts what the queue allows, in arrival order among the first
+        SCAN requests: a coalesced group for a request of a batched dataset
+        whose evaluator is idle (with the dataset's other queued requests), a
+        slot for any other request while a slot is free and the HBM budget
+        holds.  Requests that cannot start yet are passed over."""
+        launches = []
+        with self._cv:
+            q = [self._queue.popleft() for _ in range(min(len(self._queue), self.SCAN))]
+            free = [s for s in self._slots if s.req is None]
+            taken = set()
+            for i in range(len(q)):
+                if i in taken:
+                    continue
+                req = q[i]
+                ds = req.ds
+                if req.rows is not None:
+                    if ds.group is not None or ds in (g[0] for g in launches if g[1] == 'group'):
+                        continue
+                    group = [i]
+                    for j in range(i + 1, len(q)):
+                        if len(group) >= ds.batched.max_sets:
+                            break
+                        if j not in taken and q[j].rows is not None and q[j].ds is ds:
+                            group.append(j)
+                    taken.update(group)
+                    launches.append((ds, 'group', [q[j] for j in group]))
+                    continue
+                if not free:
+                    continue
+                need = ds.request_footprint()
+                if self._resident + self._inflight + need > self.budget and self._inflight > 0:
+                    continue
+                self._inflight += need
+                taken.add(i)
+                slot = free.pop(0)
+                slot.req = req      # reserved; _launch fills the rest
+                launches.append((slot, 'slot', (req, need)))
+                nbusy = len(self._slots) - len(free)
+                self.max_inflight = max(self.max_inflight, nbusy)
+                self.max_inflight_bytes = max(self.max_inflight_bytes, self._inflight)
+            # the requests passed over go back to the front, in order
+            self._queue.extendleft(reversed([r for k, r in enumerate(q) if k not in taken]))
+        for target, kind, what in launches:
+            if kind == 'group':
+                self._launch_group(target, what)
+            else:
+                self._launch(target, *what)
+        return bool(launches)
+
+    def _launch_group(self, ds, reqs):
+        now = time.perf_counter()
+        for r in reqs:
+            r.admit = now
+        ev, out = ds.batched.submit_rows([r.rows for r in reqs])
+        ds.group = (ev, out, reqs)
+        self.max_group = max(self.max_group, len(reqs))
+
+    def _complete_group(self, ds):
+        ev, out, reqs = ds.group
+        chi2 = out.numpy().copy()
+        now = time.perf_counter()
+        with self._cv:
+            ds.group = None
+            for r in reqs:
+                r.done = now
+                r.ds = None
+                ds.holders -= 1
+                self._done.append(r)
+            if ds.released and ds.holders == 0:
+                self._release(ds)
+        for r, c in zip(reqs, chi2):
+            r.future.set_result(dict(chi2=float(c)))
 
     def _launch(self, slot, req, need):
         ds = req.ds
@@ -398,7 +520,7 @@ class ModelServer:
         with self._cv:
             ds.holders -= 1
             if ds.released and ds.holders == 0:
-                self._resident -= ds.footprint
+                self._release(ds)
             self._inflight -= slot.bytes
             slot.req, slot.keep, slot.bytes = None, None, 0
             self._done.append(req)

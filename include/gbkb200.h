@@ -352,7 +352,8 @@ int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb2
 int gbkb200_batch_evaluate(gbkb200_batch* b, int nsets, const float* vsys, const float* xpos,
                            const float* ypos, const float* posa, const float* incl,
                            const float* const pvalues[9], float* chi2, float* model);
-/* the chosen FFT grid, chunk, work-space bytes and convolution mode (1 = FFT,
+/* the chosen FFT grid, chunk, the device bytes the evaluator holds (its
+ * work space, tables and partials) and the convolution mode (1 = FFT,
  * 2 = direct) */
 int gbkb200_batch_info(const gbkb200_batch* b, int fft_size[3], int* chunk, size_t* work_bytes,
                        int* conv_mode);

@@ -121,3 +121,73 @@ def test_unregister_keeps_submitted_requests(gpu):
             assert a == b
         else:
             assert abs(a - b) <= 1e-5 * abs(a)
+
+
+def _register_coalesced(server, stream, batch_sets=8):
+    for d in stream.datasets:
+        server.register(d['key'], d['geom'], d['data'], d['error'], smdisk=d['smdisk'],
+                        batch_sets=batch_sets)
+
+
+def test_coalesced_smdisk_same_alone_and_in_mix(gpu):
+    """Datasets with a batched evaluator: smdisk requests submitted together
+    are coalesced into launches of several sets; each chi^2 is bit-identical
+    to the same request evaluated alone (a launch of one set)."""
+    from gbkfit_b200.serving import ModelServer
+    stream = _small_stream(n=64, seed=17)
+    kinds = [q['kind'] for q in stream.requests]
+    with ModelServer(slots=1) as alone:
+        _register_coalesced(alone, stream)
+        assert all(ds.batched is not None for ds in alone.datasets.values())
+        ref = [alone.evaluate(r)['chi2'] for r in _requests(stream)]
+        assert alone.stats()['max_group'] == 1
+    with ModelServer(slots=8) as mix:
+        _register_coalesced(mix, stream)
+        futs = [mix.submit(r) for r in _requests(stream)]
+        got = [f.result()['chi2'] for f in futs]
+        assert mix.stats()['max_group'] > 1          # requests were coalesced
+    for k, a, b in zip(kinds, ref, got):
+        if k == 'smdisk':
+            assert a == b
+        else:
+            assert abs(a - b) <= 1e-5 * abs(a)
+
+
+def test_coalesced_chi2_matches_oracle_and_fft_path(gpu, oracle_built):
+    """Coalesced smdisk chi^2 (direct separable convolution) against the fp64
+    oracle and against the same requests on the per-request FFT path."""
+    from oracle.oracle import chi2, scube_pipeline
+    from gbkfit_b200.serving import ModelServer
+    stream = _small_stream(n=24, seed=19)
+    reqs = [r for r in _requests(stream) if r.kind == 'smdisk'][:6]
+    with ModelServer(slots=4) as srv:
+        _register_coalesced(srv, stream)
+        got = [f.result()['chi2'] for f in [srv.submit(r) for r in reqs]]
+    with ModelServer(slots=4) as srv:
+        _register(srv, stream)
+        fft = [f.result()['chi2'] for f in [srv.submit(r) for r in _requests(stream)
+                                            if r.kind == 'smdisk'][:6]]
+    for r, c, f in zip(reqs, got, fft):
+        d = stream.datasets[r.dataset]
+        ref = chi2(scube_pipeline(r.disk.pack(r.params), d['geom']), d['data'], d['error'])
+        assert abs(c - ref) <= 1e-4 * ref, (c, ref)
+        assert abs(c - f) <= 1e-4 * ref, (c, f)
+
+
+def test_coalesced_unregister_releases_budget(gpu):
+    """Unregistering batched datasets with requests in flight: the requests
+    complete with the same results and the datasets' bytes (evaluators
+    included) leave the budget once the last of them is done."""
+    from gbkfit_b200.serving import ModelServer
+    stream = _small_stream(n=20, seed=23)
+    with ModelServer(slots=4) as srv:
+        _register_coalesced(srv, stream)
+        assert srv._resident > 0
+        ref = [f.result()['chi2'] for f in [srv.submit(r) for r in _requests(stream)]]
+        futs = [srv.submit(r) for r in _requests(stream)]
+        for d in stream.datasets:
+            srv.unregister(d['key'])
+        got = [f.result()['chi2'] for f in futs]
+        assert srv._resident == 0 and srv._group_ds == []
+    for a, b in zip(ref, got):
+        assert abs(a - b) <= 1e-5 * abs(a)
