@@ -797,6 +797,69 @@ def run_grad96(args):
                             path='SMDiskChi2.value_and_grad (host vector in, host gradient out)'))
 
 
+def run_fft_conv(args):
+    """fft_conv: the drop-in FFT convolution (gbkb200_fft_convolve_cached:
+    r2c, multiply by the cached PSF x LSF spectrum / N, c2r; fft.hpp:98-207)
+    on the padded grids of the mcdisk configuration (320 x 320 x 160) and of
+    the largest serving request (288 x 288 x 224), and the batched evaluator
+    in FFT mode (a Moffat PSF, not separable) on the batched configuration's
+    512 sets of 128 x 128 x 96.  The convolution's bytes are those of its own
+    five passes over the cube: x r2c (4 V read, 8 C written), y (16 C), z with
+    the multiply (24 C: read, spectrum, write), inverse y (16 C), x c2r (8 C
+    read, 4 V written) = 8 V + 72 C, V = voxels, C = (nx/2 + 1) ny nz."""
+    import torch
+    from gbkfit_b200 import psflsf, workloads
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    from gbkfit_b200.driver import DriverB200
+    hbm, peak_kind = peaks()
+    fft = DriverB200(torch.cuda.current_device()).backends().fft(np.float32)
+    grids = []
+    for name, (nx, ny, nz) in (('mcdisk_cube256 padded', (320, 320, 160)),
+                               ('serving max padded', (288, 288, 224))):
+        g = torch.Generator(device='cuda').manual_seed(1)
+        cube = torch.rand((nz, ny, nx), device='cuda', generator=g)
+        kern = torch.rand((nz, ny, nx), device='cuda', generator=g)
+        kern /= kern.sum()
+        work = cube.clone()
+
+        def call():
+            work.copy_(cube)
+            fft.fft_convolve_cached(work, kern)
+
+        copy_ms = _events_ms(lambda: work.copy_(cube), args.steps, args.warmup)
+        ms = _events_ms(call, args.steps, args.warmup) - copy_ms
+        v, c = nx * ny * nz, (nx // 2 + 1) * ny * nz
+        b = 8 * v + 72 * c
+        grids.append(dict(grid=[nx, ny, nz], what=name, ms=round(ms, 4),
+                          pass_bytes=b, achieved_gbs=round(b / (ms / 1e3) / 1e9, 1),
+                          frac=round(b / (ms / 1e3) / 1e9 / hbm, 3),
+                          minimal_bytes=8 * v + 8 * c,
+                          note='ms excludes the copy that restores the input'))
+    # batched FFT mode: Moffat PSF (FWHM 3 px, beta 2.5) on the batched cube
+    w = workloads.smdisk_batch128(nsets=args.nsets)
+    w.geom = workloads.Geometry(w.geom.size, w.geom.step, (0, 0, (w.geom.size[2] - 1) / 2),
+                                (0, 0, 0), psflsf.PSFMoffat(psflsf.moffat_fwhm_beta_to_alpha(3.0, 2.5),
+                                                            2.5), w.geom.lsf)
+    data, err, _ = synthetic_data(w)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=args.nsets, chunk=16, conv='fft')
+    bufs = ev.alloc_inputs(args.nsets)
+    ev.upload(ev.pack(w.params, args.nsets), bufs, args.nsets)
+    ev.capture(bufs, args.nsets)
+    bms = _events_ms(ev.replay, args.steps, args.warmup)
+    return dict(metric='drop-in FFT convolution GB/s (own passes) and batched FFT-mode evals/s',
+                value=grids[0]['achieved_gbs'], unit='GB/s', n_gpus=1, steps=args.steps,
+                warmup=args.warmup, higher_is_better=True, dtype='f32', data='synthetic',
+                roofline=dict(bound='hbm', achieved=grids[0]['achieved_gbs'], peak=hbm,
+                              unit='GB/s', frac=grids[0]['frac'], peak_kind=peak_kind,
+                              kernel='fft_convolve_cached (5 passes)', traffic=None),
+                grids=grids,
+                batched_fft=dict(workload='smdisk_batch128 sets with a Moffat PSF (FWHM 3 px, '
+                                          'beta 2.5): FFT mode', nsets=args.nsets,
+                                 fft_grid=list(ev.fft_size), chunk=ev.chunk,
+                                 ms_per_step=round(bms, 4),
+                                 evals_per_s=round(args.nsets / (bms / 1e3), 1)))
+
+
 def run_serving(args):
     out = serving_run(nrequests=args.requests)
     return dict(metric='serving capacity evals/s and latency (ms)',
@@ -826,14 +889,14 @@ def main():
                     help='force the output rows per PSF block of the direct mode (default: tuned)')
     ap.add_argument('--workload', default='smdisk_batch128',
                     choices=['smdisk_batch128', 'mcdisk_cube256', 'smdisk_cube64', 'grad96',
-                             'serving'],
+                             'serving', 'fft_conv'],
                     help='smdisk_batch128 is the headline; the others print their own line')
     ap.add_argument('--requests', type=int, default=10000, help='serving workload: requests')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     other = dict(mcdisk_cube256=run_mcdisk, smdisk_cube64=run_smdisk64, grad96=run_grad96,
-                 serving=run_serving)
+                 serving=run_serving, fft_conv=run_fft_conv)
     if args.workload in other and args.impl != 'reference':
         import torch
         torch.cuda.set_device(0)

@@ -30,13 +30,14 @@ from .disk import Disk, KINDS
 from .workloads import fft_optimal_shape
 
 
-def _merge(pdesc_list, prefix):
-    """utils/miscutils.py:70-95 with zero_prefix = zero_index = False."""
+def _merge(pdesc_list, prefix, zero_prefix=False):
+    """utils/miscutils.py:70-95 with zero_index = False: component i > 0 gets
+    '<prefix><i>_', component 0 gets '<prefix>_' with zero_prefix, else none."""
     merged, maps = {}, []
     for i, d in enumerate(pdesc_list):
         m = {}
         for name, v in d.items():
-            new = f'{prefix}{i}_{name}' if i else name
+            new = f'{prefix}{i}_{name}' if i else (f'{prefix}_{name}' if zero_prefix else name)
             m[name] = new
             merged[new] = v
         maps.append(m)
@@ -108,12 +109,13 @@ class _DiskComponent:
         shape = tuple(spat_size[::-1])
         extra = {}
         if out_extra is not None:
+            dv = dev['subrnodes'].device
             if d.traits['rpt']:
-                extra['rdata_cmp'] = torch.zeros(shape, device=scube.device)
+                extra['rdata_cmp'] = torch.zeros(shape, device=dv)
             if d.traits['vpt']:
-                extra['vdata_cmp'] = torch.full(shape, np.nan, device=scube.device)
+                extra['vdata_cmp'] = torch.full(shape, np.nan, device=dv)
             if d.traits['dpt']:
-                extra['ddata_cmp'] = torch.full(shape, np.nan, device=scube.device)
+                extra['ddata_cmp'] = torch.full(shape, np.nan, device=dv)
         tset = []
         for k in KINDS:
             t = dev[k]

@@ -431,15 +431,22 @@ def chi2_gradient_f64(packed, geom, data, error, scale):
 
 
 def dcube_pipeline(packed, size, step, rpix, rval, scale, psf, lsf, precision='f64',
-                   mask_cutoff=None, mask_apply=False, thick=False):
+                   mask_cutoff=None, mask_apply=False, thick=False, image=False,
+                   opacity_packed=None):
     """The reference's DCube chain with supersampling and masking
     (_dcube.py:128-313): the padded high-resolution grid (size x scale +
     kernel - 1, padded by backend.py:51-66), smdisk on it, FFT convolution
     with the rolled PSF x LSF cube sampled at the high-resolution step, the
     downscale of the crop (dmodels.hpp:8-46, host/kernels.hpp:55-80) and the
     mask (dmodels.hpp:49-74).  psf/lsf are gbkfit_b200.psflsf objects (their
-    arrays are pinned to the reference's by the golden fixtures).  Returns
-    (dcube_lo, mcube_lo or None)."""
+    arrays are pinned to the reference's by the golden fixtures).
+
+    image: the disk is evaluated into the spatial image instead of the
+    spectral cube (the intensity gmodels, intensity_2d/3d.py; size z is 1).
+    opacity_packed: an opacity disk evaluated first into the 3-D spatial
+    opacity cube (its density output), which the disk then reads
+    (intensity_3d.py:154-167, gmodels.hpp:933-937).  Returns (dcube_lo,
+    mcube_lo or None)."""
     from gbkfit_b200.workloads import dcube_geometry
     o = Oracle(precision)
     real = o.real
@@ -455,8 +462,16 @@ def dcube_pipeline(packed, size, step, rpix, rval, scale, psf, lsf, precision='f
     g = dict(loose=False, tilted=False, spat_size=spat[0], spat_step=spat[1],
              spat_zero=spat[2], spec_size=sz, spec_step=step_hi[2], spec_zero=zero_hi[2],
              opacity=None)
+    if opacity_packed is not None:
+        op = np.zeros(tuple(spat[0])[::-1], real)
+        o.smdisk_evaluate(opacity_packed, g, dict(rdata=op))
+        g['opacity'] = op
     cube = np.zeros((sz, sy, sx), real)
-    o.smdisk_evaluate(packed, g, dict(scube=cube))
+    if image:
+        g['spec_size'], g['spec_step'], g['spec_zero'] = 1, 0.0, 0.0
+        o.smdisk_evaluate(packed, g, dict(image=cube[0]))
+    else:
+        o.smdisk_evaluate(packed, g, dict(scube=cube))
     if psf is not None or lsf is not None:
         from gbkfit_b200 import psflsf as P
         off = [(n % 2) - 1 for n in size_hi]

@@ -191,3 +191,26 @@ def test_serve_entry_rejects_missing_arguments():
     assert lib.gbkb200_serve_scube_chi2_f32(None, None) == 1
     a = _native.ServeArgs()
     assert lib.gbkb200_serve_scube_chi2_f32(None, ctypes.byref(a)) == 1
+
+
+def test_imaging_model_parameter_names():
+    """intensity_3d.py / gmodels/_detail.py:339-342 and utils/miscutils.py:
+    70-95: brightness components keep their names (the second and later get
+    'cmp<i>_'), opacity components are always prefixed ('ocmp_', 'ocmp1_')."""
+    from gbkfit_b200 import traits as T
+    from gbkfit_b200.imaging import (BrightnessSMDisk2D, BrightnessSMDisk3D, GModelIntensity2D,
+                                     GModelIntensity3D, OpacitySMDisk3D, DModelImage,
+                                     DModelLSlit)
+    rn = np.linspace(0, 20, 6)
+    b2 = [BrightnessSMDisk2D(False, False, T.bpt('exponential'), rnodes=rn) for _ in range(2)]
+    assert set(GModelIntensity2D(b2).pdescs()) == {
+        'xpos', 'ypos', 'posa', 'incl', 'bpt_a', 'bpt_s', 'cmp1_xpos', 'cmp1_ypos', 'cmp1_posa',
+        'cmp1_incl', 'cmp1_bpt_a', 'cmp1_bpt_s'}
+    b3 = BrightnessSMDisk3D(False, False, T.bpt('gauss'), T.bht('sech2'), rnodes=rn)
+    o3 = [OpacitySMDisk3D(False, False, T.opt('exponential'), T.oht('sech2'), rnodes=rn)
+          for _ in range(2)]
+    names = set(GModelIntensity3D([b3], o3).pdescs())
+    assert {'bpt_a', 'bht_s', 'ocmp_opt_a', 'ocmp_oht_a', 'ocmp1_opt_s', 'ocmp1_xpos'} <= names
+    assert o3[0].disk().tables['rpt']['uids'][0] == T.OPT_OFFSET + T.RPT['exponential']
+    assert DModelImage((30, 20)).size() == (30, 20) and DModelImage((30, 20)).keys() == ['image']
+    assert DModelLSlit((30, 40)).size() == (30, 1, 40)
