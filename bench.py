@@ -644,7 +644,7 @@ def run_mcdisk(args):
                            None, None)
 
     ms = {}
-    for mode, name in ((0, 'fast'), (1, 'deterministic')):
+    for mode, name in ((0, 'fast'), (1, 'deterministic'), (2, 'vector_atomics')):
         gm.set_mcdisk(seed=42, mode=mode)
         ms[name] = _events_ms(call, args.steps, args.warmup)
     gm.set_mcdisk(seed=42, mode=0)
@@ -663,7 +663,8 @@ def run_mcdisk(args):
     return dict(metric='mcdisk evals/s (1e7 clouds, thick disk, padded 320x320x320 x 160 grid)',
                 value=round(1e3 / ms['fast'], 2), unit='evals/s', n_gpus=1, steps=args.steps,
                 warmup=args.warmup, ms_per_step=round(ms['fast'], 4),
-                ms_deterministic=round(ms['deterministic'], 4), higher_is_better=True,
+                ms_deterministic=round(ms['deterministic'], 4),
+                ms_vector_atomics=round(ms['vector_atomics'], 4), higher_is_better=True,
                 dtype='f32', data='synthetic', gpu_launches=args.steps,
                 config=dict(workload='mcdisk_cube256', nclouds=n, grid=[nx, ny, g['spat_size'][2], nz],
                             l2='flushed before every call (256 MB write)'),

@@ -363,6 +363,76 @@ __global__ void __launch_bounds__(256) mcdisk_kernel(DiskArgs a, McArgs m, int* 
     if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
 }
 
+// ---- mcdisk mode 2: channel-contiguous lines, 16-byte vector atomics ---------
+// The cube lines go to a scratch cube laid out spaxel-major with the channels
+// contiguous (a column of nzp = spec_size rounded up to 4 floats per spaxel),
+// four channels per red.global.add.v4.f32 (about spectral window / 4 + 1
+// atomics per cloud instead of one per channel); a tiled transpose then adds
+// the scratch cube to scube in the reference's (channel, y, x) layout.  The
+// other outputs are accumulated as in mode 0.
+__global__ void __launch_bounds__(256) mcdisk_v4_kernel(DiskArgs a, McArgs m, float* lines,
+                                                        int nzp, int* status)
+{
+    int bad = 0;
+    for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < m.nclouds;
+         ci += gridDim.x * blockDim.x) {
+        int x, y, z;
+        SpaxelOut o;
+        if (!mcdisk_cloud(a, m, ci, x, y, z, o, bad)) continue;
+        if (a.image) atomicAdd(&a.image[x + (long long)a.sx * y], o.orv);
+        int zlo, zhi;
+        if (lines && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
+            const float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
+            const float inv2c2 = 2 * o.dv * o.dv;
+            float* col = lines + (x + (long long)a.sx * y) * nzp;
+            for (int z4 = zlo & ~3; z4 <= zhi; z4 += 4) {
+                float v[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int zs = z4 + j;
+                    const float d = (a.spec_zero + zs * a.spec_step) - o.vv;
+                    v[j] = (zs >= zlo && zs <= zhi) ? o.orv * (amp * expf(-d * d / inv2c2)) : 0.f;
+                }
+                atomicAdd(reinterpret_cast<float4*>(col + z4), make_float4(v[0], v[1], v[2], v[3]));
+            }
+        }
+        long long idx = idx3(x, y, z, a.sx, a.sy);
+        if (a.wdata) a.wdata[idx] = o.wv;
+        if (a.wdata_cmp) a.wdata_cmp[idx] = o.wv;
+        if (a.rdata) atomicAdd(&a.rdata[idx], o.rv);
+        if (a.rdata_cmp) atomicAdd(&a.rdata_cmp[idx], o.rv);
+        if (a.ordata) atomicAdd(&a.ordata[idx], o.orv);
+        if (a.ordata_cmp) atomicAdd(&a.ordata_cmp[idx], o.orv);
+        if (a.vdata_cmp) a.vdata_cmp[idx] = o.vv;
+        if (a.ddata_cmp) a.ddata_cmp[idx] = o.dv;
+    }
+    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
+}
+
+// scube[z][s] += lines[s][z] for spaxels s < nsp, channels z < nz (32 x 32 tiles)
+__global__ void __launch_bounds__(256) mc_lines_add_kernel(const float* __restrict__ lines,
+                                                           float* __restrict__ scube,
+                                                           long long nsp, int nzp, int nz)
+{
+    __shared__ float tile[32][33];
+    const long long s0 = (long long)blockIdx.x * 32;
+    const int z0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const long long s = s0 + ty + k;
+        const int z = z0 + tx;
+        tile[ty + k][tx] = (s < nsp && z < nz) ? lines[s * nzp + z] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const int z = z0 + ty + k;
+        const long long s = s0 + tx;
+        if (s < nsp && z < nz) scube[(long long)z * nsp + s] += tile[tx][ty + k];
+    }
+}
+
 // ---- deterministic mcdisk: 64-bit fixed-point accumulation ------------------
 // Integer addition is associative, so the sums do not depend on the order in
 // which clouds land.  A bound pass finds the largest contribution M of the
@@ -588,8 +658,28 @@ extern "C" int gbkb200_gmodel_mcdisk_evaluate_f32(gbkb200_ctx* ctx, float cflux,
     m.seed = ctx->seed;
     int blocks = (nclouds + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    if (ctx->mc_mode != 1) {
+    if (ctx->mc_mode == 0 || (ctx->mc_mode == 2 && !a.scube)) {
         mcdisk_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, ctx->d_status);
+        GBK_CUDA_TRY(cudaGetLastError());
+        return gbk_finish(ctx);
+    }
+    if (ctx->mc_mode == 2) {
+        // channel-contiguous line cube in the context's scratch
+        const long long nsp = (long long)a.sx * a.sy;
+        const int nzp = (a.spec_size + 3) & ~3;
+        const size_t need = (size_t)nsp * nzp * sizeof(float);
+        if (ctx->mc_scratch_bytes < need) {
+            if (ctx->mc_scratch) cudaFree(ctx->mc_scratch);
+            ctx->mc_scratch = nullptr;
+            ctx->mc_scratch_bytes = 0;
+            if (cudaMalloc(&ctx->mc_scratch, need) != cudaSuccess) return GBKB200_ERR_OOM;
+            ctx->mc_scratch_bytes = need;
+        }
+        float* lines = static_cast<float*>(ctx->mc_scratch);
+        GBK_CUDA_TRY(cudaMemsetAsync(lines, 0, need, ctx->stream));
+        mcdisk_v4_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, lines, nzp, ctx->d_status);
+        const dim3 tg((unsigned)((nsp + 31) / 32), (unsigned)((a.spec_size + 31) / 32));
+        mc_lines_add_kernel<<<tg, 256, 0, ctx->stream>>>(lines, a.scube, nsp, nzp, a.spec_size);
         GBK_CUDA_TRY(cudaGetLastError());
         return gbk_finish(ctx);
     }

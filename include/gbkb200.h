@@ -62,9 +62,12 @@ int gbkb200_ctx_set_sync(gbkb200_ctx* ctx, int sync);
  * ordata and their _cmp forms) are summed in 64-bit fixed point, bit-identical
  * run to run and exact to ~2^-(62 - log2 nclouds) of the largest contribution;
  * it takes an extra bound pass over the clouds and scratch of 8 bytes per
- * accumulated element held by the context.  The assigned maps (wdata,
- * vdata_cmp, ddata_cmp) keep the reference's last-writer-wins race in both
- * modes. */
+ * accumulated element held by the context; mode 2 = fast with the lines
+ * accumulated channel-contiguous in a scratch cube held by the context (4
+ * bytes per scube element) with 16-byte vector atomics, then added to scube
+ * (sums order-dependent in the last bits, as mode 0).  The assigned maps
+ * (wdata, vdata_cmp, ddata_cmp) keep the reference's last-writer-wins race in
+ * every mode. */
 int gbkb200_ctx_set_mcdisk(gbkb200_ctx* ctx, unsigned long long seed, int mode);
 /* waits for the context's stream, then returns the status raised by kernels
  * since the last call (GBKB200_OK, _BAD_TRAIT or _TIMEOUT) and clears it */

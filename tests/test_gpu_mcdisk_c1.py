@@ -76,6 +76,19 @@ def test_c1_fast_mode_matches_deterministic(c1):
         <= 1e-5 * det['scube'].astype(np.float64).sum()
 
 
+def test_c1_vector_mode_matches_deterministic(c1):
+    """Mode 2 (lines accumulated channel-contiguous with 16-byte vector
+    atomics, then added to the cube) sums the same contributions as the
+    deterministic mode, to fp32 accumulation error."""
+    det = c1.get('det') or c1['run'](1)
+    v4 = c1['run'](2)
+    assert np.array_equal(v4['rdata'] != 0, det['rdata'] != 0)
+    assert rel_err(v4['rdata'], det['rdata']) <= 1e-4
+    assert rel_err(v4['scube'], det['scube']) <= 1e-5
+    assert abs(v4['scube'].astype(np.float64).sum() - det['scube'].astype(np.float64).sum()) \
+        <= 1e-5 * det['scube'].astype(np.float64).sum()
+
+
 def test_c1_vs_compiled_reference_shot_noise(c1, oracle_built):
     from oracle.oracle import Reference
     if not Reference.available():

@@ -305,8 +305,13 @@ def test_mcdisk_deterministic_mode(be, oracle_built):
                    torch.from_numpy(hoi).cuda(), pd, g, outs)
         return {k: v.cpu().numpy() for k, v in outs.items()}
 
-    a, b, fast = run(1), run(1), run(0)
+    a, b, fast, v4 = run(1), run(1), run(0), run(2)
     be['gmodel'].set_mcdisk(seed=42, mode=0)
+    # mode 2 (vector atomics into a channel-contiguous scratch cube) sums the
+    # same contributions
+    assert rel_err(v4['scube'], a['scube']) <= 1e-5
+    for k in ('image', 'rdata'):
+        assert rel_err(v4[k], a[k]) <= 1e-4, k
     for k in a:
         assert np.array_equal(a[k], b[k]), k
     # every cloud adds cflux / (dx dy) to the maps: the fixed-point sums are
