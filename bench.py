@@ -291,6 +291,8 @@ def run_b200(args):
         cfg['chunk'] = args.chunk
     if args.band:
         cfg['band'] = args.band
+    if args.psf_blocks:
+        cfg['psf_blocks'] = args.psf_blocks
     ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
     bufs = ev.alloc_inputs(nsets)
     ev.upload(ev.pack(mine, nsets), bufs, nsets)
@@ -886,6 +888,8 @@ def main():
     ap.add_argument('--conv', choices=['fft', 'direct'], default=None,
                     help='force the convolution mode (default: tuned)')
     ap.add_argument('--chunk', type=int, default=0, help='force the sets per wave (default: tuned)')
+    ap.add_argument('--psf-blocks', type=int, default=0, choices=[0, 4, 5],
+                    help='PSF kernel resident blocks per SM of the direct mode (default: tuned)')
     ap.add_argument('--band', type=int, default=0,
                     help='force the output rows per PSF block of the direct mode (default: tuned)')
     ap.add_argument('--workload', default='smdisk_batch128',

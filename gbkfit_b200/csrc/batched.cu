@@ -401,11 +401,15 @@ static KaFn ka_fn(int Kz)
     return t[Kz / 2];
 }
 
-static KbFn kb_fn(int K)
+static KbFn kb_fn(int K, int blocks)
 {
-    static KbFn t[(KB_KMAX - KB_KMIN) / 2 + 1] = {};
-    if (!t[0]) kb_register(t);
-    return t[(K - KB_KMIN) / 2];
+    static KbFn t4[(KB_KMAX - KB_KMIN) / 2 + 1] = {};
+    static KbFn t5[(KB_KMAX - KB_KMIN) / 2 + 1] = {};
+    if (!t4[0]) {
+        kb_register(t4);
+        kb_register5(t5);
+    }
+    return (blocks == 5 ? t5 : t4)[(K - KB_KMIN) / 2];
 }
 
 // Direct-mode setup: reversed FIR coefficients, plane buffers, the data's
@@ -479,7 +483,10 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     const long long xr_bytes = (long long)(P.band + P.K - 1) * P.nch * sizeof(int);
     const long long need_min = (long long)(P.K + 15) * bpmax;
     const long long need_all = (long long)(P.band + P.K + 7) * bpmax;
-    const long long cap = std::max(need_min, std::min(need_all, (55LL * 1024 - xr_bytes) / 4));
+    // shared memory per block: 55 KB for 4 resident blocks per SM, 43 KB for 5
+    const int blocks = d->psf_blocks == 5 ? 5 : 4;
+    const long long budget = blocks == 5 ? 43LL * 1024 : 55LL * 1024;
+    const long long cap = std::max(need_min, std::min(need_all, (budget - xr_bytes) / 4));
     if (cap * (long long)sizeof(float) + xr_bytes > 227LL * 1024) return GBKB200_ERR_UNSUPPORTED;
     P.cap = (int)cap;
     bt->smemB = (size_t)cap * sizeof(float) + (size_t)xr_bytes;
@@ -511,7 +518,7 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     GBK_CUDA_TRY(cudaGetLastError());
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
     bt->ka = ka_fn(P.Kz);
-    bt->kb = kb_fn(P.K);
+    bt->kb = kb_fn(P.K, blocks);
     GBK_CUDA_TRY(cudaFuncSetAttribute(bt->kb, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)bt->smemB));
     bt->nper = P.Nz * P.nbands;

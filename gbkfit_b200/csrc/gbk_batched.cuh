@@ -247,8 +247,11 @@ __device__ __forceinline__ double sat_box(const double* T, int ld, int y0, int y
 constexpr int KB_THREADS = 128;
 constexpr int KB_NX_MAX = 512;  // widest data cube of the direct mode
 
-template<int K>
-__global__ void __launch_bounds__(KB_THREADS, 4) kb_psf_residual(BatchKernelArgs P)
+// MINB: resident blocks per SM the registers are sized for (4: up to 128
+// registers a thread; 5: up to 102, with the shared memory per block sized to
+// match, see setup_direct)
+template<int K, int MINB>
+__global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelArgs P)
 {
     constexpr int NW = (K + 7 + 3) / 4;     // float4 slots of one 8-output x window
     constexpr int NWARPS = KB_THREADS / 32;
@@ -542,6 +545,7 @@ static_assert(KA_KMAX <= 33 && KB_KMAX <= 33, "coefficient arrays of BatchKernel
 // fill t[Kz / 2] (model kernel) and t[(K - KB_KMIN) / 2] (PSF kernel)
 void ka_register_short(KaFn* t);
 void ka_register_long(KaFn* t);
-void kb_register(KbFn* t);
+void kb_register(KbFn* t);    // 4 blocks per SM
+void kb_register5(KbFn* t);   // 5 blocks per SM
 
 }  // namespace gbk

@@ -345,6 +345,7 @@ typedef struct {
     const double* psf_u;    /* host: (psf_rank, kernel_size[1]) */
     const double* psf_v;    /* host: (psf_rank, kernel_size[0]) */
     int psf_band;           /* direct mode: output rows per PSF block (0 = automatic) */
+    int psf_blocks;         /* direct mode: PSF blocks resident per SM, 4 or 5 (0 = 4) */
 } gbkb200_batch_desc;
 
 int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);
