@@ -268,6 +268,44 @@ def autotune(w, data, err, nsets, budget_s=60.0):
     return tune_batched(w, data, err, nsets, budget_s=budget_s)
 
 
+def run_e2e(args, w, data, err, cfg, nsets, total, world, local):
+    """The same metric through the public API: every rank takes the whole batch
+    of host parameter dicts, packs and copies its share (pinned H2D),
+    evaluates it, reads its chi^2 back (D2H) and gathers all chi^2 values
+    (NCCL all_gather across the ranks)."""
+    import torch
+    from gbkfit_b200.batched import BatchedSMDisk
+    from gbkfit_b200.sharded import ShardedEvaluator
+    ev_api = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
+    sharded = ShardedEvaluator(ev_api)
+    d2h = nsets * 4
+    try:
+        for _ in range(max(1, args.warmup)):
+            sharded.evaluate(w.params, total)
+    except Exception:
+        print(f'e2e diagnostics: world {sharded.world} rank {sharded.rank} share '
+              f'{sharded.share(total)} max_sets {ev_api.max_sets} chunk {ev_api.chunk} '
+              f'total {total} shapes { {k: np.shape(v) for k, v in w.params.items()} }',
+              file=sys.stderr, flush=True)
+        raise
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        chi2_all = sharded.evaluate(w.params, total)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, world)
+    assert len(chi2_all) == total and np.all(np.isfinite(chi2_all))
+    h2d = int(ev_api.last_h2d_bytes)     # pinned input pieces copied per call
+    e2e = dict(value=total / e2e_s, unit=UNIT, h2d_bytes_per_step=h2d,
+               d2h_bytes_per_step=d2h, ms_per_step=e2e_s * 1e3,
+               gather_bytes_per_step=sharded.last_gather_bytes,
+               path='ShardedEvaluator(BatchedSMDisk).evaluate: host parameter dicts of all '
+                    f'{total} sets in, chi^2 of all sets out on every rank')
+
+    return e2e
+
+
 def run_b200(args):
     import torch
     from gbkfit_b200 import workloads
@@ -343,30 +381,9 @@ def run_b200(args):
                        ms_per_launch=round(t / n, 5), share=round(t / total, 4))
                for k, (t, n) in stages.items()}
 
-    # end to end through the public API: every rank takes the whole batch of
-    # host parameter dicts, packs and copies its share (pinned H2D), evaluates
-    # it, reads its chi^2 back (D2H) and gathers all chi^2 values (NCCL
-    # all_gather across the ranks)
-    ev_api = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
-    sharded = ShardedEvaluator(ev_api)
-    d2h = nsets * 4
-    for _ in range(max(1, args.warmup)):
-        sharded.evaluate(w.params, total)
-    torch.cuda.synchronize()
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        chi2_all = sharded.evaluate(w.params, total)
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, world)
-    assert len(chi2_all) == total and np.all(np.isfinite(chi2_all))
-    h2d = int(ev_api.last_h2d_bytes)     # pinned input pieces copied per call
-    e2e = dict(value=total / e2e_s, unit=UNIT, h2d_bytes_per_step=h2d,
-               d2h_bytes_per_step=d2h, ms_per_step=e2e_s * 1e3,
-               gather_bytes_per_step=sharded.last_gather_bytes,
-               path='ShardedEvaluator(BatchedSMDisk).evaluate: host parameter dicts of all '
-                    f'{total} sets in, chi^2 of all sets out on every rank')
-
+    e2e = None
+    if args.e2e:
+        e2e = run_e2e(args, w, data, err, cfg, nsets, total, world, local)
     out = None
     if rank == 0:
         n_chunks = (nsets + ev.chunk - 1) // ev.chunk
@@ -883,6 +900,8 @@ def main():
     ap.add_argument('--no-plain', dest='plain', action='store_false')
     ap.add_argument('--no-serving', dest='serving', action='store_false')
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
+    ap.add_argument('--no-e2e', dest='e2e', action='store_false',
+                    help='skip the end-to-end (public API) measurement')
     ap.add_argument('--no-parity', dest='parity', action='store_false',
                     help='skip the sampled parity check against the fp64 oracle')
     ap.add_argument('--conv', choices=['fft', 'direct'], default=None,

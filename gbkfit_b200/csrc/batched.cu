@@ -519,8 +519,10 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
     bt->ka = ka_fn(P.Kz);
     bt->kb = kb_fn(P.K, blocks);
-    GBK_CUDA_TRY(cudaFuncSetAttribute(bt->kb, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)bt->smemB));
+    {
+        const int rc = gbk_raise_smem_limit(reinterpret_cast<const void*>(bt->kb), bt->smemB);
+        if (rc) return rc;
+    }
     bt->nper = P.Nz * P.nbands;
     if (cudaMalloc(&bt->partials, (size_t)bt->max_sets * bt->nper * sizeof(double)) != cudaSuccess)
         return GBKB200_ERR_OOM;
@@ -744,11 +746,13 @@ extern "C" int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* 
         gbkb200_batch_destroy(bt);
         return GBKB200_ERR_UNSUPPORTED;
     }
-    cudaFuncSetAttribute(k1_model_xfft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bt->smem1);
-    cudaFuncSetAttribute(k5_c2r_residual, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)bt->smem5);
-    cudaFuncSetAttribute(k_lines, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)std::max(bt->smem_y, bt->smem_z));
+    if ((rc = gbk_raise_smem_limit(reinterpret_cast<const void*>(k1_model_xfft), bt->smem1)) ||
+        (rc = gbk_raise_smem_limit(reinterpret_cast<const void*>(k5_c2r_residual), bt->smem5)) ||
+        (rc = gbk_raise_smem_limit(reinterpret_cast<const void*>(k_lines),
+                                   std::max(bt->smem_y, bt->smem_z)))) {
+        gbkb200_batch_destroy(bt);
+        return rc;
+    }
     GBK_CUDA_TRY(cudaGetLastError());
     *out = bt;
     return GBKB200_OK;

@@ -1,6 +1,10 @@
 // Context (module object) management and error reporting of the C ABI.
 #include "gbk_common.cuh"
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include <new>
 
 static thread_local cudaError_t g_last_cuda_error = cudaSuccess;
@@ -110,4 +114,24 @@ extern "C" const char* gbkb200_error_string(int code)
 extern "C" const char* gbkb200_last_cuda_error(void)
 {
     return cudaGetErrorString(g_last_cuda_error);
+}
+
+namespace {
+std::mutex g_smem_mutex;
+std::map<std::pair<int, const void*>, size_t> g_smem_limits;   // (device, kernel) -> bytes
+}  // namespace
+
+int gbk_raise_smem_limit(const void* fn, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return GBKB200_OK;      // the default limit
+    int dev = 0;
+    GBK_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_smem_mutex);
+    size_t& cur = g_smem_limits[{dev, fn}];
+    if (bytes > cur) {
+        GBK_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)bytes));
+        cur = bytes;
+    }
+    return GBKB200_OK;
 }

@@ -94,7 +94,9 @@ __global__ void moments_kernel(int nx, int ny, int nz, float stz, float zz, cons
     const float m1 = valid ? (float)m1d : NAN;
     if (m < norders && orders[m] == 1) { md[i2 + sxy * m] = m1; m++; }
     if (maxo == 1) return;
-    const double var = fmax(s2 / s0 - m1d * m1d, 0.0);
+    // a negative variance (negative cube values, e.g. convolution ringing)
+    // gives NaN, as the reference's sqrt of its negative sum does
+    const double var = s2 / s0 - m1d * m1d;
     const float m2 = valid ? (float)sqrt(var) : NAN;
     if (m < norders && orders[m] == 2) { md[i2 + sxy * m] = m2; m++; }
     for (; m < norders; ++m) {

@@ -277,9 +277,7 @@ static int get_plan(FftState* st, const Size3& s, Plan** out)
 
 static int set_smem(const void* fn, size_t bytes)
 {
-    if (bytes > 48 * 1024)
-        GBK_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    return GBKB200_OK;
+    return gbk_raise_smem_limit(fn, bytes);
 }
 
 // x-pass launch helpers

@@ -83,6 +83,11 @@ struct gbkb200_ctx {
 };
 
 int gbk_finish(gbkb200_ctx* ctx);   // launch check, and sync + status read in sync mode
+// Raises kernel fn's dynamic shared-memory limit on the current device to at
+// least `bytes`, never lowering it: the limit is one setting per function,
+// shared by every evaluator and context of the process, so a smaller later
+// request must not cut under a larger earlier one.
+int gbk_raise_smem_limit(const void* fn, size_t bytes);
 int gbk_fft_state_destroy(gbkb200_ctx* ctx);
 
 // Debug builds (-DGBK_CHECKED) bounds-check the accesses of the batched and

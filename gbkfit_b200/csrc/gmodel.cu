@@ -610,10 +610,9 @@ int gbk_launch_smdisk(const DiskArgs& a, cudaStream_t stream, int* status)
         dim3 block(32, 8), grid((a.sx + 31) / 32, a.sy);
         size_t smem = a.scube ? (size_t)a.spec_size * 32 * sizeof(float) : 0;
         if (smem <= 200 * 1024) {
-            if (smem > 48 * 1024)
-                GBK_CUDA_TRY(cudaFuncSetAttribute(smdisk_thick_kernel<true>,
-                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  (int)smem));
+            const int rc = gbk_raise_smem_limit(
+                reinterpret_cast<const void*>(smdisk_thick_kernel<true>), smem);
+            if (rc) return rc;
             smdisk_thick_kernel<true><<<grid, block, smem, stream>>>(a, status);
         } else {
             smdisk_thick_kernel<false><<<grid, block, 0, stream>>>(a, status);

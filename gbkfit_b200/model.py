@@ -71,9 +71,22 @@ class _DiskComponent:
         d = self._disk
         dev = {}
         dev['subrnodes'] = driver.mem_copy_h2d(d.subrnodes.astype(np.float32))
+        # the per-call parameter arrays (common parameters, trait parameter
+        # values) share one device buffer, filled from one pinned host buffer
+        # by one copy per evaluation
+        sizes = [(name, d.common_size(name)) for name in ('vsys', 'xpos', 'ypos', 'posa', 'incl')
+                 if name in d.pdescs]
+        sizes += [(k, max(d.tables[k]['npv'], 1)) for k in KINDS if d.tables[k] is not None]
+        total = sum(n for _, n in sizes)
+        self._flat_d = torch.empty(total, dtype=torch.float32, device=driver.stream.device)
+        self._flat_h = torch.empty(total, dtype=torch.float32, pin_memory=True)
+        views, off = {}, 0
+        for name, n in sizes:
+            views[name] = (self._flat_d[off:off + n], self._flat_h[off:off + n].numpy())
+            off += n
+        self._views = views
         for name in ('vsys', 'xpos', 'ypos', 'posa', 'incl'):
-            dev[name] = (driver.mem_alloc_d(d.common_size(name), np.float32)
-                         if name in d.pdescs else None)
+            dev[name] = views[name][0] if name in views else None
         for k in KINDS:
             t = d.tables[k]
             if t is None:
@@ -83,7 +96,7 @@ class _DiskComponent:
                           cvalues=driver.mem_copy_h2d(t['cvalues']) if len(t['cvalues'])
                           else driver.mem_alloc_d(1, np.float32),
                           ccounts=driver.mem_copy_h2d(t['ccounts']),
-                          pvalues=driver.mem_alloc_d(max(t['npv'], 1), np.float32),
+                          pvalues=views[k][0],
                           pcounts=driver.mem_copy_h2d(t['pcounts']))
         if self.MC:
             dev['hasordint'] = driver.mem_copy_h2d(d.hasordint())
@@ -101,11 +114,15 @@ class _DiskComponent:
         packed = d.pack(params)
         for name in ('vsys', 'xpos', 'ypos', 'posa', 'incl'):
             if dev[name] is not None:
-                dev[name].copy_(torch.from_numpy(packed[name]))
+                self._views[name][1][:] = packed[name]
         for k in KINDS:
             if dev[k] is not None and packed[k]['pvalues'].size:
-                dev[k]['pvalues'][:packed[k]['pvalues'].size].copy_(
-                    torch.from_numpy(packed[k]['pvalues']))
+                self._views[k][1][:packed[k]['pvalues'].size] = packed[k]['pvalues']
+        # one copy on the driver's stream, ahead of the native call on the same
+        # stream; the call synchronises before returning, so the pinned buffer
+        # is free again for the next evaluation
+        with torch.cuda.stream(driver.stream):
+            self._flat_d.copy_(self._flat_h, non_blocking=True)
         shape = tuple(spat_size[::-1])
         extra = {}
         if out_extra is not None:

@@ -449,11 +449,22 @@ class ModelServer:
                 self.max_inflight_bytes = max(self.max_inflight_bytes, self._inflight)
             # the requests passed over go back to the front, in order
             self._queue.extendleft(reversed([r for k, r in enumerate(q) if k not in taken]))
-        for target, kind, what in launches:
-            if kind == 'group':
-                self._launch_group(target, what)
-            else:
-                self._launch(target, *what)
+        done = 0
+        try:
+            for target, kind, what in launches:
+                if kind == 'group':
+                    self._launch_group(target, what)
+                else:
+                    self._launch(target, *what)
+                done += 1
+        except BaseException as e:
+            # the requests taken for launches that did not start are in no
+            # queue, slot or group any more: fail their futures here
+            for target, kind, what in launches[done:]:
+                for r in (what if kind == 'group' else [what[0]]):
+                    if not r.future.done():
+                        r.future.set_exception(e)
+            raise
         return bool(launches)
 
     def _launch_group(self, ds, reqs):

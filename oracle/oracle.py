@@ -432,7 +432,7 @@ def chi2_gradient_f64(packed, geom, data, error, scale):
 
 def dcube_pipeline(packed, size, step, rpix, rval, scale, psf, lsf, precision='f64',
                    mask_cutoff=None, mask_apply=False, thick=False, image=False,
-                   opacity_packed=None):
+                   opacity_packed=None, fft_f32=False):
     """The reference's DCube chain with supersampling and masking
     (_dcube.py:128-313): the padded high-resolution grid (size x scale +
     kernel - 1, padded by backend.py:51-66), smdisk on it, FFT convolution
@@ -445,8 +445,9 @@ def dcube_pipeline(packed, size, step, rpix, rval, scale, psf, lsf, precision='f
     spectral cube (the intensity gmodels, intensity_2d/3d.py; size z is 1).
     opacity_packed: an opacity disk evaluated first into the 3-D spatial
     opacity cube (its density output), which the disk then reads
-    (intensity_3d.py:154-167, gmodels.hpp:933-937).  Returns (dcube_lo,
-    mcube_lo or None)."""
+    (intensity_3d.py:154-167, gmodels.hpp:933-937).  fft_f32: the FFT in
+    single precision (as FFTW's float plans of the reference driver) instead
+    of float64.  Returns (dcube_lo, mcube_lo or None)."""
     from gbkfit_b200.workloads import dcube_geometry
     o = Oracle(precision)
     real = o.real
@@ -479,7 +480,8 @@ def dcube_pipeline(packed, size, step, rpix, rval, scale, psf, lsf, precision='f
         l_ = (lsf or P.LSFPoint()).asarray(step_hi[2], sz, off[2])
         pc = (p * l_[:, None, None]).astype(real)
         pc = np.roll(pc, np.array(pc.shape) // 2 + 1, axis=(0, 1, 2))
-        cube = fft_convolve_cached(cube, pc).astype(real)
+        cube = fft_convolve_cached(cube, pc, dtype=np.float32 if fft_f32 else np.float64)
+        cube = cube.astype(real)
     nx, ny, nz = size
     lo = o.dcube_downscale(scale, edge, cube, (nz, ny, nx))
     mcube = None

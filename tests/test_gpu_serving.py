@@ -61,7 +61,7 @@ def test_chi2_matches_oracle(gpu, oracle_built):
     assert reqs
     with ModelServer(slots=4) as srv:
         _register(srv, stream)
-        got = [f.result()['chi2'] for f in [srv.submit(r) for r in reqs]]
+        got = [f.result(timeout=300)['chi2'] for f in [srv.submit(r) for r in reqs]]
     for r, c in zip(reqs, got):
         d = stream.datasets[r.dataset]
         m = scube_pipeline(r.disk.pack(r.params), d['geom'])
@@ -81,7 +81,7 @@ def test_admission_respects_hbm_budget(gpu):
         _register(srv, stream)
         futs = [srv.submit(r) for r in _requests(stream)]
         for f in futs:
-            assert np.isfinite(f.result()['chi2'])
+            assert np.isfinite(f.result(timeout=300)['chi2'])
         st = srv.stats()
     assert st['requests'] == len(futs)
     assert st['max_inflight_bytes'] <= budget - resident
@@ -109,12 +109,12 @@ def test_unregister_keeps_submitted_requests(gpu):
     kinds = [q['kind'] for q in stream.requests][:10]
     with ModelServer(slots=4) as srv:
         _register(srv, stream)
-        ref = [f.result()['chi2'] for f in [srv.submit(r) for r in _requests(stream)[:10]]]
+        ref = [f.result(timeout=300)['chi2'] for f in [srv.submit(r) for r in _requests(stream)[:10]]]
         futs = [srv.submit(r) for r in _requests(stream)[:10]]
         for d in stream.datasets:
             srv.unregister(d['key'])
         gc.collect()
-        got = [f.result()['chi2'] for f in futs]
+        got = [f.result(timeout=300)['chi2'] for f in futs]
         assert srv.datasets == {}
     for k, a, b in zip(kinds, ref, got):
         if k == 'smdisk':
@@ -139,12 +139,12 @@ def test_coalesced_smdisk_same_alone_and_in_mix(gpu):
     with ModelServer(slots=1) as alone:
         _register_coalesced(alone, stream)
         assert all(ds.batched is not None for ds in alone.datasets.values())
-        ref = [alone.evaluate(r)['chi2'] for r in _requests(stream)]
+        ref = [alone.submit(r).result(timeout=300)['chi2'] for r in _requests(stream)]
         assert alone.stats()['max_group'] == 1
     with ModelServer(slots=8) as mix:
         _register_coalesced(mix, stream)
         futs = [mix.submit(r) for r in _requests(stream)]
-        got = [f.result()['chi2'] for f in futs]
+        got = [f.result(timeout=300)['chi2'] for f in futs]
         assert mix.stats()['max_group'] > 1          # requests were coalesced
     for k, a, b in zip(kinds, ref, got):
         if k == 'smdisk':
@@ -162,10 +162,10 @@ def test_coalesced_chi2_matches_oracle_and_fft_path(gpu, oracle_built):
     reqs = [r for r in _requests(stream) if r.kind == 'smdisk'][:6]
     with ModelServer(slots=4) as srv:
         _register_coalesced(srv, stream)
-        got = [f.result()['chi2'] for f in [srv.submit(r) for r in reqs]]
+        got = [f.result(timeout=300)['chi2'] for f in [srv.submit(r) for r in reqs]]
     with ModelServer(slots=4) as srv:
         _register(srv, stream)
-        fft = [f.result()['chi2'] for f in [srv.submit(r) for r in _requests(stream)
+        fft = [f.result(timeout=300)['chi2'] for f in [srv.submit(r) for r in _requests(stream)
                                             if r.kind == 'smdisk'][:6]]
     for r, c, f in zip(reqs, got, fft):
         d = stream.datasets[r.dataset]
@@ -183,11 +183,11 @@ def test_coalesced_unregister_releases_budget(gpu):
     with ModelServer(slots=4) as srv:
         _register_coalesced(srv, stream)
         assert srv._resident > 0
-        ref = [f.result()['chi2'] for f in [srv.submit(r) for r in _requests(stream)]]
+        ref = [f.result(timeout=300)['chi2'] for f in [srv.submit(r) for r in _requests(stream)]]
         futs = [srv.submit(r) for r in _requests(stream)]
         for d in stream.datasets:
             srv.unregister(d['key'])
-        got = [f.result()['chi2'] for f in futs]
+        got = [f.result(timeout=300)['chi2'] for f in futs]
         assert srv._resident == 0 and srv._group_ds == []
     for a, b in zip(ref, got):
         assert abs(a - b) <= 1e-5 * abs(a)
