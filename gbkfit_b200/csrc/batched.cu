@@ -213,25 +213,33 @@ __global__ void __launch_bounds__(256) k_lines(float2* data, long long set_strid
     const int o = blockIdx.x / tiles;
     const int i0 = (blockIdx.x % tiles) * BLT;
     const long long base = (long long)blockIdx.y * set_stride + (long long)o * so + i0;
-    for (int e = threadIdx.x; e < BLT * n; e += blockDim.x) {
-        int l = e % BLT, k = e / BLT;
-        const long long gi = base + l + k * sk;
-        b0[k * BLT + l] = (i0 + l < inner && k < nload && GBK_OK_IDX(gi, lim_data, 10))
-                              ? data[gi] : make_float2(0.f, 0.f);
-    }
+    staged_copy<8>(
+        BLT * n,
+        [&](int e) {
+            const int l = e % BLT, k = e / BLT;
+            const long long gi = base + l + k * sk;
+            return (i0 + l < inner && k < nload && GBK_OK_IDX(gi, lim_data, 10))
+                       ? data[gi] : make_float2(0.f, 0.f);
+        },
+        [&](int e, float2 v) { b0[e] = v; });
     __syncthreads();
     float2* res = fft_smem(b0, b1, ax, BLT, BLT, 1, false, s_tw, mode == 0 ? inv != 0 : false);
     if (mode == 1) {
         const long long sbase = (long long)o * spec_so + i0;
-        for (int e = threadIdx.x; e < BLT * n; e += blockDim.x) {
-            int l = e % BLT, k = e / BLT;
-            if (i0 + l < inner && GBK_OK_IDX(sbase + l + k * spec_sk, lim_spec, 11)) {
-                float2 a = res[k * BLT + l];
-                float2 w = spec[sbase + l + k * spec_sk];
-                res[k * BLT + l] = make_float2((a.x * w.x - a.y * w.y) * scale,
-                                               (a.x * w.y + a.y * w.x) * scale);
-            }
-        }
+        staged_copy<8>(
+            BLT * n,
+            [&](int e) {
+                const int l = e % BLT, k = e / BLT;
+                return (i0 + l < inner && GBK_OK_IDX(sbase + l + k * spec_sk, lim_spec, 11))
+                           ? spec[sbase + l + k * spec_sk] : make_float2(0.f, 0.f);
+            },
+            [&](int e, float2 w) {
+                if (i0 + e % BLT < inner) {
+                    const float2 a = res[e];
+                    res[e] = make_float2((a.x * w.x - a.y * w.y) * scale,
+                                         (a.x * w.y + a.y * w.x) * scale);
+                }
+            });
         __syncthreads();
         res = fft_smem(res, res == b0 ? b1 : b0, ax, BLT, BLT, 1, false, s_tw, true);
     }

@@ -48,16 +48,19 @@ __global__ void __launch_bounds__(FFT_THREADS) x_r2c_kernel(const float* in, flo
     const bool even = (nx & 1) == 0;
     if (even) load_twiddles(s_post, post, hx);
     const long long row0 = (long long)blockIdx.x * L;
-    for (int e = threadIdx.x; e < L * M; e += blockDim.x) {
-        int l = e / M, m = e % M;
-        long long row = row0 + l;
-        float2 v = make_float2(0.f, 0.f);
-        if (row < rows) {
-            if (even) v = reinterpret_cast<const float2*>(in + row * nx)[m];
-            else v = make_float2(in[row * nx + m], 0.f);
-        }
-        b0[l * M + m] = v;
-    }
+    staged_copy<8>(
+        L * M,
+        [&](int e) {
+            const int l = e / M, m = e % M;
+            const long long row = row0 + l;
+            float2 v = make_float2(0.f, 0.f);
+            if (row < rows) {
+                if (even) v = reinterpret_cast<const float2*>(in + row * nx)[m];
+                else v = make_float2(in[row * nx + m], 0.f);
+            }
+            return v;
+        },
+        [&](int e, float2 v) { b0[e] = v; });
     __syncthreads();
     float2* z = fft_smem(b0, b1, ax, L, 1, M, true, s_tw, false);
     for (int e = threadIdx.x; e < L * hx; e += blockDim.x) {
@@ -97,25 +100,46 @@ __global__ void __launch_bounds__(FFT_THREADS) x_c2r_kernel(const float2* in, fl
     if (even) load_twiddles(s_post, post, hx);
     __syncthreads();
     const long long row0 = (long long)blockIdx.x * L;
-    for (int e = threadIdx.x; e < L * M; e += blockDim.x) {
-        int l = e / M, k = e % M;
-        long long row = row0 + l;
-        float2 v = make_float2(0.f, 0.f);
-        if (row < rows) {
-            const float2* r = in + row * hx;
-            if (even) {
-                // Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k])
-                float2 a = r[k], b = conjf2(r[M - k]);
-                float2 s = cadd(a, b), d = csub(a, b);
-                float2 w = conjf2(s_post[k]);
-                float2 t = cmul(w, d);
-                v = make_float2(s.x - t.y, s.y + t.x);
-            } else {
-                // full Hermitian extension
-                v = k < hx ? r[k] : conjf2(r[nx - k]);
-            }
+    if (even) {
+        // Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k]): the two
+        // halves are staged first (b0: X[k], b1: X[M-k]), then combined
+        staged_copy<8>(
+            L * M,
+            [&](int e) {
+                const int l = e / M, k = e % M;
+                const long long row = row0 + l;
+                return row < rows ? in[row * hx + k] : make_float2(0.f, 0.f);
+            },
+            [&](int e, float2 v) { b0[e] = v; });
+        staged_copy<8>(
+            L * M,
+            [&](int e) {
+                const int l = e / M, k = e % M;
+                const long long row = row0 + l;
+                return row < rows ? in[row * hx + M - k] : make_float2(0.f, 0.f);
+            },
+            [&](int e, float2 v) { b1[e] = v; });
+        __syncthreads();
+        for (int e = threadIdx.x; e < L * M; e += blockDim.x) {
+            const int k = e % M;
+            const float2 a = b0[e], b = conjf2(b1[e]);
+            const float2 s = cadd(a, b), d = csub(a, b);
+            const float2 w = conjf2(s_post[k]);
+            const float2 t = cmul(w, d);
+            b0[e] = make_float2(s.x - t.y, s.y + t.x);
         }
-        b0[l * M + k] = v;
+    } else {
+        // full Hermitian extension
+        staged_copy<8>(
+            L * M,
+            [&](int e) {
+                const int l = e / M, k = e % M;
+                const long long row = row0 + l;
+                if (row >= rows) return make_float2(0.f, 0.f);
+                const float2* r = in + row * hx;
+                return k < hx ? r[k] : conjf2(r[nx - k]);
+            },
+            [&](int e, float2 v) { b0[e] = v; });
     }
     __syncthreads();
     float2* z = fft_smem(b0, b1, ax, L, 1, M, true, s_tw, true);
@@ -151,22 +175,30 @@ __global__ void __launch_bounds__(FFT_THREADS) lines_kernel(float2* data, int in
     const int o = blockIdx.x / tiles;
     const int i0 = (blockIdx.x % tiles) * LT;
     const long long base = (long long)o * so + i0;
-    for (int e = threadIdx.x; e < LT * n; e += blockDim.x) {
-        int l = e % LT, k = e / LT;
-        b0[k * LT + l] = (i0 + l < inner) ? data[base + l + k * sk] : make_float2(0.f, 0.f);
-    }
+    staged_copy<8>(
+        LT * n,
+        [&](int e) {
+            const int l = e % LT, k = e / LT;
+            return (i0 + l < inner) ? data[base + l + k * sk] : make_float2(0.f, 0.f);
+        },
+        [&](int e, float2 v) { b0[e] = v; });
     __syncthreads();
     float2* res = fft_smem(b0, b1, ax, LT, LT, 1, false, s_tw, mode == 0 ? inv != 0 : false);
     if (mode == 1) {
-        for (int e = threadIdx.x; e < LT * n; e += blockDim.x) {
-            int l = e % LT, k = e / LT;
-            if (i0 + l < inner) {
-                float2 a = res[k * LT + l];
-                float2 b = spec[base + l + k * sk];
-                float2 p = make_float2((a.x * b.x - a.y * b.y) * scale, (a.x * b.y + a.y * b.x) * scale);
-                res[k * LT + l] = p;
-            }
-        }
+        staged_copy<8>(
+            LT * n,
+            [&](int e) {
+                const int l = e % LT, k = e / LT;
+                return (i0 + l < inner) ? spec[base + l + k * sk] : make_float2(0.f, 0.f);
+            },
+            [&](int e, float2 b) {
+                const int l = e % LT;
+                if (i0 + l < inner) {
+                    const float2 a = res[e];
+                    res[e] = make_float2((a.x * b.x - a.y * b.y) * scale,
+                                         (a.x * b.y + a.y * b.x) * scale);
+                }
+            });
         __syncthreads();
         float2* other = (res == b0) ? b1 : b0;
         res = fft_smem(res, other, ax, LT, LT, 1, false, s_tw, true);

@@ -183,4 +183,26 @@ __device__ __forceinline__ void load_twiddles(float2* s_tw, const float2* g_tw, 
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_tw[i] = g_tw[i];
 }
 
+// Element-wise copy of count elements in rounds of U per thread: the U global
+// loads of a round are issued before any of their results is used, so each
+// thread keeps U loads in flight (load(e) reads element e, store(e, v) writes
+// it; elements e >= count are neither read nor written).
+template<int U, typename Load, typename Store>
+__device__ __forceinline__ void staged_copy(int count, Load load, Store store)
+{
+    for (int e0 = threadIdx.x; e0 < count; e0 += U * (int)blockDim.x) {
+        float2 v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * (int)blockDim.x;
+            v[u] = e < count ? load(e) : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * (int)blockDim.x;
+            if (e < count) store(e, v[u]);
+        }
+    }
+}
+
 }  // namespace gbk
