@@ -329,8 +329,8 @@ def run_b200(args):
         cfg['chunk'] = args.chunk
     if args.band:
         cfg['band'] = args.band
-    if args.psf_blocks:
-        cfg['psf_blocks'] = args.psf_blocks
+    if args.psf_variant >= 0:
+        cfg['psf_variant'] = args.psf_variant
     ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
     bufs = ev.alloc_inputs(nsets)
     ev.upload(ev.pack(mine, nsets), bufs, nsets)
@@ -376,9 +376,9 @@ def run_b200(args):
     stages = ev.stage_times()
     counters = ev.work_counters()
     ev.set_timing(False)
-    total = sum(t for t, _ in stages.values())
+    tsum = sum(t for t, _ in stages.values())
     kernels = {k: dict(launches_per_step=n / args.steps, ms_per_step=round(t / args.steps, 4),
-                       ms_per_launch=round(t / n, 5), share=round(t / total, 4))
+                       ms_per_launch=round(t / n, 5), share=round(t / tsum, 4))
                for k, (t, n) in stages.items()}
 
     e2e = None
@@ -907,8 +907,8 @@ def main():
     ap.add_argument('--conv', choices=['fft', 'direct'], default=None,
                     help='force the convolution mode (default: tuned)')
     ap.add_argument('--chunk', type=int, default=0, help='force the sets per wave (default: tuned)')
-    ap.add_argument('--psf-blocks', type=int, default=0, choices=[0, 4, 5],
-                    help='PSF kernel resident blocks per SM of the direct mode (default: tuned)')
+    ap.add_argument('--psf-variant', type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5],
+                    help='PSF kernel variant of the direct mode (default: tuned)')
     ap.add_argument('--band', type=int, default=0,
                     help='force the output rows per PSF block of the direct mode (default: tuned)')
     ap.add_argument('--workload', default='smdisk_batch128',

@@ -8,7 +8,9 @@ Knobs (all change speed only, never results beyond fp32 rounding):
   should stay in L2);
 * ``band``: output rows per PSF block of the direct mode (smaller bands: more
   resident blocks, more halo rows);
-* ``psf_blocks``: PSF kernel sized for 4 or 5 resident blocks per SM;
+* ``psf_variant``: PSF kernel sized for 4 or 5 resident blocks per SM, with
+  its residual in a separate pass or in the y-FIR items (data loaded after or
+  before each item's FIR);
 * ``rows_k1``: spectral rows per shared-memory group of the model kernel.
 
 Coordinate descent from the defaults; every trial builds an evaluator and
@@ -96,7 +98,8 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
         c = _load().get(key)
         if c:
             return dict(fft_size=tuple(c['fft_size']), chunk=c['chunk'], rows_k1=c['rows_k1'],
-                        conv=c['conv'], band=c.get('band', 0), psf_blocks=c.get('psf_blocks', 0))
+                        conv=c['conv'], band=c.get('band', 0),
+                        psf_variant=c.get('psf_variant', 0))
     g = w.geom
     t_end = time.time() + budget_s
     # direct separable convolution (when the PSF is rank 1): chunk, then band
@@ -114,12 +117,10 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
             t = time_config(w, data, err, nsets, cfg)
             if t < best_dt:
                 best_d, best_dt = cfg, t
-        # PSF kernel sized for 5 resident blocks per SM (fewer registers and
-        # shared memory per block)
-        for band in (0, 96, 64):
-            if band and band >= g.size[1]:
-                continue
-            cfg = dict(best_d, band=band, psf_blocks=5)
+        # the PSF kernel's variants (resident blocks per SM x epilogue)
+        base = dict(best_d)
+        for variant in range(1, 6):
+            cfg = dict(base, psf_variant=variant)
             t = time_config(w, data, err, nsets, cfg)
             if t < best_dt:
                 best_d, best_dt = cfg, t

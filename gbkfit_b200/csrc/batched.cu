@@ -29,6 +29,7 @@
 #include "gbk_fft.cuh"
 
 #include <climits>
+#include <mutex>
 #include <cmath>
 #include <vector>
 
@@ -409,15 +410,15 @@ static KaFn ka_fn(int Kz)
     return t[Kz / 2];
 }
 
-static KbFn kb_fn(int K, int blocks)
+static KbFn kb_fn(int K, int variant)
 {
-    static KbFn t4[(KB_KMAX - KB_KMIN) / 2 + 1] = {};
-    static KbFn t5[(KB_KMAX - KB_KMIN) / 2 + 1] = {};
-    if (!t4[0]) {
-        kb_register(t4);
-        kb_register5(t5);
-    }
-    return (blocks == 5 ? t5 : t4)[(K - KB_KMIN) / 2];
+    static KbFn t[KB_VARIANTS][(KB_KMAX - KB_KMIN) / 2 + 1] = {};
+    static std::once_flag once;
+    std::call_once(once, [] {
+        kb_register4(t);
+        kb_register5(t + 3);
+    });
+    return t[variant][(K - KB_KMIN) / 2];
 }
 
 // Direct-mode setup: reversed FIR coefficients, plane buffers, the data's
@@ -491,8 +492,11 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     const long long xr_bytes = (long long)(P.band + P.K - 1) * P.nch * sizeof(int);
     const long long need_min = (long long)(P.K + 15) * bpmax;
     const long long need_all = (long long)(P.band + P.K + 7) * bpmax;
-    // shared memory per block: 55 KB for 4 resident blocks per SM, 43 KB for 5
-    const int blocks = d->psf_blocks == 5 ? 5 : 4;
+    // PSF kernel variant: 0-2 sized for 4 resident blocks per SM, 3-5 for 5,
+    // epilogue (variant % 3) as in kb_psf_residual; shared memory per block:
+    // 55 KB for 4 blocks per SM, 43 KB for 5
+    if (d->psf_variant < 0 || d->psf_variant >= KB_VARIANTS) return GBKB200_ERR_INVALID_ARG;
+    const int blocks = d->psf_variant >= 3 ? 5 : 4;
     const long long budget = blocks == 5 ? 43LL * 1024 : 55LL * 1024;
     const long long cap = std::max(need_min, std::min(need_all, (budget - xr_bytes) / 4));
     if (cap * (long long)sizeof(float) + xr_bytes > 227LL * 1024) return GBKB200_ERR_UNSUPPORTED;
@@ -526,7 +530,7 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     GBK_CUDA_TRY(cudaGetLastError());
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
     bt->ka = ka_fn(P.Kz);
-    bt->kb = kb_fn(P.K, blocks);
+    bt->kb = kb_fn(P.K, d->psf_variant);
     {
         const int rc = gbk_raise_smem_limit(reinterpret_cast<const void*>(bt->kb), bt->smemB);
         if (rc) return rc;

@@ -250,7 +250,12 @@ constexpr int KB_NX_MAX = 512;  // widest data cube of the direct mode
 // MINB: resident blocks per SM the registers are sized for (4: up to 128
 // registers a thread; 5: up to 102, with the shared memory per block sized to
 // match, see setup_direct)
-template<int K, int MINB>
+// EPI: how the y FIR meets the residual.  0: y FIR in place in rounds of
+// items with a barrier between loads and stores, then a residual pass over the
+// pass's rows reading shared memory; 1: the residual in each y-FIR item's
+// epilogue (no write-back, no barriers between items), its data loaded after
+// the item's FIR; 2: as 1, with the item's data requested before its FIR.
+template<int K, int MINB, int EPI>
 __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelArgs P)
 {
     constexpr int NW = (K + 7 + 3) / 4;     // float4 slots of one 8-output x window
@@ -439,77 +444,210 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
             }
         }
         __syncthreads();
-        // y FIR with the residual in its epilogue: item (8-row group rb, float4
-        // column s4) computes model(ys + rb + q, xb0 + 4 s4 + j) = sum_t ur[t]
-        // S[rb + q + t][4 s4 + j] for q < 8, j < 4 in registers, on packed FP32
-        // pairs (FFMA2: two lanes of fma, each rounded as fmaf), then compares
-        // them with the data (crop + residual, objective.hpp:7-31) and adds
-        // r^2.  S is only read here, so items need no barriers between them.
-        {
-            const int nitems = ng * ns4;
-            const bool vec = (P.Nx & 3) == 0;
-            float2 s2 = make_float2(0.f, 0.f);
-            for (int item = threadIdx.x; item < nitems; item += KB_THREADS) {
-                const int rb = 8 * (item / ns4), s4 = item % ns4;
-                float2 acc[8][2];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    acc[q][0] = make_float2(0.f, 0.f);
-                    acc[q][1] = make_float2(0.f, 0.f);
-                }
-                const float4* colp = reinterpret_cast<const float4*>(S) + rb * bp4 + s4;
-#pragma unroll
-                for (int m = 0; m < K + 7; ++m) {
-                    const float4 p = colp[m * bp4];
-                    const float2 pxy = make_float2(p.x, p.y), pzw = make_float2(p.z, p.w);
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const int t = m - q;
-                        if (t >= 0 && t < K) {
-                            acc[q][0] = __ffma2_rn(P.ur2[t], pxy, acc[q][0]);
-                            acc[q][1] = __ffma2_rn(P.ur2[t], pzw, acc[q][1]);
+        if constexpr (EPI == 0) {
+            constexpr int kIt = 1;     // y items per thread and round
+            // y FIR in place: model(yo, xo) = sum_t ur[t] S[yo + t][xo], written to S row yo.
+            // Packed FP32 pairs (FFMA2: two lanes of fma, each rounded as fmaf),
+            // columns (x, x+1) and (x+2, x+3) of a float4 per instruction.  Items
+            // (8-row group, float4 column) in ascending order, KB_THREADS x kIt
+            // per round, loads before the round's barrier and stores after it: a
+            // column's group is written only after every lower group of that
+            // column, the only readers of its rows, has loaded them.
+            {
+                float2 u2[K];
+    #pragma unroll
+                for (int t = 0; t < K; ++t) u2[t] = make_float2(P.ur[t], P.ur[t]);
+                const int nitems = ng * ns4;
+                for (int gr0 = 0; gr0 < nitems; gr0 += KB_THREADS * kIt) {
+                    float2 acc[kIt][8][2];
+    #pragma unroll
+                    for (int it = 0; it < kIt; ++it) {
+                        const int item = gr0 + threadIdx.x + it * KB_THREADS;
+    #pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            acc[it][q][0] = make_float2(0.f, 0.f);
+                            acc[it][q][1] = make_float2(0.f, 0.f);
+                        }
+                        if (item < nitems) {
+                            const int rb = 8 * (item / ns4), s4 = item % ns4;
+                            const float4* colp = reinterpret_cast<const float4*>(S) + rb * bp4 + s4;
+    #pragma unroll
+                            for (int m = 0; m < K + 7; ++m) {
+                                const float4 p = colp[m * bp4];
+                                const float2 pxy = make_float2(p.x, p.y), pzw = make_float2(p.z, p.w);
+    #pragma unroll
+                                for (int q = 0; q < 8; ++q) {
+                                    const int t = m - q;
+                                    if (t >= 0 && t < K) {
+                                        acc[it][q][0] = __ffma2_rn(u2[t], pxy, acc[it][q][0]);
+                                        acc[it][q][1] = __ffma2_rn(u2[t], pzw, acc[it][q][1]);
+                                    }
+                                }
+                            }
                         }
                     }
-                }
-                const int xo = xb0 + 4 * s4;
-                if (xo >= xb_end) continue;
-                if (vec) {
-                    // Nx % 4 == 0: a float4 column lies wholly inside or outside the crop
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const int yo = ys + rb + q;
-                        if (yo >= ye) break;
-                        const int vi = pbase + yo * P.Nx + xo;
-                        const float4 o = *reinterpret_cast<const float4*>(P.obs + vi);
-                        const float4 w = *reinterpret_cast<const float4*>(P.iw + vi);
-                        const float2 r01 = __fmul2_rn(__fadd2_rn(acc[q][0], make_float2(-o.x, -o.y)),
-                                                      make_float2(w.x, w.y));
-                        const float2 r23 = __fmul2_rn(__fadd2_rn(acc[q][1], make_float2(-o.z, -o.w)),
-                                                      make_float2(w.z, w.w));
-                        s2 = __ffma2_rn(r01, r01, s2);
-                        s2 = __ffma2_rn(r23, r23, s2);
-                        if (model)
-                            *reinterpret_cast<float4*>(model + (vi - pbase)) =
-                                make_float4(acc[q][0].x, acc[q][0].y, acc[q][1].x, acc[q][1].y);
-                    }
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const int yo = ys + rb + q;
-                        if (yo >= ye) break;
-                        const float mv[4] = {acc[q][0].x, acc[q][0].y, acc[q][1].x, acc[q][1].y};
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            if (xo + j >= xb_end) break;
-                            const int vi = pbase + yo * P.Nx + xo + j;
-                            const float r0 = (mv[j] - P.obs[vi]) * P.iw[vi];
-                            s2.x = fmaf(r0, r0, s2.x);
-                            if (model) model[yo * P.Nx + xo + j] = mv[j];
+                    __syncthreads();
+    #pragma unroll
+                    for (int it = 0; it < kIt; ++it) {
+                        const int item = gr0 + threadIdx.x + it * KB_THREADS;
+                        if (item < nitems) {
+                            const int rb = 8 * (item / ns4), s4 = item % ns4;
+    #pragma unroll
+                            for (int q = 0; q < 8; ++q)
+                                if (ys + rb + q < ye)
+                                    reinterpret_cast<float4*>(S)[(rb + q) * bp4 + s4] =
+                                        make_float4(acc[it][q][0].x, acc[it][q][0].y,
+                                                    acc[it][q][1].x, acc[it][q][1].y);
                         }
                     }
+                    __syncthreads();
                 }
             }
-            sum += s2.x + s2.y;
+            // crop + residual over rows [ys, ye), columns [xb0, xb_end)
+            if ((P.Nx & 3) == 0) {
+                // flat float4 index over the pass, stepped without divisions
+                const int nv = (xb_end - xb0) >> 2;        // xb0 and xb_end are multiples of 4
+                const int n = (ye - ys) * nv;
+                const int dq = KB_THREADS / nv, dr = KB_THREADS % nv;
+                int row = threadIdx.x / nv, col = threadIdx.x % nv;
+                // running offsets: si in S (float4), vi in the data plane (float)
+                int si = row * bp4 + col, vi = pbase + (ys + row) * P.Nx + xb0 + 4 * col;
+                const int dsi = dq * bp4 + dr, dvi = dq * P.Nx + 4 * dr;
+                float2 s2 = make_float2(0.f, 0.f);
+    #pragma unroll 4
+                for (int i = threadIdx.x; i < n; i += KB_THREADS) {
+                    const float4 m = reinterpret_cast<const float4*>(S)[si];
+                    const float4 o = *reinterpret_cast<const float4*>(P.obs + vi);
+                    const float4 w = *reinterpret_cast<const float4*>(P.iw + vi);
+                    // packed pairs: r = (m - o) w, s2 += r^2
+                    const float2 r01 = __fmul2_rn(__fadd2_rn(make_float2(m.x, m.y),
+                                                             make_float2(-o.x, -o.y)),
+                                                  make_float2(w.x, w.y));
+                    const float2 r23 = __fmul2_rn(__fadd2_rn(make_float2(m.z, m.w),
+                                                             make_float2(-o.z, -o.w)),
+                                                  make_float2(w.z, w.w));
+                    s2 = __ffma2_rn(r01, r01, s2);
+                    s2 = __ffma2_rn(r23, r23, s2);
+                    if (model) *reinterpret_cast<float4*>(model + (vi - pbase)) = m;
+                    col += dr;
+                    si += dsi;
+                    vi += dvi;
+                    if (col >= nv) {
+                        col -= nv;
+                        si += bp4 - nv;
+                        vi += P.Nx - 4 * nv;
+                    }
+                }
+                sum += s2.x + s2.y;
+            } else {
+                const int nw = xb_end - xb0, n = (ye - ys) * nw;
+                for (int i = threadIdx.x; i < n; i += KB_THREADS) {
+                    const int row = i / nw, col = i % nw;
+                    const int yo = ys + row, xo = xb0 + col;
+                    const float m = S[row * bp + col];
+                    const int vi = pbase + yo * P.Nx + xo;
+                    const float r0 = (m - P.obs[vi]) * P.iw[vi];
+                    sum += r0 * r0;
+                    if (model) model[yo * P.Nx + xo] = m;
+                }
+            }
+        } else {
+            // y FIR with the residual in its epilogue: item (8-row group rb, float4
+            // column s4) computes model(ys + rb + q, xb0 + 4 s4 + j) = sum_t ur[t]
+            // S[rb + q + t][4 s4 + j] for q < 8, j < 4 in registers, on packed FP32
+            // pairs (FFMA2: two lanes of fma, each rounded as fmaf), then compares
+            // them with the data (crop + residual, objective.hpp:7-31) and adds
+            // r^2.  S is only read here, so items need no barriers between them.
+            {
+                const int nitems = ng * ns4;
+                const bool vec = (P.Nx & 3) == 0;
+                float2 s2 = make_float2(0.f, 0.f);
+                for (int item = threadIdx.x; item < nitems; item += KB_THREADS) {
+                    const int rb = 8 * (item / ns4), s4 = item % ns4;
+                    float2 acc[8][2];
+    #pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        acc[q][0] = make_float2(0.f, 0.f);
+                        acc[q][1] = make_float2(0.f, 0.f);
+                    }
+                    const int xo = xb0 + 4 * s4;
+                    const bool inside = xo < xb_end;
+                    // the item's data and weights, requested before its FIR so that
+                    // their loads are in flight while the multiply-adds run
+                    // (Nx % 4 == 0: a float4 column lies wholly inside or outside the crop)
+                    float4 ov[8], wv[8];
+                    if (EPI == 2 && vec) {
+    #pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int yo = ys + rb + q;
+                            if (inside && yo < ye) {
+                                const int vi = pbase + yo * P.Nx + xo;
+                                ov[q] = __ldg(reinterpret_cast<const float4*>(P.obs + vi));
+                                wv[q] = __ldg(reinterpret_cast<const float4*>(P.iw + vi));
+                            } else {
+                                ov[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+                                wv[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+                            }
+                        }
+                    }
+                    const float4* colp = reinterpret_cast<const float4*>(S) + rb * bp4 + s4;
+    #pragma unroll
+                    for (int m = 0; m < K + 7; ++m) {
+                        const float4 p = colp[m * bp4];
+                        const float2 pxy = make_float2(p.x, p.y), pzw = make_float2(p.z, p.w);
+    #pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int t = m - q;
+                            if (t >= 0 && t < K) {
+                                acc[q][0] = __ffma2_rn(P.ur2[t], pxy, acc[q][0]);
+                                acc[q][1] = __ffma2_rn(P.ur2[t], pzw, acc[q][1]);
+                            }
+                        }
+                    }
+                    if (!inside) continue;
+                    if (vec) {
+    #pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int yo = ys + rb + q;
+                            if (yo >= ye) break;
+                            const int vi = pbase + yo * P.Nx + xo;
+                            float4 o, w;
+                            if constexpr (EPI == 2) {
+                                o = ov[q];
+                                w = wv[q];
+                            } else {
+                                o = __ldg(reinterpret_cast<const float4*>(P.obs + vi));
+                                w = __ldg(reinterpret_cast<const float4*>(P.iw + vi));
+                            }
+                            const float2 r01 = __fmul2_rn(__fadd2_rn(acc[q][0], make_float2(-o.x, -o.y)),
+                                                          make_float2(w.x, w.y));
+                            const float2 r23 = __fmul2_rn(__fadd2_rn(acc[q][1], make_float2(-o.z, -o.w)),
+                                                          make_float2(w.z, w.w));
+                            s2 = __ffma2_rn(r01, r01, s2);
+                            s2 = __ffma2_rn(r23, r23, s2);
+                            if (model)
+                                *reinterpret_cast<float4*>(model + (vi - pbase)) =
+                                    make_float4(acc[q][0].x, acc[q][0].y, acc[q][1].x, acc[q][1].y);
+                        }
+                    } else {
+    #pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int yo = ys + rb + q;
+                            if (yo >= ye) break;
+                            const float mv[4] = {acc[q][0].x, acc[q][0].y, acc[q][1].x, acc[q][1].y};
+    #pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                if (xo + j >= xb_end) break;
+                                const int vi = pbase + yo * P.Nx + xo + j;
+                                const float r0 = (mv[j] - P.obs[vi]) * P.iw[vi];
+                                s2.x = fmaf(r0, r0, s2.x);
+                                if (model) model[yo * P.Nx + xo + j] = mv[j];
+                            }
+                        }
+                    }
+                }
+                sum += s2.x + s2.y;
+            }
         }
         __syncthreads();    // S is reloaded by the next pass
     }
@@ -545,7 +683,9 @@ static_assert(KA_KMAX <= 33 && KB_KMAX <= 33, "coefficient arrays of BatchKernel
 // fill t[Kz / 2] (model kernel) and t[(K - KB_KMIN) / 2] (PSF kernel)
 void ka_register_short(KaFn* t);
 void ka_register_long(KaFn* t);
-void kb_register(KbFn* t);    // 4 blocks per SM
-void kb_register5(KbFn* t);   // 5 blocks per SM
+// t[v][(K - KB_KMIN) / 2] for the PSF kernel variant v = 3 * (MINB == 5) + EPI
+constexpr int KB_VARIANTS = 6;
+void kb_register4(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1]);   // MINB 4, EPI 0-2
+void kb_register5(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1]);   // MINB 5, EPI 0-2
 
 }  // namespace gbk

@@ -82,6 +82,8 @@ class ShardedEvaluator:
         return out
 
     def evaluate(self, params, nsets):
+        if int(nsets) != nsets or nsets < 0:
+            raise ValueError(f"a batch of {nsets!r} sets")
         nsets = int(nsets)
         mine = self._local(params, nsets)
         if self.world == 1:

@@ -345,7 +345,10 @@ typedef struct {
     const double* psf_u;    /* host: (psf_rank, kernel_size[1]) */
     const double* psf_v;    /* host: (psf_rank, kernel_size[0]) */
     int psf_band;           /* direct mode: output rows per PSF block (0 = automatic) */
-    int psf_blocks;         /* direct mode: PSF blocks resident per SM, 4 or 5 (0 = 4) */
+    int psf_variant;        /* direct mode: PSF kernel variant 0-5: resident blocks per SM
+                             * (0-2: 4, 3-5: 5) x epilogue (variant % 3: 0 residual pass,
+                             * 1 residual in the y-FIR items, 2 as 1 with the data
+                             * prefetched); 0 = the first */
 } gbkb200_batch_desc;
 
 int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);

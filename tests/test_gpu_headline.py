@@ -14,7 +14,7 @@ gmodels.hpp:646-958, _dcube.py:245-313, objective.hpp:8-31):
 * chi^2: relative error <= 1e-4.
 
 Every other shape the autotuner can pick for this workload (sets per wave,
-output rows per PSF block, PSF kernel sized for 4 or 5 resident blocks per SM)
+output rows per PSF block, PSF kernel variants)
 gives the same chi^2 and model cubes within fp32 rounding.
 """
 
@@ -85,8 +85,10 @@ def test_headline_set_vs_fp64_oracle(headline, oracle_built, i):
 @pytest.mark.parametrize('cfg', [dict(chunk=32), dict(chunk=128), dict(chunk=256),
                                  dict(chunk=512, band=96), dict(chunk=512, band=64),
                                  dict(chunk=512, band=48), dict(chunk=512, band=32),
-                                 dict(chunk=512, psf_blocks=5),
-                                 dict(chunk=512, band=64, psf_blocks=5)])
+                                 dict(chunk=512, psf_variant=1), dict(chunk=512, psf_variant=2),
+                                 dict(chunk=512, psf_variant=3), dict(chunk=512, psf_variant=4),
+                                 dict(chunk=512, psf_variant=5),
+                                 dict(chunk=512, band=64, psf_variant=2)])
 def test_headline_tuner_shapes_agree(headline, cfg):
     """The other direct-mode shapes of the autotuner's search give the same
     results: chi^2 of all 512 sets within 1e-6 relative, sampled cubes
