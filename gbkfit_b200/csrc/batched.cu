@@ -174,8 +174,9 @@ __global__ void __launch_bounds__(512) k1_model_xfft(BatchKernelArgs P, int* sta
         // even/odd split into hx = M + 1 bins, stored as rows (z, y, kx)
         float2* out = P.work + (((long long)c * P.Wz + g0) * P.Py + y) * P.hx;
         const long long zs = (long long)P.Py * P.hx;
+        const unsigned long long mhx = fdiv_magic(P.hx);
         for (int e = threadIdx.x; e < gn * P.hx; e += blockDim.x) {
-            int l = e / P.hx, k = e % P.hx;
+            const int l = fdiv(e, mhx), k = e - l * P.hx;
             float2 zk = r[l * M + (k % M)];
             float2 zc = conjf2(r[l * M + ((M - k) % M)]);
             float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(256) k5_c2r_residual(BatchKernelArgs P)
     __syncthreads();
     const float2* rows = P.work + (((long long)c * P.Wz + z) * P.Py + y0) * P.hx;
     for (int e = threadIdx.x; e < G * M; e += blockDim.x) {
-        int l = e / M, k = e % M;
+        const int l = fdiv(e, P.ax.mn), k = e - l * M;
         float2 v = make_float2(0.f, 0.f);
         if (l < gn && GBK_OK_IDX((rows - P.work) + (long long)l * P.hx + M, P.lim_work, 20)) {
             const float2* r = rows + (long long)l * P.hx;
@@ -287,8 +288,9 @@ __global__ void __launch_bounds__(256) k5_c2r_residual(BatchKernelArgs P)
     float2* res = fft_smem(b0, b1, P.ax, G, 1, M, true, s_tw, true);
     const float* real = reinterpret_cast<const float*>(res);   // (G, Px) reals
     float acc = 0.f;
+    const unsigned long long mnx = fdiv_magic(P.Nx);
     for (int e = threadIdx.x; e < gn * P.Nx; e += blockDim.x) {
-        int l = e / P.Nx, x = e % P.Nx;
+        const int l = fdiv(e, mnx), x = e - l * P.Nx;
         if (!GBK_OK_IDX(l * P.Px + x + P.ex, 2 * G * M, 21)) continue;
         float m = real[l * P.Px + x + P.ex];
         long long vi = ((long long)z * P.Ny + (y0 + l)) * P.Nx + x;
@@ -565,6 +567,7 @@ static int auto_fft_size(int w, bool even)
 static int make_axis_dev(AxisDev& a, float2*& tw, int n)
 {
     a.n = n;
+    if (n < 1 || n > (1 << 16)) return GBKB200_ERR_UNSUPPORTED;   // fdiv_magic's range
     int m = n, nr = 0;
     int r[FFT_MAX_PASSES];
     while (m % 8 == 0 && m > 8) { r[nr++] = 8; m /= 8; }
@@ -575,6 +578,7 @@ static int make_axis_dev(AxisDev& a, float2*& tw, int n)
     if (m != 1) return GBKB200_ERR_UNSUPPORTED;
     a.nr = nr;
     for (int i = 0; i < nr; ++i) a.r[i] = r[i];
+    axis_fill_magics(a);
     std::vector<float2> h(n);
     for (int k = 0; k < n; ++k) {
         double ang = -2.0 * M_PI * (double)k / (double)n;

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(FFT_THREADS) x_r2c_kernel(const float* in, flo
     staged_copy<8>(
         L * M,
         [&](int e) {
-            const int l = e / M, m = e % M;
+            const int l = fdiv(e, ax.mn), m = e - l * M;
             const long long row = row0 + l;
             float2 v = make_float2(0.f, 0.f);
             if (row < rows) {
@@ -63,8 +63,9 @@ __global__ void __launch_bounds__(FFT_THREADS) x_r2c_kernel(const float* in, flo
         [&](int e, float2 v) { b0[e] = v; });
     __syncthreads();
     float2* z = fft_smem(b0, b1, ax, L, 1, M, true, s_tw, false);
+    const unsigned long long mhx = fdiv_magic(hx);
     for (int e = threadIdx.x; e < L * hx; e += blockDim.x) {
-        int l = e / hx, k = e % hx;
+        const int l = fdiv(e, mhx), k = e - l * hx;
         long long row = row0 + l;
         if (row >= rows) continue;
         float2 X;
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(FFT_THREADS) x_c2r_kernel(const float2* in, fl
         staged_copy<8>(
             L * M,
             [&](int e) {
-                const int l = e / M, k = e % M;
+                const int l = fdiv(e, ax.mn), k = e - l * M;
                 const long long row = row0 + l;
                 return row < rows ? in[row * hx + k] : make_float2(0.f, 0.f);
             },
@@ -114,14 +115,14 @@ __global__ void __launch_bounds__(FFT_THREADS) x_c2r_kernel(const float2* in, fl
         staged_copy<8>(
             L * M,
             [&](int e) {
-                const int l = e / M, k = e % M;
+                const int l = fdiv(e, ax.mn), k = e - l * M;
                 const long long row = row0 + l;
                 return row < rows ? in[row * hx + M - k] : make_float2(0.f, 0.f);
             },
             [&](int e, float2 v) { b1[e] = v; });
         __syncthreads();
         for (int e = threadIdx.x; e < L * M; e += blockDim.x) {
-            const int k = e % M;
+            const int k = e - fdiv(e, ax.mn) * M;
             const float2 a = b0[e], b = conjf2(b1[e]);
             const float2 s = cadd(a, b), d = csub(a, b);
             const float2 w = conjf2(s_post[k]);
@@ -133,7 +134,7 @@ __global__ void __launch_bounds__(FFT_THREADS) x_c2r_kernel(const float2* in, fl
         staged_copy<8>(
             L * M,
             [&](int e) {
-                const int l = e / M, k = e % M;
+                const int l = fdiv(e, ax.mn), k = e - l * M;
                 const long long row = row0 + l;
                 if (row >= rows) return make_float2(0.f, 0.f);
                 const float2* r = in + row * hx;
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(FFT_THREADS) x_c2r_kernel(const float2* in, fl
     __syncthreads();
     float2* z = fft_smem(b0, b1, ax, L, 1, M, true, s_tw, true);
     for (int e = threadIdx.x; e < L * M; e += blockDim.x) {
-        int l = e / M, m = e % M;
+        const int l = fdiv(e, ax.mn), m = e - l * M;
         long long row = row0 + l;
         if (row >= rows) continue;
         float2 v = z[l * M + m];
@@ -260,7 +261,9 @@ static bool factorize(int n, int* r, int& nr)
 static int make_axis(Axis& a, int n)
 {
     a.dev.n = n;
+    if (n < 1 || n > (1 << 16)) return GBKB200_ERR_UNSUPPORTED;   // fdiv_magic's range
     if (!factorize(n, a.dev.r, a.dev.nr)) return GBKB200_ERR_UNSUPPORTED;
+    axis_fill_magics(a.dev);
     std::vector<float2> h(n);
     for (int k = 0; k < n; ++k) {
         double ang = -2.0 * M_PI * (double)k / (double)n;

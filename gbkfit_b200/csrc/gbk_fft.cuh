@@ -10,12 +10,42 @@ constexpr int FFT_MAX_PASSES = 24;
 constexpr int FFT_MAX_PRIME = 61;
 constexpr int FFT_THREADS = 256;
 
+// Division by a run-time divisor as a multiply and a shift: for 0 <= x < 2^24
+// and 1 <= d <= 2^16, x / d = (x * m) >> 40 with m = ceil(2^40 / d) (exact: with
+// x = q d + r the product is q + r / d + x (m - 2^40 / d) / 2^40, and
+// r / d + x / 2^40 < 1 because x d < 2^40).
+__host__ __device__ inline unsigned long long fdiv_magic(int d)
+{
+    return ((1ull << 40) + (unsigned long long)d - 1) / (unsigned long long)d;
+}
+__device__ __forceinline__ int fdiv(int x, unsigned long long m)
+{
+    return (int)(((unsigned long long)(unsigned)x * m) >> 40);
+}
+
 struct AxisDev {
     int n;
     int nr;
     int r[FFT_MAX_PASSES];
     const float2* tw;   // tw[k] = exp(-2 pi i k / n), k in [0, n)
+    // division multipliers (fdiv_magic): of n, and per pass of n / r[p] (the
+    // butterflies of the pass) and of Ns (the product of the earlier radices)
+    unsigned long long mn;
+    unsigned long long mnb[FFT_MAX_PASSES];
+    unsigned long long mns[FFT_MAX_PASSES];
 };
+
+// fills the division multipliers of an axis whose n, nr and r[] are set
+inline void axis_fill_magics(AxisDev& a)
+{
+    a.mn = fdiv_magic(a.n);
+    int ns = 1;
+    for (int p = 0; p < a.nr; ++p) {
+        a.mnb[p] = fdiv_magic(a.n / a.r[p]);
+        a.mns[p] = fdiv_magic(ns);
+        ns *= a.r[p];
+    }
+}
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
@@ -90,16 +120,19 @@ __device__ __forceinline__ void dft_small(float2* v, bool inv, const float2* tw,
 // (k, l) of the lines sits at k * sk + l * sl.
 template<int R>
 __device__ __forceinline__ void pass_r(const float2* src, float2* dst, int n, int Ns, int L, int sk,
-                                       int sl, bool rows, const float2* tw, bool inv)
+                                       int sl, bool rows, const float2* tw, bool inv,
+                                       unsigned long long m_nb, unsigned long long m_ns,
+                                       unsigned long long m_L)
 {
     const int nb = n / R;
     const int twstep = n / (Ns * R);
     const int total = nb * L;
     for (int u = threadIdx.x; u < total; u += blockDim.x) {
         int j, l;
-        if (rows) { j = u % nb; l = u / nb; }
-        else { l = u % L; j = u / L; }
-        const int k = j % Ns;
+        if (rows) { l = fdiv(u, m_nb); j = u - l * nb; }
+        else { j = fdiv(u, m_L); l = u - j * L; }
+        const int jq = fdiv(j, m_ns);          // j / Ns
+        const int k = j - jq * Ns;
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -114,7 +147,7 @@ __device__ __forceinline__ void pass_r(const float2* src, float2* dst, int n, in
             v[r] = x;
         }
         dft_small<R>(v, inv, tw, n);
-        const int d0 = (j / Ns) * Ns * R + k;
+        const int d0 = jq * Ns * R + k;
 #pragma unroll
         for (int m = 0; m < R; ++m) {
             const int di = (d0 + m * Ns) * sk + l * sl;
@@ -125,19 +158,23 @@ __device__ __forceinline__ void pass_r(const float2* src, float2* dst, int n, in
 
 // generic prime radix (11..61): inputs re-read from shared memory
 static __device__ void pass_generic(const float2* src, float2* dst, int n, int R, int Ns, int L, int sk,
-                             int sl, bool rows, const float2* tw, bool inv)
+                             int sl, bool rows, const float2* tw, bool inv,
+                             unsigned long long m_nb, unsigned long long m_ns,
+                             unsigned long long m_L)
 {
     const int nb = n / R;
     const int twstep = n / (Ns * R);
     const int step = n / R;
     const int total = nb * L * R;
+    const unsigned long long m_R = fdiv_magic(R);
     for (int u = threadIdx.x; u < total; u += blockDim.x) {
-        int m = u % R;
-        int w = u / R;
+        const int w = fdiv(u, m_R);
+        const int m = u - w * R;
         int j, l;
-        if (rows) { j = w % nb; l = w / nb; }
-        else { l = w % L; j = w / L; }
-        const int k = j % Ns;
+        if (rows) { l = fdiv(w, m_nb); j = w - l * nb; }
+        else { j = fdiv(w, m_L); l = w - j * L; }
+        const int jq = fdiv(j, m_ns);          // j / Ns
+        const int k = j - jq * Ns;
         float2 acc = make_float2(0.f, 0.f);
         for (int r = 0; r < R; ++r) {
             float2 x = src[(j + r * nb) * sk + l * sl];
@@ -146,7 +183,7 @@ static __device__ void pass_generic(const float2* src, float2* dst, int n, int R
             if (inv) t = conjf2(t);
             acc = cadd(acc, cmul(x, t));
         }
-        const int d0 = (j / Ns) * Ns * R + k;
+        const int d0 = jq * Ns * R + k;
         dst[(d0 + m * Ns) * sk + l * sl] = acc;
     }
 }
@@ -158,16 +195,18 @@ static __device__ float2* fft_smem(float2* b0, float2* b1, const AxisDev& ax, in
     float2* src = b0;
     float2* dst = b1;
     int Ns = 1;
+    const unsigned long long m_L = rows ? 0ull : fdiv_magic(L);
     for (int p = 0; p < ax.nr; ++p) {
         const int R = ax.r[p];
+        const unsigned long long mb = ax.mnb[p], ms = ax.mns[p];
         switch (R) {
-        case 2: pass_r<2>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv); break;
-        case 3: pass_r<3>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv); break;
-        case 4: pass_r<4>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv); break;
-        case 5: pass_r<5>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv); break;
-        case 7: pass_r<7>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv); break;
-        case 8: pass_r<8>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv); break;
-        default: pass_generic(src, dst, ax.n, R, Ns, L, sk, sl, rows, tw, inv); break;
+        case 2: pass_r<2>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv, mb, ms, m_L); break;
+        case 3: pass_r<3>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv, mb, ms, m_L); break;
+        case 4: pass_r<4>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv, mb, ms, m_L); break;
+        case 5: pass_r<5>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv, mb, ms, m_L); break;
+        case 7: pass_r<7>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv, mb, ms, m_L); break;
+        case 8: pass_r<8>(src, dst, ax.n, Ns, L, sk, sl, rows, tw, inv, mb, ms, m_L); break;
+        default: pass_generic(src, dst, ax.n, R, Ns, L, sk, sl, rows, tw, inv, mb, ms, m_L); break;
         }
         __syncthreads();
         float2* t = src;

@@ -43,6 +43,22 @@ def test_fft_optimal_shape_matches_reference_rule():
         (1, 2, 4, 32, 32, 64, 96, 96, 160, 320)
 
 
+def test_fft_index_division_multipliers_are_exact():
+    """The FFT passes divide thread indices (< 2^24) by run-time lengths
+    (<= 2^16) as (x * ceil(2^40 / d)) >> 40: exact on the whole range, checked
+    at every divisor on the last multiple below 2^24 minus one, the largest
+    index and a random sample."""
+    d = np.arange(1, (1 << 16) + 1, dtype=np.uint64)
+    m = ((np.uint64(1) << np.uint64(40)) + d - np.uint64(1)) // d
+    top = np.uint64((1 << 24) - 1)
+    rng = np.random.default_rng(0)
+    cols = [(top // d) * d - np.uint64(1), np.full_like(d, top), (top // d) * d,
+            np.ones_like(d), np.zeros_like(d)]
+    cols += [rng.integers(0, 1 << 24, d.size).astype(np.uint64) for _ in range(64)]
+    for x in cols:
+        assert np.array_equal((x * m) >> np.uint64(40), x // d)
+
+
 def test_dcube_geometry_reference_pins():
     """tests/unit/test_dmodel.py:102-170 of the reference: scratch size, step
     and zero of a DCube without PSF/LSF."""
