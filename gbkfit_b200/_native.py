@@ -117,6 +117,7 @@ _SIGS = {
                                        c_void_p, c_void_p, c_int, c_float, c_void_p],
     'gbkb200_objective_residual_sum_f32': [c_void_p, c_void_p, c_int, c_int, c_void_p],
     'gbkb200_serve_scube_chi2_f32': [c_void_p, ctypes.POINTER(ServeArgs)],
+    'gbkb200_serve_model_f32': [c_void_p, ctypes.POINTER(ServeArgs)],
 }
 
 EXPORTED = sorted(_SIGS) + ['gbkb200_error_string', 'gbkb200_last_cuda_error']

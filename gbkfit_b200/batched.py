@@ -320,6 +320,41 @@ class BatchedSMDisk:
             ev.record(self.stream)
         return ev, out
 
+    # ---- given model cubes (direct mode) ---------------------------------------
+    def window(self):
+        """The model window of the direct mode: (offset, size), the voxel
+        offset (x, y, z) of its first voxel in the padded grid (whose zero is
+        geom.zero_hi) and its size (Wx, Wy, Wz)."""
+        off, size = (c_int * 3)(), (c_int * 3)()
+        check(_lib.gbkb200_batch_window(self.handle, off, size), 'batch_window')
+        return tuple(off), tuple(size)
+
+    def evaluate_cubes_device(self, cubes, nsets, chi2=None, model=None):
+        """chi^2 of nsets model cubes (device (>= nsets, Wz, Wy, Wx) float32,
+        any gmodel's output on the window) through the direct mode's
+        convolution, residual and sum (enqueued on the evaluator's stream,
+        not synchronised)."""
+        chi2 = self.chi2 if chi2 is None else chi2
+        check(_lib.gbkb200_batch_evaluate_cubes(
+            self.handle, c_int(int(nsets)), c_void_p(cubes.data_ptr()), c_void_p(chi2.data_ptr()),
+            c_void_p(model.data_ptr()) if model is not None else None), 'batch_evaluate_cubes')
+        return chi2[:nsets]
+
+    def submit_cubes(self, cubes, n):
+        """As submit_rows, for n model cubes already enqueued into `cubes` on
+        the evaluator's stream: the convolution, residual and sum, and chi^2
+        copied back to pinned memory.  Returns (event, chi2 host view)."""
+        if not 0 < n <= self.max_sets:
+            raise ValueError(f"a group of {n} sets (max_sets {self.max_sets})")
+        st = self._e2e_buffers(self.max_sets, 1)
+        with torch.cuda.stream(self.stream):
+            self.evaluate_cubes_device(cubes, n)
+            out = st['chi2'][:n]
+            out.copy_(self.chi2[:n], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+        return ev, out
+
     def capture(self, bufs, nsets):
         """Capture one evaluate_device call for nsets sets in a CUDA graph."""
         s = torch.cuda.Stream(self.dev)

@@ -363,6 +363,7 @@ struct gbkb200_batch {
     double* partials = nullptr;
     int nper = 0;
     int direct = 0;
+    int trim[3] = {0, 0, 0};          // direct mode: taps trimmed from each end (x, y, z)
     size_t smemB = 0;
     float* mplanes = nullptr;
     int* xr = nullptr;
@@ -412,6 +413,14 @@ static KaFn ka_fn(int Kz)
     return t[Kz / 2];
 }
 
+static KcFn kc_fn(int Kz)
+{
+    static KcFn t[KA_KMAX / 2 + 1] = {};
+    static std::once_flag once;
+    std::call_once(once, [] { kc_register(t); });
+    return t[Kz / 2];
+}
+
 static KbFn kb_fn(int K, int variant)
 {
     static KbFn t[KB_VARIANTS][(KB_KMAX - KB_KMIN) / 2 + 1] = {};
@@ -446,6 +455,7 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     };
     const int tx = trim(d->psf_v, d->kernel_size[0]), ty = trim(d->psf_u, d->kernel_size[1]);
     const int tz = trim(d->lsf, d->kernel_size[2]);
+    bt->trim[0] = tx; bt->trim[1] = ty; bt->trim[2] = tz;
     P.Kx = d->kernel_size[0] - 2 * tx;
     P.Ky = d->kernel_size[1] - 2 * ty;
     P.Kz = d->kernel_size[2] - 2 * tz;
@@ -882,6 +892,55 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
         stage_mark(bt, 4, true);
         k5_c2r_residual<<<dim3((P.Ny + P.rows_k5 - 1) / P.rows_k5, P.Nz, cn), 256, bt->smem5,
                           st>>>(P);
+        stage_mark(bt, 4, false);
+    }
+    stage_mark(bt, 5, true);
+    if (nsets > 0) k6_sum<<<nsets, 256, 0, st>>>(P.partials, bt->nper, 0, chi2);
+    stage_mark(bt, 5, false);
+    GBK_CUDA_TRY(cudaGetLastError());
+    return gbk_finish(bt->ctx);
+}
+
+extern "C" int gbkb200_batch_window(const gbkb200_batch* bt, int offset[3], int size[3])
+{
+    if (!bt || !offset || !size) return GBKB200_ERR_INVALID_ARG;
+    if (!bt->direct) return GBKB200_ERR_UNSUPPORTED;
+    const BatchKernelArgs& P = bt->P;
+    // the window starts t trimmed taps into the untrimmed one, whose first
+    // voxel is the high-resolution grid's first voxel
+    offset[0] = bt->trim[0]; offset[1] = bt->trim[1]; offset[2] = bt->trim[2];
+    size[0] = P.Wx; size[1] = P.Wy; size[2] = P.Wz;
+    return GBKB200_OK;
+}
+
+extern "C" int gbkb200_batch_evaluate_cubes(gbkb200_batch* bt, int nsets, const float* cubes,
+                                            float* chi2, float* model)
+{
+    if (!bt || nsets < 0 || nsets > bt->max_sets || !cubes || !chi2)
+        return GBKB200_ERR_INVALID_ARG;
+    if (!bt->direct) return GBKB200_ERR_UNSUPPORTED;
+    BatchKernelArgs P = bt->P;
+    cudaStream_t st = bt->ctx->stream;
+    P.model = model;
+    P.lim_model = model ? (long long)nsets * P.Nz * P.Ny * P.Nx : 0;
+    P.counters = bt->timing ? bt->counters : nullptr;
+    const KcFn kc = kc_fn(P.Kz);
+    for (int s0 = 0; s0 < nsets; s0 += bt->chunk) {
+        const int cn = std::min(bt->chunk, nsets - s0);
+        P.set0 = s0;
+        stage_mark(bt, 0, true);
+        kc<<<dim3((P.Wy * P.nch + KA_THREADS / 32 - 1) / (KA_THREADS / 32), cn), KA_THREADS, 0,
+             st>>>(P, cubes);
+        stage_mark(bt, 0, false);
+        stage_mark(bt, 1, true);
+        {
+            const int R = P.Wy * P.nch;
+            k_xr_transpose<<<dim3((R + 31) / 32, (P.Nz + 31) / 32, cn), 256, 0, st>>>(
+                P.xr, P.xrt, R, P.Nz);
+        }
+        stage_mark(bt, 1, false);
+        stage_mark(bt, 4, true);
+        bt->kb<<<dim3(cn, P.Nz * P.nbands), KB_THREADS, bt->smemB, st>>>(P);
         stage_mark(bt, 4, false);
     }
     stage_mark(bt, 5, true);

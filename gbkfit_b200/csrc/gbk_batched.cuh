@@ -732,6 +732,69 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     }
 }
 
+// The LSF FIR of given model cubes (any gmodel's output on the evaluation
+// window, e.g. mcdisk's clouds) into the PSF kernel's input: the same
+// planes and range table as ka_lines_lsf, so that the PSF FIR, residual and
+// sum run unchanged.  cubes: (sets, Wz, Wy, Wx), set b = P.set0 + slot;
+// one warp per (window row y, 32-column chunk), a lane per column, the
+// channel axis walked with a KZ-deep register window (each cube value is
+// read once).  A plane row chunk's range covers its nonzero outputs (all
+// outputs are written), so the PSF kernel skips exactly the zero ones.
+template<int KZ>
+__global__ void __launch_bounds__(KA_THREADS) kc_cube_lsf(BatchKernelArgs P,
+                                                          const float* __restrict__ cubes)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int item = blockIdx.x * (KA_THREADS / 32) + warp;
+    if (item >= P.Wy * P.nch) return;                    // whole warp
+    const int y = item / P.nch, chunk = item % P.nch;
+    const int c = blockIdx.y, b = P.set0 + c;
+    const int x = chunk * 32 + lane;
+    const bool in = x < P.Wx;
+    const long long plane = (long long)P.Wy * P.Wx;
+    const float* col = cubes + (long long)b * P.Wz * plane + (long long)y * P.Wx + (in ? x : 0);
+    auto ld = [&](int z) { return in ? __ldg(col + z * plane) : 0.f; };
+    float lz[KZ];
+#pragma unroll
+    for (int t = 0; t < KZ; ++t) lz[t] = P.lsfr[t];
+    float w[KZ];
+#pragma unroll
+    for (int t = 0; t < KZ - 1; ++t) w[t] = ld(t);
+    int* xr = P.xr + (((long long)c * P.Wy + y) * P.nch + chunk) * P.Nz;
+    const long long zstride = (long long)P.Wy * P.pitch;
+    float* dp = P.mplanes + ((long long)c * P.Nz * P.Wy + y) * P.pitch + x;
+    unsigned mm = 0u;
+    for (int zb = 0; zb < P.Nz; zb += KZ) {
+#pragma unroll
+        for (int k = 0; k < KZ; ++k) {
+            const int zo = zb + k;
+            if (zo >= P.Nz) break;
+            w[(k + KZ - 1) % KZ] = ld(zo + KZ - 1);
+            float acc0 = 0.f, acc1 = 0.f;
+#pragma unroll
+            for (int t = 0; t < KZ; t += 2) acc0 += lz[t] * w[(k + t) % KZ];
+#pragma unroll
+            for (int t = 1; t < KZ; t += 2) acc1 += lz[t] * w[(k + t) % KZ];
+            const float v = acc0 + acc1;
+            *dp = v;        // plane zo
+            dp += zstride;
+            // lane (zo % 32) keeps the ballot of plane zo; written every 32
+            // planes and at the last one
+            const unsigned m = __ballot_sync(0xffffffffu, v != 0.f);
+            if ((zo & 31) == lane) mm = m;
+            if ((zo & 31) == 31 || zo == P.Nz - 1) {
+                const int own = (zo & ~31) + lane;
+                if (own <= zo)
+                    xr[own] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
+                                    ((chunk * 32 + 31 - __clz(mm)) << 16))
+                                 : -1;
+            }
+        }
+    }
+    if (P.counters && lane == 0)
+        atomicAdd(&P.counters[GBK_CTR_KA_FMA], (unsigned long long)P.Nz * 32 * KZ);
+}
+
 typedef void (*KaFn)(BatchKernelArgs, int*);
 typedef void (*KbFn)(BatchKernelArgs);
 constexpr int KA_KMAX = 33;                 // longest LSF of the direct path
@@ -740,6 +803,9 @@ static_assert(KA_KMAX <= 33 && KB_KMAX <= 33, "coefficient arrays of BatchKernel
 // fill t[Kz / 2] (model kernel) and t[(K - KB_KMIN) / 2] (PSF kernel)
 void ka_register_short(KaFn* t);
 void ka_register_long(KaFn* t);
+// t[Kz / 2]: the LSF FIR of given model cubes
+typedef void (*KcFn)(BatchKernelArgs, const float*);
+void kc_register(KcFn* t);
 // t[v][(K - KB_KMIN) / 2] for the PSF kernel variant v = 3 * (MINB == 5) + EPI
 constexpr int KB_VARIANTS = 6;
 void kb_register4(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1]);   // MINB 4, EPI 0-2

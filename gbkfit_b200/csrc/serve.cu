@@ -69,20 +69,10 @@ __global__ void __launch_bounds__(TAIL_THREADS)
 
 using namespace gbk;
 
-extern "C" int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serve_args* a)
+// The packed parameters' copy, the zeroing of the cube (ncube floats at
+// a->scube) and the model evaluation of one request.
+static int serve_model(gbkb200_ctx* ctx, const gbkb200_serve_args* a, long long ncube)
 {
-    if (!ctx || !a || !a->blob_dev || !a->scube || !a->work || !a->spectrum || !a->obs ||
-        !a->chi2_dev || !a->chi2_host || !a->status_host)
-        return GBKB200_ERR_INVALID_ARG;
-    if (a->kind != 0 && a->kind != 1) return GBKB200_ERR_INVALID_ARG;
-    for (int k = 0; k < 3; ++k)
-        if (a->size_hi[k] < 1 || a->size[k] < 1 || a->edge[k] < 0 ||
-            a->edge[k] + a->size[k] > a->size_hi[k])
-            return GBKB200_ERR_INVALID_ARG;
-    // sizes are checked before anything is enqueued on the stream
-    const long long vhi = (long long)a->size_hi[0] * a->size_hi[1] * a->size_hi[2];
-    if ((long long)a->size[0] * a->size[1] * a->size[2] >= (1ll << 31) || vhi >= (1ll << 31))
-        return GBKB200_ERR_TOO_LARGE;
     char* base = static_cast<char*>(a->blob_dev);
     auto at = [&](long long off) -> char* { return off < 0 ? nullptr : base + off; };
     const cudaStream_t st = ctx->stream;
@@ -91,7 +81,7 @@ extern "C" int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serv
         GBK_CUDA_TRY(cudaMemcpyAsync(a->blob_dev, a->blob_host, (size_t)a->blob_bytes,
                                      cudaMemcpyHostToDevice, st));
     }
-    GBK_CUDA_TRY(cudaMemsetAsync(a->scube, 0, (size_t)vhi * sizeof(float), st));
+    GBK_CUDA_TRY(cudaMemsetAsync(a->scube, 0, (size_t)ncube * sizeof(float), st));
 #define GBK_T(k)                                                                                 \
     reinterpret_cast<const int*>(at(a->off_uids[k])),                                            \
         reinterpret_cast<const float*>(at(a->off_cvalues[k])),                                   \
@@ -120,6 +110,39 @@ extern "C" int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serv
             reinterpret_cast<const unsigned char*>(at(a->off_hasordint)), GBK_SERVE_DISK);
 #undef GBK_SERVE_DISK
 #undef GBK_T
+    return rc;
+}
+
+extern "C" int gbkb200_serve_model_f32(gbkb200_ctx* ctx, const gbkb200_serve_args* a)
+{
+    if (!ctx || !a || !a->blob_dev || !a->scube) return GBKB200_ERR_INVALID_ARG;
+    if (a->kind != 0 && a->kind != 1) return GBKB200_ERR_INVALID_ARG;
+    if (a->spat_size[0] < 1 || a->spat_size[1] < 1 || a->spat_size[2] < 1 || a->spec_size < 1)
+        return GBKB200_ERR_INVALID_ARG;
+    const long long n = (long long)a->spat_size[0] * a->spat_size[1] * a->spec_size;
+    if (n >= (1ll << 31)) return GBKB200_ERR_TOO_LARGE;
+    const int rc = serve_model(ctx, a, n);
+    if (rc) return rc;
+    GBK_CUDA_TRY(cudaGetLastError());
+    return GBKB200_OK;
+}
+
+extern "C" int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serve_args* a)
+{
+    if (!ctx || !a || !a->blob_dev || !a->scube || !a->work || !a->spectrum || !a->obs ||
+        !a->chi2_dev || !a->chi2_host || !a->status_host)
+        return GBKB200_ERR_INVALID_ARG;
+    if (a->kind != 0 && a->kind != 1) return GBKB200_ERR_INVALID_ARG;
+    for (int k = 0; k < 3; ++k)
+        if (a->size_hi[k] < 1 || a->size[k] < 1 || a->edge[k] < 0 ||
+            a->edge[k] + a->size[k] > a->size_hi[k])
+            return GBKB200_ERR_INVALID_ARG;
+    // sizes are checked before anything is enqueued on the stream
+    const long long vhi = (long long)a->size_hi[0] * a->size_hi[1] * a->size_hi[2];
+    if ((long long)a->size[0] * a->size[1] * a->size[2] >= (1ll << 31) || vhi >= (1ll << 31))
+        return GBKB200_ERR_TOO_LARGE;
+    const cudaStream_t st = ctx->stream;
+    int rc = serve_model(ctx, a, vhi);
     if (rc) return rc;
     if ((rc = gbkb200_fft_convolve_f32(ctx, a->size_hi, a->scube, a->work, a->spectrum))) return rc;
     if (!ctx->serve_scratch) {

@@ -31,7 +31,13 @@ optionally, its model cube).
   to the evaluator's batch, whenever the evaluator is idle: one H2D copy of
   the rows, one batched evaluation, one D2H copy of chi^2 on the dataset's
   own stream.  Each request's chi^2 does not depend on the others of its
-  launch (per-set partial sums in a fixed order).
+  launch (per-set partial sums in a fixed order).  Its queued mcdisk
+  requests are coalesced the same way, up to mc_sets per launch: each
+  request's clouds are splatted into its own cube on the evaluator's model
+  window (gbkb200_serve_model_f32), and one launch convolves all of them
+  with the separable PSF and LSF and takes their residual sums
+  (gbkb200_batch_evaluate_cubes), instead of an FFT convolution of the
+  padded grid per request.
 * Latency: completion minus arrival (the submit time, or the arrival time a
   caller passes); the packing of the parameters happens in submit, after
   the arrival.  ``ModelServer.stats()`` gives p50/p99 and throughput.
@@ -74,7 +80,10 @@ class Dataset:
     its own stream) and queued smdisk requests of that disk are coalesced
     into its launches."""
 
-    def __init__(self, key, geom, data, error, ctx, dev, stream, smdisk=None, batch_sets=16):
+    MC_STAGE = 1 << 16      # bytes of a coalesced mcdisk request's packed parameters at most
+
+    def __init__(self, key, geom, data, error, ctx, dev, stream, smdisk=None, batch_sets=16,
+                 mc_sets=4, mc_seed=42):
         self.key, self.geom = key, geom
         f32 = lambda a: None if a is None else torch.as_tensor(
             np.ascontiguousarray(a, np.float32)).to(dev)
@@ -92,6 +101,8 @@ class Dataset:
         self.released = False   # unregistered
         self.smdisk, self.batched = smdisk, None
         self.group = None       # (event, chi2 host view, requests) of the launch in flight
+        self.window = None      # (size, zero) of the model window of coalesced mcdisk requests
+        self.mc_sets = 0
         if smdisk is not None and not smdisk.traits['rht'] and batch_sets > 0:
             from .batched import BatchedSMDisk, kernel_boxes, separable_factors
             if separable_factors(kernel_boxes(geom)[0])[0] == 1:
@@ -100,6 +111,18 @@ class Dataset:
                     chunk=int(batch_sets), conv='direct', device=dev.index,
                     stream=torch.cuda.Stream(dev))
                 self.footprint += self.batched.work_bytes + 4 * self.batched.max_sets
+        if self.batched is not None and mc_sets > 0:
+            (ox, oy, oz), (wx, wy, wz) = self.batched.window()
+            st, z = geom.step, geom.zero_hi
+            self.window = ((wx, wy, wz), (z[0] + ox * st[0], z[1] + oy * st[1], z[2] + oz * st[2]))
+            self.mc_sets = min(int(mc_sets), self.batched.max_sets)
+            self.mc_cubes = torch.empty((self.mc_sets, wz, wy, wx), dtype=torch.float32,
+                                        device=dev)
+            self.mc_h = torch.empty((self.mc_sets, self.MC_STAGE), dtype=torch.uint8,
+                                    pin_memory=True)
+            self.mc_d = torch.empty((self.mc_sets, self.MC_STAGE), dtype=torch.uint8, device=dev)
+            self.batched.ctx.set_mcdisk(mc_seed, 0)
+            self.footprint += self.mc_cubes.numel() * 4 + self.mc_d.numel()
 
     def request_layout(self):
         """Byte offsets of one in-flight request's device buffers (padded
@@ -137,6 +160,7 @@ class Request:
         self.future = Future()
         self.blob = self.layout = self.args = self.ds = None
         self.rows = None        # packed parameter row of a coalesced smdisk request
+        self.cube = False       # a coalesced mcdisk request (model on the dataset's window)
 
     def prepare(self):
         """Pack the parameters (Disk.pack, and the cloud budget of mcdisk)
@@ -173,9 +197,11 @@ class Request:
             self.nclouds = int(arrays[-2][1][-1]) if c[1] else 0
         self.blob, self.layout = blob, layout
 
-    def serve_args(self, ds):
+    def serve_args(self, ds, window=None):
         """The native argument block of this request against dataset ds
-        (everything but the slot's buffers, which the scheduler sets)."""
+        (everything but the slot's buffers, which the scheduler sets); with
+        window = (size, zero) of a batched evaluator's model window, the model
+        is evaluated on that window instead of the padded grid."""
         lay, g = self.layout, ds.geom
         off = lambda name: -1 if lay[name][0] is None else lay[name][0]
         a = _native.ServeArgs()
@@ -198,6 +224,10 @@ class Request:
             a.off_pcounts[i] = off(k + '.pcounts')
         ss, st, sz = g.spat(self.thick)
         spec = g.spec()
+        if window is not None:
+            (wx, wy, wz), (zx, zy, zz) = window
+            ss, sz = (wx, wy, ss[2]), (zx, zy, sz[2])
+            spec = (wz, spec[1], zz)
         a.spat_size[:] = [int(v) for v in ss]
         a.spat_step[:] = [float(v) for v in st]
         a.spat_zero[:] = [float(v) for v in sz]
@@ -236,6 +266,7 @@ class ModelServer:
     def __init__(self, device=0, hbm_budget=8 << 30, slots=8, mc_seed=42):
         self.dev = torch.device('cuda', device)
         self.budget = int(hbm_budget)
+        self.mc_seed = mc_seed
         self._setup_stream = torch.cuda.Stream(self.dev)
         self._setup_ctx = _native.Context(device=device, stream=self._setup_stream, sync=False)
         self.datasets = {}
@@ -255,13 +286,15 @@ class ModelServer:
         self._thread.start()
 
     # ---- datasets --------------------------------------------------------------
-    def register(self, key, geom, data, error=None, smdisk=None, batch_sets=16):
+    def register(self, key, geom, data, error=None, smdisk=None, batch_sets=16, mc_sets=4):
         """Make a dataset resident (its spectrum is computed now).  smdisk:
         the thin disk of its smdisk requests, whose requests are then
-        coalesced into batched launches (see Dataset)."""
+        coalesced into batched launches of up to batch_sets sets, and its
+        mcdisk requests into launches of up to mc_sets (see Dataset)."""
         with torch.cuda.device(self.dev):
             ds = Dataset(key, geom, data, error, self._setup_ctx, self.dev, self._setup_stream,
-                         smdisk=smdisk, batch_sets=batch_sets)
+                         smdisk=smdisk, batch_sets=batch_sets, mc_sets=mc_sets,
+                         mc_seed=self.mc_seed)
         with self._cv:
             if key in self.datasets:
                 raise KeyError(f"dataset {key!r} is already registered")
@@ -310,6 +343,13 @@ class ModelServer:
         else:
             if request.blob is None:
                 request.prepare()
+            # mcdisk requests of a dataset with a batched evaluator are
+            # coalesced: the model on the evaluator's window
+            request.cube = bool(ds.mc_sets and request.kind == 'mcdisk' and
+                                not request.want_model and request.blob.size <= ds.MC_STAGE)
+        if request.cube:
+            request.args = request.serve_args(ds, window=ds.window)
+        elif request.rows is None:
             if request.blob.size > _Slot.STAGE:
                 raise ValueError("the request's parameter arrays exceed the staging buffer")
             # the request holds its dataset: the native arguments point into the
@@ -422,14 +462,18 @@ class ModelServer:
                     continue
                 req = q[i]
                 ds = req.ds
-                if req.rows is not None:
+                if req.rows is not None or req.cube:
                     if ds.group is not None or ds in (g[0] for g in launches if g[1] == 'group'):
                         continue
+                    # a group of the same kind: parameter rows or mcdisk cubes
+                    cube = req.cube
+                    cap = ds.mc_sets if cube else ds.batched.max_sets
                     group = [i]
                     for j in range(i + 1, len(q)):
-                        if len(group) >= ds.batched.max_sets:
+                        if len(group) >= cap:
                             break
-                        if j not in taken and q[j].rows is not None and q[j].ds is ds:
+                        if j not in taken and q[j].ds is ds and q[j].cube == cube and (
+                                cube or q[j].rows is not None):
                             group.append(j)
                     taken.update(group)
                     launches.append((ds, 'group', [q[j] for j in group]))
@@ -471,9 +515,30 @@ class ModelServer:
         now = time.perf_counter()
         for r in reqs:
             r.admit = now
-        ev, out = ds.batched.submit_rows([r.rows for r in reqs])
+        if reqs[0].cube:
+            ev, out = self._launch_cubes(ds, reqs)
+        else:
+            ev, out = ds.batched.submit_rows([r.rows for r in reqs])
         ds.group = (ev, out, reqs)
         self.max_group = max(self.max_group, len(reqs))
+
+    def _launch_cubes(self, ds, reqs):
+        """The models of a group of mcdisk requests, each into its own cube of
+        the window, then one convolution + residual + sum launch, all on the
+        evaluator's stream.  The staging and cube buffers are the dataset's:
+        its previous group has completed (one group in flight per dataset)."""
+        bt = ds.batched
+        cube_bytes = ds.mc_cubes[0].numel() * 4
+        h, d = ds.mc_h.data_ptr(), ds.mc_d.data_ptr()
+        hn = ds.mc_h.numpy()
+        for i, r in enumerate(reqs):
+            nb = r.blob.size
+            hn[i, :nb] = r.blob
+            a = r.args
+            a.blob_host, a.blob_dev = h + i * ds.MC_STAGE, d + i * ds.MC_STAGE
+            a.scube = ds.mc_cubes.data_ptr() + i * cube_bytes
+            check(_lib.gbkb200_serve_model_f32(bt.ctx.handle, a), 'serve_model')
+        return bt.submit_cubes(ds.mc_cubes, len(reqs))
 
     def _complete_group(self, ds):
         ev, out, reqs = ds.group
@@ -483,7 +548,7 @@ class ModelServer:
             ds.group = None
             for r in reqs:
                 r.done = now
-                r.ds = None
+                r.ds = r.args = None
                 ds.holders -= 1
                 self._done.append(r)
             if ds.released and ds.holders == 0:

@@ -249,6 +249,12 @@ typedef struct {
 } gbkb200_serve_args;
 
 int gbkb200_serve_scube_chi2_f32(gbkb200_ctx* ctx, const gbkb200_serve_args* args);
+/* The first half of the chain only: the parameters' copy, the zeroing of
+ * the spat_size[0] x spat_size[1] x spec_size cube at scube and its model
+ * evaluation (kind 0 smdisk, 1 mcdisk) on the geometry of the arguments;
+ * the fields after spec_zero other than scube are not read.  For a model
+ * that a batched evaluator convolves (gbkb200_batch_evaluate_cubes). */
+int gbkb200_serve_model_f32(gbkb200_ctx* ctx, const gbkb200_serve_args* args);
 
 /* ---- differentiable chi^2 of a thin smooth disk (no reference counterpart:
  *      the reference computes no gradients).  A hand-written adjoint of
@@ -359,6 +365,17 @@ int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb2
 int gbkb200_batch_evaluate(gbkb200_batch* b, int nsets, const float* vsys, const float* xpos,
                            const float* ypos, const float* posa, const float* incl,
                            const float* const pvalues[9], float* chi2, float* model);
+/* Direct mode: the evaluation window of the model, as the voxel offset of
+ * its first voxel in the padded (high-resolution) grid whose zero the
+ * descriptor gives, and its size {Wx, Wy, Wz} = data size + FIR lengths - 1
+ * (GBKB200_ERR_UNSUPPORTED in FFT mode). */
+int gbkb200_batch_window(const gbkb200_batch* b, int offset[3], int size[3]);
+/* Direct mode: chi2[s] of given model cubes instead of the evaluator's disk
+ * (any gmodel's output sampled on the window: cubes is device (nsets, Wz,
+ * Wy, Wx)), through the same LSF FIR, PSF FIR, residual and sum; model as
+ * in gbkb200_batch_evaluate (GBKB200_ERR_UNSUPPORTED in FFT mode). */
+int gbkb200_batch_evaluate_cubes(gbkb200_batch* b, int nsets, const float* cubes, float* chi2,
+                                 float* model);
 /* the chosen FFT grid, chunk, the device bytes the evaluator holds (its
  * work space, tables and partials) and the convolution mode (1 = FFT,
  * 2 = direct) */

@@ -227,3 +227,52 @@ def test_batched_direct_box_shapes(gpu, oracle_built, size, psf_fwhm, lsf_fwhm):
         assert not np.any(model[i] == 7.0), i
         c_ref = chi2(ref, data, err)
         assert abs(got[i] - c_ref) / c_ref < 1e-4, (i, got[i], c_ref)
+
+
+def test_batched_cubes_match_disk_path(gpu):
+    """gbkb200_batch_evaluate_cubes: model cubes sampled on the evaluator's
+    window (here the drop-in smdisk on that window) give the chi^2 and cropped
+    models of the evaluator's own disk path within fp32 rounding (the two
+    evaluate the line profile with different exponentials)."""
+    import torch
+    from gbkfit_b200 import workloads
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    from gbkfit_b200.driver import DriverB200
+    from tests.helpers import gpu_smdisk, upload
+    n = 5
+    w = _small_batch_workload(n)
+    data, err, _ = synthetic_data(w)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=n, chunk=4, conv='direct')
+    (ox, oy, oz), (wx, wy, wz) = ev.window()
+    g = w.geom
+    assert wx > g.size[0] and wy > g.size[1] and wz > g.size[2]
+    assert min(ox, oy, oz) >= 0 and all(g.size_hi[i] >= (ox, oy, oz)[i] + (wx, wy, wz)[i]
+                                        for i in range(3))
+    geo = dict(loose=False, tilted=False, spat_size=(wx, wy, 1),
+               spat_step=(g.step[0], g.step[1], 0.0),
+               spat_zero=(g.zero_hi[0] + ox * g.step[0], g.zero_hi[1] + oy * g.step[1], 0.0),
+               spec_size=wz, spec_step=g.step[2], spec_zero=g.zero_hi[2] + oz * g.step[2])
+    gm = DriverB200(0).backends().gmodel(np.float32)
+    cubes = torch.zeros((n, wz, wy, wx), device='cuda')
+    for i in range(n):
+        gpu_smdisk(gm, upload(w.disk.pack(workloads.set_params(w, i)), 'cuda'), geo,
+                   dict(scube=cubes[i]))
+    torch.cuda.synchronize()
+    nx, ny, nz = g.size
+    m_cube = torch.zeros((n, nz, ny, nx), device='cuda')
+    m_disk = torch.zeros((n, nz, ny, nx), device='cuda')
+    got = ev.evaluate_cubes_device(cubes, n, model=m_cube).cpu().numpy().copy()
+    bufs = ev.alloc_inputs(n)
+    ev.upload(ev.pack(w.params, n), bufs, n)
+    ref = ev.evaluate_device(bufs, n, model=m_disk).cpu().numpy().copy()
+    assert np.all(ref > 0)
+    assert np.max(np.abs(got - ref) / ref) <= 1e-5, (got, ref)
+    for i in range(n):
+        assert rel_err(m_cube[i].cpu().numpy(), m_disk[i].cpu().numpy()) <= 1e-5, i
+    # an all-zero cube: the model is zero and chi^2 is the data's own sum
+    cubes.zero_()
+    z = ev.evaluate_cubes_device(cubes, 1, model=m_cube).cpu().numpy()[0]
+    d = np.asarray(data, np.float64) / np.asarray(err, np.float64)
+    assert abs(z - np.sum(d * d)) <= 1e-5 * np.sum(d * d)
+    assert float(m_cube[0].abs().max()) == 0.0
+    ev.close()

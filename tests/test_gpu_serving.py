@@ -191,3 +191,29 @@ def test_coalesced_unregister_releases_budget(gpu):
         assert srv._resident == 0 and srv._group_ds == []
     for a, b in zip(ref, got):
         assert abs(a - b) <= 1e-5 * abs(a)
+
+
+def test_coalesced_mcdisk_matches_fft_path(gpu):
+    """mcdisk requests of datasets with a batched evaluator: their clouds are
+    splatted onto the evaluator's model window and the group is convolved by
+    the direct separable kernels; chi^2 agrees with the same requests on the
+    per-request FFT path of the padded grid (same clouds: the cloud stream is
+    keyed by seed and cloud index, not by the grid)."""
+    from gbkfit_b200.serving import ModelServer
+    stream = _small_stream(n=40, seed=29)
+    with ModelServer(slots=4) as srv:
+        _register_coalesced(srv, stream)
+        assert all(ds.mc_sets > 0 for ds in srv.datasets.values())
+        reqs = [r for r in _requests(stream) if r.kind == 'mcdisk']
+        assert len(reqs) >= 6
+        futs = [srv.submit(r) for r in reqs]
+        assert all(r.cube for r in reqs)
+        got = [f.result(timeout=300)['chi2'] for f in futs]
+        assert srv.stats()['max_group'] > 1
+    with ModelServer(slots=4) as srv:
+        _register(srv, stream)
+        reqs = [r for r in _requests(stream) if r.kind == 'mcdisk']
+        fft = [f.result(timeout=300)['chi2'] for f in [srv.submit(r) for r in reqs]]
+        assert not any(r.cube for r in reqs)
+    for c, f in zip(got, fft):
+        assert abs(c - f) <= 1e-4 * abs(f), (c, f)
