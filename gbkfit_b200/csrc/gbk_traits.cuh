@@ -289,8 +289,47 @@ enum TraitKind { K_RP, K_RH, K_VP, K_VH, K_DP, K_DH, K_ZP, K_SP, K_WP };
 
 // traits.hpp:1887-1919: evaluate the n traits of a set, advancing the
 // constants/parameters pointers by the per-trait counts.
+// The per-set trait values live in fixed-size arrays that are only indexed by
+// constants (the loops over the set's n traits are unrolled to the maximum
+// with a guard, stores go through selects), so they stay in registers
+// instead of the stack.
+typedef float TraitVals[GBK_TRAIT_NUM_MAX];
+
+__device__ __forceinline__ void tv_set(TraitVals& o, int i, float v)
+{
+#pragma unroll
+    for (int j = 0; j < GBK_TRAIT_NUM_MAX; ++j) o[j] = i == j ? v : o[j];
+}
+// sum of the first n values, in index order
+__device__ __forceinline__ float tv_sum(const TraitVals& a, int n)
+{
+    float s = 0;
+#pragma unroll
+    for (int i = 0; i < GBK_TRAIT_NUM_MAX; ++i)
+        if (i < n) s += a[i];
+    return s;
+}
+// sum of a[i] * b[i] over the first n, in index order (b = null: a[i] * 1)
+__device__ __forceinline__ float tv_dot(const TraitVals& a, const TraitVals* b, int n)
+{
+    float s = 0;
+#pragma unroll
+    for (int i = 0; i < GBK_TRAIT_NUM_MAX; ++i)
+        if (i < n) s += a[i] * (b ? (*b)[i] : 1.f);
+    return s;
+}
+// product of the first n values, in index order
+__device__ __forceinline__ float tv_prod(const TraitVals& a, int n)
+{
+    float s = 1;
+#pragma unroll
+    for (int i = 0; i < GBK_TRAIT_NUM_MAX; ++i)
+        if (i < n) s *= a[i];
+    return s;
+}
+
 template<int KIND>
-__device__ __forceinline__ void eval_set(float* out, const TraitSet& ts, const Ring& g,
+__device__ __forceinline__ void eval_set(TraitVals& out, const TraitSet& ts, const Ring& g,
                                          float sin_incl, float cos_incl, float z, int& bad)
 {
     const float* cv = ts.cv;
@@ -315,7 +354,7 @@ __device__ __forceinline__ void eval_set(float* out, const TraitSet& ts, const R
             if (uid == 1) v = 1.f;
             else { bad = 1; v = NAN; }
         }
-        out[i] = v;
+        tv_set(out, i, v);
         cv += ts.cc[i];
         pv += ts.pc[i];
     }

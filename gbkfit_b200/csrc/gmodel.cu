@@ -118,9 +118,20 @@ __global__ void __launch_bounds__(256) smdisk_thick_kernel(DiskArgs a, int* stat
 
 // ---- mcdisk ------------------------------------------------------------------
 
+// The cloud's line at distance d from its centre without the amplitude:
+// exp(-d^2 / (2 sigma^2)) as 2^(-d^2 rinv) with rinv = log2(e) / (2 sigma^2),
+// by the PTX ex2.approx instruction (relative error ~2^-22; inside the +-5
+// sigma window the argument is >= -18.1, far from the flush to zero)
+__device__ __forceinline__ float line_e2(float d, float rinv)
+{
+    float e;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-(d * d) * rinv));
+    return e;
+}
+
 // Philox-4x32-10 (Salmon et al., SC'11), counter {ci, k/4, 0, 0}, key = seed
 struct Philox {
-    unsigned ci, k0, k1, k, w[4];
+    unsigned ci, k0, k1, k, w0, w1, w2, w3;   // the current block in registers
     __device__ void block(unsigned j)
     {
         unsigned c0 = ci, c1 = j, c2 = 0, c3 = 0, a = k0, b = k1;
@@ -133,12 +144,13 @@ struct Philox {
             a += 0x9E3779B9u;
             b += 0xBB67AE85u;
         }
-        w[0] = c0; w[1] = c1; w[2] = c2; w[3] = c3;
+        w0 = c0; w1 = c1; w2 = c2; w3 = c3;
     }
     __device__ float next()
     {
-        if ((k & 3u) == 0) block(k >> 2);
-        unsigned v = w[k & 3u];
+        const unsigned j = k & 3u;
+        if (j == 0) block(k >> 2);
+        const unsigned v = j == 0 ? w0 : j == 1 ? w1 : j == 2 ? w2 : w3;
         ++k;
         return (float)(((double)(v >> 8) + 0.5) * (1.0 / 16777216.0));
     }
@@ -155,7 +167,7 @@ __device__ __forceinline__ void sample_polar(float& r, float& t, Philox& rng, fl
 
 // math.hpp:207-217 (rejection sampling of ggauss; the moffat pdf is a stub 0
 // in the reference, so its loop always accepts the first x)
-__device__ float rejection(int kind, Philox& rng, float trunc, float c, float d)
+__device__ __forceinline__ float rejection(int kind, Philox& rng, float trunc, float c, float d)
 {
     // bounded: after 4096 rejections the last proposal is kept (the reference
     // loops without a limit; its acceptance rate here is >= 1/10)
@@ -171,8 +183,8 @@ __device__ float rejection(int kind, Philox& rng, float trunc, float c, float d)
 }
 
 // math.hpp:152-498 samplers as selected by traits.hpp:596-631, 1516-1590
-__device__ float rh_trait_rnd(Philox& rng, int uid, const float* c, const float* p, const Ring& g,
-                              int& bad)
+__device__ __forceinline__ float rh_trait_rnd(Philox& rng, int uid, const float* c, const float* p,
+                                              const Ring& g, int& bad)
 {
     int off = uid >= 1000 ? 1 : 0;
     int kind = uid - 1000 * off;
@@ -196,8 +208,8 @@ __device__ float rh_trait_rnd(Philox& rng, int uid, const float* c, const float*
 
 // gmodels.hpp:325-608 up to the splat: sample one cloud and return its
 // voxel and line.  false if the cloud is discarded.
-__device__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m, int ci, int& xo, int& yo, int& zo,
-                             SpaxelOut& o, int& bad)
+__device__ __forceinline__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m, int ci, int& xo,
+                                             int& yo, int& zo, SpaxelOut& o, int& bad)
 {
     Philox rng;
     rng.ci = (unsigned)ci;
@@ -263,18 +275,16 @@ __device__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m, int ci, int& xo
     g.r = rd;
     g.theta = theta;
     if (!disk_info(g.rnidx, rd, nrn, rnodes)) return false;
-    float pt[GBK_TRAIT_NUM_MAX] = {0, 0, 0, 0}, ht[GBK_TRAIT_NUM_MAX] = {0, 0, 0, 0};
+    TraitVals pt = {0, 0, 0, 0}, ht = {0, 0, 0, 0};
     if (a.spt.uids) {
         eval_set<K_SP>(pt, a.spt, g, 0, 0, 0, bad);
-        float sv = 0;
-        for (int i = 0; i < a.spt.n; ++i) sv += pt[i];
+        const float sv = tv_sum(pt, a.spt.n);
         if (!sv) return false;
     }
     float zd = rh_trait_rnd(rng, a.rht.uids[tidx], rhc, rhp, g, bad);
     if (a.zpt.uids) {
         eval_set<K_ZP>(pt, a.zpt, g, 0, 0, 0, bad);
-        float zv = 0;
-        for (int i = 0; i < a.zpt.n; ++i) zv += pt[i];
+        const float zv = tv_sum(pt, a.zpt.n);
         zd += zv;
     }
     float vsysi = a.vsys ? (a.loose ? lerp(rd, g.rnidx, rnodes, a.vsys, 0) : a.vsys[0]) : 0.f;
@@ -300,15 +310,15 @@ __device__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m, int ci, int& xo
     float vv = 0, dv = 0, wv = 1;
     if (a.vpt.uids) eval_set<K_VP>(pt, a.vpt, g, sinf(incli), cosf(incli), 0, bad);
     if (a.vht.uids) eval_set<K_VH>(ht, a.vht, g, 0, 0, fabsf(zd), bad);
-    for (int i = 0; i < a.vpt.n; ++i) vv += pt[i] * ht[i];
+    vv += tv_dot(pt, &ht, a.vpt.n);
     vv += vsysi;
     if (a.dpt.uids) eval_set<K_DP>(pt, a.dpt, g, 0, 0, 0, bad);
     if (a.dht.uids) eval_set<K_DH>(ht, a.dht, g, 0, 0, fabsf(zd), bad);
-    for (int i = 0; i < a.dpt.n; ++i) dv += pt[i] * ht[i];
+    dv += tv_dot(pt, &ht, a.dpt.n);
     dv = fabsf(dv);
     if (a.wpt.uids && a.wdata) {
         eval_set<K_WP>(pt, a.wpt, g, 0, 0, 0, bad);
-        for (int i = 0; i < a.wpt.n; ++i) wv *= pt[i];
+        wv *= tv_prod(pt, a.wpt.n);
     }
     float orv = rv;
     if (a.opacity) {
@@ -339,14 +349,14 @@ __global__ void __launch_bounds__(256) mcdisk_kernel(DiskArgs a, McArgs m, int* 
         if (a.image) atomicAdd(&a.image[x + (long long)a.sx * y], o.orv);
         int zlo, zhi;
         if (a.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
-            float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
-            float inv2c2 = 2 * o.dv * o.dv;
+            const float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
+            const float rinv = 1.4426950408889634f / (2 * o.dv * o.dv);
             float* col = a.scube + (x + (long long)a.sx * y);
             long long plane = (long long)a.sx * a.sy;
             for (int zs = zlo; zs <= zhi; ++zs) {
                 float zv = a.spec_zero + zs * a.spec_step;
                 float d = zv - o.vv;
-                atomicAdd(&col[plane * zs], o.orv * (amp * expf(-d * d / inv2c2)));
+                atomicAdd(&col[plane * zs], o.orv * (amp * line_e2(d, rinv)));
             }
         }
         long long idx = idx3(x, y, z, a.sx, a.sy);
@@ -383,7 +393,7 @@ __global__ void __launch_bounds__(256) mcdisk_v4_kernel(DiskArgs a, McArgs m, fl
         int zlo, zhi;
         if (lines && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
             const float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
-            const float inv2c2 = 2 * o.dv * o.dv;
+            const float rinv = 1.4426950408889634f / (2 * o.dv * o.dv);
             float* col = lines + (x + (long long)a.sx * y) * nzp;
             for (int z4 = zlo & ~3; z4 <= zhi; z4 += 4) {
                 float v[4];
@@ -391,7 +401,7 @@ __global__ void __launch_bounds__(256) mcdisk_v4_kernel(DiskArgs a, McArgs m, fl
                 for (int j = 0; j < 4; ++j) {
                     const int zs = z4 + j;
                     const float d = (a.spec_zero + zs * a.spec_step) - o.vv;
-                    v[j] = (zs >= zlo && zs <= zhi) ? o.orv * (amp * expf(-d * d / inv2c2)) : 0.f;
+                    v[j] = (zs >= zlo && zs <= zhi) ? o.orv * (amp * line_e2(d, rinv)) : 0.f;
                 }
                 atomicAdd(reinterpret_cast<float4*>(col + z4), make_float4(v[0], v[1], v[2], v[3]));
             }
@@ -506,12 +516,12 @@ __global__ void __launch_bounds__(256) mcdisk_fixed_kernel(DiskArgs a, McArgs m,
         int zlo, zhi;
         if (f.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
             const float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
-            const float inv2c2 = 2 * o.dv * o.dv;
+            const float rinv = 1.4426950408889634f / (2 * o.dv * o.dv);
             const long long plane = (long long)a.sx * a.sy;
             for (int zs = zlo; zs <= zhi; ++zs) {
                 const float zv = a.spec_zero + zs * a.spec_step;
                 const float d = zv - o.vv;
-                fixed_add(&f.scube[sp + plane * zs], o.orv * (amp * expf(-d * d / inv2c2)), kc);
+                fixed_add(&f.scube[sp + plane * zs], o.orv * (amp * line_e2(d, rinv)), kc);
             }
         }
         const long long idx = idx3(x, y, z, a.sx, a.sy);
