@@ -46,6 +46,7 @@ optionally, its model cube).
 import collections
 import threading
 import time
+import weakref
 from concurrent.futures import Future
 
 import numpy as np
@@ -57,6 +58,8 @@ from .disk import KINDS
 
 c_int3 = c_int * 3
 _lib = _native.lib()
+# per disk: {kind: (blob template, layout)} of Request.prepare
+_BLOBS = weakref.WeakKeyDictionary()
 
 
 def _ptr(t):
@@ -97,6 +100,7 @@ class Dataset:
                                            _ptr(self.spectrum)), 'fft_r2c')
         stream.synchronize()
         self.footprint = self.spectrum.numel() * 4 + 2 * 4 * int(np.prod(geom.size))
+        self.args_cache = {}    # (layout id, thick, window) -> (layout, ServeArgs template)
         self.holders = 0        # submitted requests that have not completed
         self.released = False   # unregistered
         self.smdisk, self.batched = smdisk, None
@@ -162,10 +166,46 @@ class Request:
         self.rows = None        # packed parameter row of a coalesced smdisk request
         self.cube = False       # a coalesced mcdisk request (model on the dataset's window)
 
+    @staticmethod
+    def _varying(packed, csum):
+        """The blob's arrays that change from request to request of one disk."""
+        for k in ('vsys', 'xpos', 'ypos', 'posa', 'incl'):
+            yield k, packed[k]
+        for k in KINDS:
+            t = packed[k]
+            yield k + '.pvalues', None if t is None else t['pvalues']
+        if csum is not None:
+            yield 'csum', csum
+
     def prepare(self):
         """Pack the parameters (Disk.pack, and the cloud budget of mcdisk)
-        into one byte blob: the arrays at 16-byte aligned offsets."""
+        into one byte blob: the arrays at 16-byte aligned offsets.  The
+        layout and the arrays that do not depend on the parameters (nodes,
+        trait uids, constants and counts) are kept per disk and kind, so a
+        request of a disk seen before only writes its own values into a copy
+        of that blob."""
         packed = self.disk.pack(self.params)
+        csum = None
+        if self.kind == 'mcdisk':
+            csum = np.asarray(self.disk.ncloudscsum(self.params, self.cflux), np.int32)
+            self.nclouds = int(csum[-1]) if csum.size else 0
+        cache = _BLOBS.get(self.disk)
+        if cache is None:
+            cache = _BLOBS[self.disk] = {}
+        ent = cache.get(self.kind)
+        if ent is not None:
+            template, layout = ent
+            blob = template.copy()
+            for name, a in self._varying(packed, csum):
+                off, n = layout[name]
+                if (a is None) != (off is None) or (a is not None and a.size != n):
+                    break       # another shape: lay the blob out again
+                if a is not None:
+                    a = np.ascontiguousarray(a, np.int32 if name == 'csum' else np.float32)
+                    blob[off:off + a.nbytes] = a.view(np.uint8).ravel()
+            else:
+                self.blob, self.layout = blob, layout
+                return
         arrays = []
         for k in ('subrnodes', 'vsys', 'xpos', 'ypos', 'posa', 'incl'):
             arrays.append((k, packed[k]))
@@ -173,9 +213,8 @@ class Request:
             t = packed[k]
             for f in ('uids', 'cvalues', 'ccounts', 'pvalues', 'pcounts'):
                 arrays.append((k + '.' + f, None if t is None else t[f]))
-        if self.kind == 'mcdisk':
-            csum = self.disk.ncloudscsum(self.params, self.cflux)
-            arrays.append(('csum', np.asarray(csum, np.int32)))
+        if csum is not None:
+            arrays.append(('csum', csum))
             arrays.append(('hoi', np.asarray(self.disk.hasordint(), np.uint8)))
         layout, off, chunks = {}, 0, []
         for name, a in arrays:
@@ -192,16 +231,27 @@ class Request:
         blob = np.zeros(max(off, 16), np.uint8)
         for o, b in chunks:
             blob[o:o + b.size] = b
-        if self.kind == 'mcdisk':
-            c = layout['csum']
-            self.nclouds = int(arrays[-2][1][-1]) if c[1] else 0
+        cache[self.kind] = (blob.copy(), layout)
         self.blob, self.layout = blob, layout
 
     def serve_args(self, ds, window=None):
         """The native argument block of this request against dataset ds
         (everything but the slot's buffers, which the scheduler sets); with
         window = (size, zero) of a batched evaluator's model window, the model
-        is evaluated on that window instead of the padded grid."""
+        is evaluated on that window instead of the padded grid.  The block
+        depends on the request only through its cloud budget: the rest is
+        built once per (layout, thick, window) and kept by the dataset."""
+        lay = self.layout
+        key = (id(lay), bool(self.thick), window is not None)
+        ent = ds.args_cache.get(key)
+        if ent is None or ent[0] is not lay:
+            ent = ds.args_cache[key] = (lay, self._serve_args(ds, window))
+        a = _native.ServeArgs.from_buffer_copy(ent[1])
+        if a.kind == 1:
+            a.cflux, a.nclouds = float(self.cflux), int(self.nclouds)
+        return a
+
+    def _serve_args(self, ds, window):
         lay, g = self.layout, ds.geom
         off = lambda name: -1 if lay[name][0] is None else lay[name][0]
         a = _native.ServeArgs()

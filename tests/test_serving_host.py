@@ -2,6 +2,8 @@
 its native argument block (gbkb200_serve_args) carry every packed array of
 the disk at the recorded offsets."""
 
+import collections
+
 import numpy as np
 
 from gbkfit_b200.disk import KINDS
@@ -15,6 +17,7 @@ class _Dataset:
         self.geom = geom
         self.size_hi = tuple(geom.size_hi)
         self.spectrum = self.obs = self.err = None
+        self.args_cache = {}
 
 
 def _stream():
@@ -37,9 +40,15 @@ def _check_array(req, name, want):
 
 
 def test_request_blob_and_argument_block():
+    """Every array of the blob and every field of the argument block, for
+    first requests of a disk (laid out in full) and later ones (written into
+    the disk's cached blob and argument templates)."""
     from gbkfit_b200.serving import Request
     st = _stream()
     kinds = set()
+    seen = collections.Counter((q['dataset'], q['kind']) for q in st.requests)
+    assert max(seen.values()) > 1       # some requests take the cached path
+    dsets = {}
     for q in st.requests:
         d = st.datasets[q['dataset']]
         r = Request(q['dataset'], q['kind'], d[q['kind']], q['params'], cflux=q['cflux'],
@@ -52,7 +61,9 @@ def test_request_blob_and_argument_block():
         for k in KINDS:
             for f in ('uids', 'cvalues', 'ccounts', 'pvalues', 'pcounts'):
                 _check_array(r, k + '.' + f, None if packed[k] is None else packed[k][f])
-        a = r.serve_args(_Dataset(d['geom']))
+        ds = dsets.setdefault(q['dataset'], _Dataset(d['geom']))
+        a = r.serve_args(ds)
+        assert bytes(a) == bytes(r._serve_args(ds, None))
         off = lambda name: -1 if r.layout[name][0] is None else r.layout[name][0]
         assert a.blob_bytes == r.blob.size and a.nrnodes == len(packed['subrnodes'])
         assert a.off_rnodes == off('subrnodes') and a.off_incl == off('incl')
