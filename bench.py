@@ -663,7 +663,7 @@ def run_mcdisk(args):
                            None, None)
 
     ms = {}
-    for mode, name in ((0, 'fast'), (1, 'deterministic'), (2, 'vector_atomics')):
+    for mode, name in ((0, 'fast'), (1, 'deterministic'), (3, 'scalar_atomics')):
         gm.set_mcdisk(seed=42, mode=mode)
         ms[name] = _events_ms(call, args.steps, args.warmup)
     gm.set_mcdisk(seed=42, mode=0)
@@ -683,7 +683,7 @@ def run_mcdisk(args):
                 value=round(1e3 / ms['fast'], 2), unit='evals/s', n_gpus=1, steps=args.steps,
                 warmup=args.warmup, ms_per_step=round(ms['fast'], 4),
                 ms_deterministic=round(ms['deterministic'], 4),
-                ms_vector_atomics=round(ms['vector_atomics'], 4), higher_is_better=True,
+                ms_scalar_atomics=round(ms['scalar_atomics'], 4), higher_is_better=True,
                 dtype='f32', data='synthetic', gpu_launches=args.steps,
                 config=dict(workload='mcdisk_cube256', nclouds=n, grid=[nx, ny, g['spat_size'][2], nz],
                             l2='flushed before every call (256 MB write)'),
@@ -763,11 +763,21 @@ def run_smdisk64(args):
                    kind='reference', ms_per_eval=round(dt * 1e3, 3),
                    sample=f'{n} evaluations of the same chain: smdisk + moments from the '
                           'reference templates (OpenMP), scipy.fft (all cores) for the FFT')
+        # moment 0 on the spaxels the reference keeps; moments 1 and 2 (ratios
+        # to moment 0) where moment 0 is at least 1e-3 of its peak: near the
+        # 1e-6 cutoff the fp32 convolution's noise dominates them in any fp32
+        # chain, the reference's included
         v = np.isfinite(rd[0])
+        m0 = np.where(v, rd[0], 0.0)
+        strong = v & (np.abs(m0) >= 1e-3 * np.max(np.abs(m0)))
+        sel = [v, strong, strong]
+        nrm = lambda a: float(np.sqrt(np.sum(np.asarray(a, np.float64) ** 2)))
         parity = dict(vs='the reference CPU chain (fp32)',
-                      cube_rel_err=float(np.max(np.abs(cube - rcube)) / np.max(np.abs(rcube))),
-                      map_rel_err=[float(np.max(np.abs(maps[i][v] - rd[i][v]))
-                                         / np.max(np.abs(rd[i][v]))) for i in range(3)])
+                      cube_rel_err=nrm(cube - rcube) / nrm(rcube),
+                      map_rel_err=[nrm(maps[i][sel[i]] - rd[i][sel[i]]) / nrm(rd[i][sel[i]])
+                                   for i in range(3)],
+                      norm='normwise (L2) relative; maps 1, 2 where map 0 >= 1e-3 of its peak '
+                           f'({int(strong.sum())} of {int(v.sum())} spaxels)')
     return dict(metric='smdisk_cube64 evaluations/s (smdisk -> PSF/LSF FFT -> moments 0/1/2 '
                        '+ cube, per call, synchronous)',
                 value=round(1e3 / ms, 1), unit='evals/s', n_gpus=1, steps=args.steps,

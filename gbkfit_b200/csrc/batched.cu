@@ -501,11 +501,7 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     // otherwise 54 KB (four blocks per SM)
     int bpmax = 4 * (2 * ((P.Nx + 7) / 8 - 1) + NW);
     bpmax += ((4 - bpmax % 32) + 32) % 32;
-    // range entries of the band's input rows, their per-row ranges and the
-    // per-group column ranges of a pass
-    const long long rows_b = P.band + P.K - 1;
-    const long long xr_bytes = rows_b * P.nch * sizeof(int) + ((rows_b + 1) & ~1LL) * sizeof(int) +
-                               ((P.band + P.K + 7) / 8 + 2) * 2 * sizeof(int);
+    const long long xr_bytes = (long long)(P.band + P.K - 1) * P.nch * sizeof(int);
     const long long need_min = (long long)(P.K + 15) * bpmax;
     const long long need_all = (long long)(P.band + P.K + 7) * bpmax;
     // PSF kernel variant: 0-2 sized for 4 resident blocks per SM, 3-5 for 5,

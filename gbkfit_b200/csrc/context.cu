@@ -72,7 +72,7 @@ extern "C" int gbkb200_ctx_set_sync(gbkb200_ctx* ctx, int sync)
 
 extern "C" int gbkb200_ctx_set_mcdisk(gbkb200_ctx* ctx, unsigned long long seed, int mode)
 {
-    if (!ctx || mode < 0 || mode > 2) return GBKB200_ERR_INVALID_ARG;
+    if (!ctx || mode < 0 || mode > 3) return GBKB200_ERR_INVALID_ARG;
     ctx->seed = seed;
     ctx->mc_mode = mode;
     return GBKB200_OK;

@@ -263,10 +263,6 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     extern __shared__ float4 sm4[];
     float* S = reinterpret_cast<float*>(sm4);                   // (rows of a pass, bp)
     int* s_xr = reinterpret_cast<int*>(S + P.cap);              // (in1 - ob0, nch) entries
-    // per input row, the nonzero column range of the row (xmin | xmax << 16, or -1)
-    int* s_rx = s_xr + (P.band + K - 1) * P.nch;
-    // per 8-row output group of a pass, the columns the y FIR can make nonzero
-    int2* s_grp = reinterpret_cast<int2*>(s_rx + ((P.band + K - 1 + 1) & ~1));
     __shared__ float warp_part[NWARPS];
     __shared__ int s_box[4];
     // sets vary fastest: the blocks in flight share a few planes of the data
@@ -335,19 +331,6 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
         if (threadIdx.x == 0) P.partials[part] = sat_box(T, ld, ob0, ob1, 0, P.Nx);
         return;
     }
-    // per-row nonzero column ranges (read after the next barrier)
-    for (int i = threadIdx.x; i < in1 - ob0; i += KB_THREADS) {
-        int lo = INT_MAX, hi = -1;
-        for (int ch = 0; ch < P.nch; ++ch) {
-            const int v = s_xr[i * P.nch + ch];
-            if (v >= 0) {
-                lo = min(lo, v & 0xffff);
-                hi = max(hi, v >> 16);
-            }
-        }
-        s_rx[i] = hi >= 0 ? (lo | (hi << 16)) : -1;
-    }
-    __syncthreads();
     // output box: x in 8-column strips [g_lo, g_hi], rows [yo_lo, yb_end) in 8-row groups
     const int g_lo = max(0, x0 - K + 1) >> 3, g_hi = min(P.Nx - 1, x1) >> 3;
     const int ns8 = g_hi - g_lo + 1, ns4 = 2 * ns8, sl0 = 2 * g_lo;
@@ -367,14 +350,15 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     const float4* src = reinterpret_cast<const float4*>(P.mplanes + prow * P.pitch);
     const int pbase = zo * P.Ny * P.Nx;       // the data cube has < 2^31 voxels
     float sum = 0.f;
-    unsigned long long c_v = 0;           // residual voxels of the box (thread 0)
-    unsigned n_x = 0, n_y = 0;            // x-FIR strips and y-FIR items this thread ran
+    unsigned long long c_x = 0, c_y = 0, c_v = 0;    // executed work (thread 0)
     for (int ys = yo_lo; ys < yb_end; ys += bo) {
         const int ye = min(yb_end, ys + bo);                 // outputs [ys, ye)
         const int ng = (ye - ys + 7) / 8;
         const int rend = ys + 8 * ng + K - 1;                // rows [ys, rend) are read
         const int ly0 = max(y0, ys), ly1 = min(y1, rend - 1);
         if (P.counters && threadIdx.x == 0) {
+            if (ly0 <= ly1) c_x += (unsigned long long)(ly1 - ly0 + 1) * ns8 * 8 * K;
+            c_y += (unsigned long long)ng * ns4 * 32 * K;
             c_v += (unsigned long long)(ye - ys) * (xb_end - xb0);
         }
         // load rows [ly0, ly1]: each row chunk's nonzero range, zeros elsewhere
@@ -409,20 +393,6 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
                 }
             }
         }
-        // per 8-row output group g of the pass, the output columns [A, B] the y FIR
-        // can make nonzero: its input rows' nonzero columns widened by the x FIR
-        // (an x-filtered row is nonzero at most on [xmin - K + 1, xmax])
-        for (int gi = threadIdx.x; gi < ng; gi += KB_THREADS) {
-            int A = INT_MAX, B = -1;
-            for (int y = ys + 8 * gi; y < ys + 8 * gi + K + 7; ++y) {
-                const int e = (y >= ob0 && y < in1) ? s_rx[y - ob0] : -1;
-                if (e >= 0) {
-                    A = min(A, (e & 0xffff) - K + 1);
-                    B = max(B, e >> 16);
-                }
-            }
-            s_grp[gi] = make_int2(A, B);
-        }
         cp_async_wait_all();
         __syncthreads();
         // x FIR in place: S[y][xo] = sum_s vr[s] S[y][xo + s].  A warp owns whole
@@ -441,14 +411,8 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
             const int di = 32 / ns8, dg = 32 % ns8;
             int ri = lane / ns8, gi = lane % ns8;       // the lane's pair: row index, strip
             for (int q0 = 0; q0 < npairs; q0 += 32) {
-                // a strip whose input window [8g, 8g + K + 7) holds no nonzero value
-                // is skipped: its columns are zeros already, as its output would be
-                const int ry = ly0 + warp + NWARPS * ri;
-                const int e = (q0 + lane < npairs && ry < in1) ? s_rx[ry - ob0] : -1;
-                const int gx = 8 * (g_lo + gi);
-                const bool act = e >= 0 && gx <= (e >> 16) && gx + K + 6 >= (e & 0xffff);
-                n_x += act;
-                float4* row = reinterpret_cast<float4*>(S) + (ry - ys) * bp4;
+                const bool act = q0 + lane < npairs;
+                float4* row = reinterpret_cast<float4*>(S) + (ly0 + warp + NWARPS * ri - ys) * bp4;
                 float w[4 * NW];
                 if (act) {
 #pragma unroll
@@ -480,13 +444,6 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
             }
         }
         __syncthreads();
-        // item (8-row group, float4 column) can be nonzero: its columns meet the
-        // group's nonzero column range
-        auto item_live = [&](int item) {
-            const int2 ab = s_grp[item / ns4];
-            const int c0 = xb0 + 4 * (item % ns4);
-            return c0 + 3 >= ab.x && c0 <= ab.y;
-        };
         if constexpr (EPI == 0) {
             constexpr int kIt = 1;     // y items per thread and round
             // y FIR in place: model(yo, xo) = sum_t ur[t] S[yo + t][xo], written to S row yo.
@@ -511,10 +468,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
                             acc[it][q][0] = make_float2(0.f, 0.f);
                             acc[it][q][1] = make_float2(0.f, 0.f);
                         }
-                        // an item whose input window is zero at its columns keeps its
-                        // rows' zeros (its output would be zero)
-                        if (item < nitems && item_live(item)) {
-                            ++n_y;
+                        if (item < nitems) {
                             const int rb = 8 * (item / ns4), s4 = item % ns4;
                             const float4* colp = reinterpret_cast<const float4*>(S) + rb * bp4 + s4;
     #pragma unroll
@@ -536,7 +490,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     #pragma unroll
                     for (int it = 0; it < kIt; ++it) {
                         const int item = gr0 + threadIdx.x + it * KB_THREADS;
-                        if (item < nitems && item_live(item)) {
+                        if (item < nitems) {
                             const int rb = 8 * (item / ns4), s4 = item % ns4;
     #pragma unroll
                             for (int q = 0; q < 8; ++q)
@@ -637,20 +591,16 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
                         }
                     }
                     const float4* colp = reinterpret_cast<const float4*>(S) + rb * bp4 + s4;
-                    // an item whose input window is zero at its columns has a zero model
-                    if (item_live(item)) {
-                        ++n_y;
     #pragma unroll
-                        for (int m = 0; m < K + 7; ++m) {
-                            const float4 p = colp[m * bp4];
-                            const float2 pxy = make_float2(p.x, p.y), pzw = make_float2(p.z, p.w);
+                    for (int m = 0; m < K + 7; ++m) {
+                        const float4 p = colp[m * bp4];
+                        const float2 pxy = make_float2(p.x, p.y), pzw = make_float2(p.z, p.w);
     #pragma unroll
-                            for (int q = 0; q < 8; ++q) {
-                                const int t = m - q;
-                                if (t >= 0 && t < K) {
-                                    acc[q][0] = __ffma2_rn(P.ur2[t], pxy, acc[q][0]);
-                                    acc[q][1] = __ffma2_rn(P.ur2[t], pzw, acc[q][1]);
-                                }
+                        for (int q = 0; q < 8; ++q) {
+                            const int t = m - q;
+                            if (t >= 0 && t < K) {
+                                acc[q][0] = __ffma2_rn(P.ur2[t], pxy, acc[q][0]);
+                                acc[q][1] = __ffma2_rn(P.ur2[t], pzw, acc[q][1]);
                             }
                         }
                     }
@@ -709,17 +659,6 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
             if (yo < yo_lo || yo >= yb_end || xo < xb0 || xo >= xb_end) model[i] = 0.f;
         }
     }
-    if (P.counters) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            n_x += __shfl_xor_sync(0xffffffffu, n_x, o);
-            n_y += __shfl_xor_sync(0xffffffffu, n_y, o);
-        }
-        if (lane == 0) {
-            atomicAdd(&P.counters[GBK_CTR_KB_XFMA], (unsigned long long)n_x * 8 * K);
-            atomicAdd(&P.counters[GBK_CTR_KB_YFMA], (unsigned long long)n_y * 32 * K);
-        }
-    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     if (lane == 0) warp_part[warp] = sum;
@@ -728,7 +667,11 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
         float s = 0.f;
         for (int w = 0; w < NWARPS; ++w) s += warp_part[w];
         P.partials[part] = (double)s + outside;
-        if (P.counters) atomicAdd(&P.counters[GBK_CTR_KB_VOX], c_v);
+        if (P.counters) {
+            atomicAdd(&P.counters[GBK_CTR_KB_XFMA], c_x);
+            atomicAdd(&P.counters[GBK_CTR_KB_YFMA], c_y);
+            atomicAdd(&P.counters[GBK_CTR_KB_VOX], c_v);
+        }
     }
 }
 

@@ -667,13 +667,12 @@ extern "C" int gbkb200_gmodel_mcdisk_evaluate_f32(gbkb200_ctx* ctx, float cflux,
     m.seed = ctx->seed;
     int blocks = (nclouds + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    if (ctx->mc_mode == 0 || (ctx->mc_mode == 2 && !a.scube)) {
-        mcdisk_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, ctx->d_status);
-        GBK_CUDA_TRY(cudaGetLastError());
-        return gbk_finish(ctx);
-    }
-    if (ctx->mc_mode == 2) {
-        // channel-contiguous line cube in the context's scratch
+    // modes 0 and 2: the lines channel-contiguous in the context's scratch with
+    // vector atomics when the spectral cube is requested (mode 0 falls back to
+    // one atomic per channel if the scratch cannot be had); mode 3 and the
+    // other outputs: one fp32 atomic per channel and element
+    bool vec = (ctx->mc_mode == 0 || ctx->mc_mode == 2) && a.scube;
+    if (vec) {
         const long long nsp = (long long)a.sx * a.sy;
         const int nzp = (a.spec_size + 3) & ~3;
         const size_t need = (size_t)nsp * nzp * sizeof(float);
@@ -681,9 +680,24 @@ extern "C" int gbkb200_gmodel_mcdisk_evaluate_f32(gbkb200_ctx* ctx, float cflux,
             if (ctx->mc_scratch) cudaFree(ctx->mc_scratch);
             ctx->mc_scratch = nullptr;
             ctx->mc_scratch_bytes = 0;
-            if (cudaMalloc(&ctx->mc_scratch, need) != cudaSuccess) return GBKB200_ERR_OOM;
-            ctx->mc_scratch_bytes = need;
+            if (cudaMalloc(&ctx->mc_scratch, need) == cudaSuccess) {
+                ctx->mc_scratch_bytes = need;
+            } else {
+                (void)cudaGetLastError();      // the failed allocation is not sticky
+                if (ctx->mc_mode == 2) return GBKB200_ERR_OOM;
+                vec = false;
+            }
         }
+    }
+    if (ctx->mc_mode == 3 || ((ctx->mc_mode == 0 || ctx->mc_mode == 2) && !vec)) {
+        mcdisk_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, ctx->d_status);
+        GBK_CUDA_TRY(cudaGetLastError());
+        return gbk_finish(ctx);
+    }
+    if (vec) {
+        const long long nsp = (long long)a.sx * a.sy;
+        const int nzp = (a.spec_size + 3) & ~3;
+        const size_t need = (size_t)nsp * nzp * sizeof(float);
         float* lines = static_cast<float*>(ctx->mc_scratch);
         GBK_CUDA_TRY(cudaMemsetAsync(lines, 0, need, ctx->stream));
         mcdisk_v4_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, lines, nzp, ctx->d_status);

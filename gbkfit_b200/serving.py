@@ -125,8 +125,11 @@ class Dataset:
             self.mc_h = torch.empty((self.mc_sets, self.MC_STAGE), dtype=torch.uint8,
                                     pin_memory=True)
             self.mc_d = torch.empty((self.mc_sets, self.MC_STAGE), dtype=torch.uint8, device=dev)
+            # fast mode: the clouds' lines go through a channel-contiguous
+            # scratch cube of the window held by the evaluator's context
             self.batched.ctx.set_mcdisk(mc_seed, 0)
-            self.footprint += self.mc_cubes.numel() * 4 + self.mc_d.numel()
+            self.footprint += (self.mc_cubes.numel() * 4 + self.mc_d.numel() +
+                               4 * wx * wy * ((wz + 3) // 4 * 4))
 
     def request_layout(self):
         """Byte offsets of one in-flight request's device buffers (padded
@@ -298,7 +301,8 @@ class _Slot:
         self.h_stage = torch.empty(self.STAGE, dtype=torch.uint8, pin_memory=True)
         self.d_stage = torch.empty(self.STAGE, dtype=torch.uint8, device=dev)
         self.ctx = _native.Context(device=dev.index, stream=self.stream, sync=False)
-        self.ctx.set_mcdisk(mc_seed, 0)
+        # one atomic per channel: no scratch cube outside the HBM budget
+        self.ctx.set_mcdisk(mc_seed, 3)
         self.event = torch.cuda.Event()
         self.out = torch.empty(1, dtype=torch.float32, pin_memory=True)
         self.status = torch.zeros(1, dtype=torch.int32, pin_memory=True)

@@ -56,18 +56,20 @@ int gbkb200_ctx_set_stream(gbkb200_ctx* ctx, void* stream);
 /* sync = 1: return after the work finished (reference semantics, wrapper.cu
  * ends every call with cudaDeviceSynchronize); sync = 0: enqueue only */
 int gbkb200_ctx_set_sync(gbkb200_ctx* ctx, int sync);
-/* seed of the counter-based cloud generator of mcdisk_evaluate; mode 0 =
- * fast (fp32 atomics: sums depend on the order clouds land in, in the last
- * bits), mode 1 = deterministic: the accumulated outputs (scube, image, rdata,
- * ordata and their _cmp forms) are summed in 64-bit fixed point, bit-identical
- * run to run and exact to ~2^-(62 - log2 nclouds) of the largest contribution;
- * it takes an extra bound pass over the clouds and scratch of 8 bytes per
- * accumulated element held by the context; mode 2 = fast with the lines
- * accumulated channel-contiguous in a scratch cube held by the context (4
- * bytes per scube element) with 16-byte vector atomics, then added to scube
- * (sums order-dependent in the last bits, as mode 0).  The assigned maps
- * (wdata, vdata_cmp, ddata_cmp) keep the reference's last-writer-wins race in
- * every mode. */
+/* seed of the counter-based cloud generator of mcdisk_evaluate and its
+ * accumulation mode.  Mode 0 = fast (the default; fp32 atomics, sums depend
+ * on the order clouds land in, in the last bits): the lines are accumulated
+ * channel-contiguous in a scratch cube held by the context (4 bytes per
+ * scube element) with 16-byte vector atomics, then added to scube; when that
+ * scratch cannot be allocated, as mode 3.  Mode 1 = deterministic: the
+ * accumulated outputs (scube, image, rdata, ordata and their _cmp forms) are
+ * summed in 64-bit fixed point, bit-identical run to run and exact to
+ * ~2^-(62 - log2 nclouds) of the largest contribution; it takes an extra
+ * bound pass over the clouds and scratch of 8 bytes per accumulated element
+ * held by the context.  Mode 2 = mode 0 without the fallback (an allocation
+ * failure is returned).  Mode 3 = fast with one fp32 atomic per channel into
+ * scube (no scratch).  The assigned maps (wdata, vdata_cmp, ddata_cmp) keep
+ * the reference's last-writer-wins race in every mode. */
 int gbkb200_ctx_set_mcdisk(gbkb200_ctx* ctx, unsigned long long seed, int mode);
 /* waits for the context's stream, then returns the status raised by kernels
  * since the last call (GBKB200_OK, _BAD_TRAIT or _TIMEOUT) and clears it */

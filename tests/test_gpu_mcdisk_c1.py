@@ -76,12 +76,14 @@ def test_c1_fast_mode_matches_deterministic(c1):
         <= 1e-5 * det['scube'].astype(np.float64).sum()
 
 
-def test_c1_vector_mode_matches_deterministic(c1):
+@pytest.mark.parametrize('mode', [2, 3])
+def test_c1_atomic_modes_match_deterministic(c1, mode):
     """Mode 2 (lines accumulated channel-contiguous with 16-byte vector
-    atomics, then added to the cube) sums the same contributions as the
-    deterministic mode, to fp32 accumulation error."""
+    atomics, then added to the cube: mode 0's path) and mode 3 (one fp32
+    atomic per channel) sum the same contributions as the deterministic
+    mode, to fp32 accumulation error."""
     det = c1.get('det') or c1['run'](1)
-    v4 = c1['run'](2)
+    v4 = c1['run'](mode)
     assert np.array_equal(v4['rdata'] != 0, det['rdata'] != 0)
     assert rel_err(v4['rdata'], det['rdata']) <= 1e-4
     assert rel_err(v4['scube'], det['scube']) <= 1e-5

@@ -281,7 +281,9 @@ def test_mcdisk_flux_and_clouds(be, oracle_built):
 
 def test_mcdisk_deterministic_mode(be, oracle_built):
     """Mode 1 (64-bit fixed-point accumulation) gives bit-identical cubes and
-    maps run to run, and agrees with the fast fp32-atomic mode."""
+    maps run to run, and agrees with the fast fp32-atomic modes (0 and 2:
+    vector atomics into a channel-contiguous scratch cube; 3: one atomic per
+    channel)."""
     import torch
     from gbkfit_b200 import workloads
     w = workloads.mcdisk_cube256(nclouds=300_000)
@@ -305,13 +307,14 @@ def test_mcdisk_deterministic_mode(be, oracle_built):
                    torch.from_numpy(hoi).cuda(), pd, g, outs)
         return {k: v.cpu().numpy() for k, v in outs.items()}
 
-    a, b, fast, v4 = run(1), run(1), run(0), run(2)
+    a, b, fast, v4, scalar = run(1), run(1), run(0), run(2), run(3)
     be['gmodel'].set_mcdisk(seed=42, mode=0)
-    # mode 2 (vector atomics into a channel-contiguous scratch cube) sums the
-    # same contributions
-    assert rel_err(v4['scube'], a['scube']) <= 1e-5
-    for k in ('image', 'rdata'):
-        assert rel_err(v4[k], a[k]) <= 1e-4, k
+    # mode 2 (vector atomics into a channel-contiguous scratch cube; mode 0's
+    # path) and mode 3 (one atomic per channel) sum the same contributions
+    for o in (v4, scalar):
+        assert rel_err(o['scube'], a['scube']) <= 1e-5
+        for k in ('image', 'rdata'):
+            assert rel_err(o[k], a[k]) <= 1e-4, k
     for k in a:
         assert np.array_equal(a[k], b[k]), k
     # every cloud adds cflux / (dx dy) to the maps: the fixed-point sums are
