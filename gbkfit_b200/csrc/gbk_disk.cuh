@@ -74,35 +74,37 @@ static __device__ bool smdisk_spaxel(const DiskArgs& a, const DiskConst& kc, int
         if (!disk_info(g.rnidx, g.r, a.nrnodes, a.rnodes)) return false;
     }
 
-    TraitVals pt = {0, 0, 0, 0}, ht = {0, 0, 0, 0};
+    float pt[GBK_TRAIT_NUM_MAX] = {0, 0, 0, 0}, ht[GBK_TRAIT_NUM_MAX] = {0, 0, 0, 0};
     float rv = 0, vv = 0, dv = 0, wv = 1;
     if (a.spt.uids) {
         eval_set<K_SP>(pt, a.spt, g, 0, 0, 0, bad);
-        const float sv = tv_sum(pt, a.spt.n);
+        float sv = 0;
+        for (int i = 0; i < a.spt.n; ++i) sv += pt[i];
         if (!sv) return false;
     }
     if (a.zpt.uids) {
         eval_set<K_ZP>(pt, a.zpt, g, 0, 0, 0, bad);
-        const float zv = tv_sum(pt, a.zpt.n);
+        float zv = 0;
+        for (int i = 0; i < a.zpt.n; ++i) zv += pt[i];
         zn += zv;
     }
     if (a.rpt.uids) eval_set<K_RP>(pt, a.rpt, g, 0, 0, 0, bad);
     if (a.rht.uids) eval_set<K_RH>(ht, a.rht, g, 0, 0, fabsf(zn), bad);
-    rv += tv_dot(pt, thin ? nullptr : &ht, a.rpt.n);
+    for (int i = 0; i < a.rpt.n; ++i) rv += pt[i] * (thin ? 1.f : ht[i]);
     if (!rv) return false;
     if (thin) rv /= cosf(incli);
     else rv *= a.stz;
     if (a.vpt.uids) eval_set<K_VP>(pt, a.vpt, g, sinf(incli), cosf(incli), 0, bad);
     if (a.vht.uids) eval_set<K_VH>(ht, a.vht, g, 0, 0, fabsf(zn), bad);
-    vv += tv_dot(pt, thin ? nullptr : &ht, a.vpt.n);
+    for (int i = 0; i < a.vpt.n; ++i) vv += pt[i] * (thin ? 1.f : ht[i]);
     vv += vsysi;
     if (a.dpt.uids) eval_set<K_DP>(pt, a.dpt, g, 0, 0, 0, bad);
     if (a.dht.uids) eval_set<K_DH>(ht, a.dht, g, 0, 0, fabsf(zn), bad);
-    dv += tv_dot(pt, thin ? nullptr : &ht, a.dpt.n);
+    for (int i = 0; i < a.dpt.n; ++i) dv += pt[i] * (thin ? 1.f : ht[i]);
     dv = fabsf(dv);
     if (a.wpt.uids && a.wdata) {
         eval_set<K_WP>(pt, a.wpt, g, 0, 0, 0, bad);
-        wv *= tv_prod(pt, a.wpt.n);
+        for (int i = 0; i < a.wpt.n; ++i) wv *= pt[i];
     }
     float orv = rv;
     if (a.opacity) {

@@ -287,9 +287,7 @@ static __device__ float rh_trait(int uid, const float* c, const float* p, const 
 
 enum TraitKind { K_RP, K_RH, K_VP, K_VH, K_DP, K_DH, K_ZP, K_SP, K_WP };
 
-// traits.hpp:1887-1919: evaluate the n traits of a set, advancing the
-// constants/parameters pointers by the per-trait counts.
-// The per-set trait values live in fixed-size arrays that are only indexed by
+// The per-set trait values of the cloud kernels live in fixed-size arrays that are only indexed by
 // constants (the loops over the set's n traits are unrolled to the maximum
 // with a guard, stores go through selects), so they stay in registers
 // instead of the stack.
@@ -328,33 +326,58 @@ __device__ __forceinline__ float tv_prod(const TraitVals& a, int n)
     return s;
 }
 
+// the value of trait uid of a set of kind KIND (traits.hpp:1887-1919)
 template<int KIND>
-__device__ __forceinline__ void eval_set(TraitVals& out, const TraitSet& ts, const Ring& g,
+__device__ __forceinline__ float trait_value(int uid, const float* cv, const float* pv,
+                                             const Ring& g, float sin_incl, float cos_incl,
+                                             float z, int& bad)
+{
+    float v;
+    if (KIND == K_RP) v = p_profile(uid >= 1000 ? uid - 1000 : uid, cv, pv, g, bad);
+    else if (KIND == K_DP) v = p_profile(uid, cv, pv, g, bad);
+    else if (KIND == K_VP) v = vp_trait(uid, cv, pv, g, sin_incl, cos_incl, bad);
+    else if (KIND == K_RH) v = rh_trait(uid, cv, pv, g, z, bad);
+    else if (KIND == K_ZP) {
+        if (uid == 101) v = nw(g, pv, 0);
+        else if (uid == 102) v = p_nw_harmonic(g, cv, pv);
+        else { bad = 1; v = NAN; }
+    } else if (KIND == K_SP) {
+        if (uid == 1) v = azrange(g.theta, pv[0] * GBK_D2R, pv[1] * GBK_D2R);
+        else if (uid == 101) v = azrange(g.theta, nw(g, pv, 0) * GBK_D2R,
+                                         nw(g, pv, g.nrnodes) * GBK_D2R);
+        else { bad = 1; v = NAN; }
+    } else {   // K_VH, K_DH, K_WP: the only implemented kind (uid 1) is 1
+        if (uid == 1) v = 1.f;
+        else { bad = 1; v = NAN; }
+    }
+    return v;
+}
+
+// the n traits of a set into out[i], advancing the constants/parameters
+// pointers by the per-trait counts (the smooth-disk kernels)
+template<int KIND>
+__device__ __forceinline__ void eval_set(float* out, const TraitSet& ts, const Ring& g,
                                          float sin_incl, float cos_incl, float z, int& bad)
 {
     const float* cv = ts.cv;
     const float* pv = ts.pv;
     for (int i = 0; i < ts.n; ++i) {
-        int uid = ts.uids[i];
-        float v;
-        if (KIND == K_RP) v = p_profile(uid >= 1000 ? uid - 1000 : uid, cv, pv, g, bad);
-        else if (KIND == K_DP) v = p_profile(uid, cv, pv, g, bad);
-        else if (KIND == K_VP) v = vp_trait(uid, cv, pv, g, sin_incl, cos_incl, bad);
-        else if (KIND == K_RH) v = rh_trait(uid, cv, pv, g, z, bad);
-        else if (KIND == K_ZP) {
-            if (uid == 101) v = nw(g, pv, 0);
-            else if (uid == 102) v = p_nw_harmonic(g, cv, pv);
-            else { bad = 1; v = NAN; }
-        } else if (KIND == K_SP) {
-            if (uid == 1) v = azrange(g.theta, pv[0] * GBK_D2R, pv[1] * GBK_D2R);
-            else if (uid == 101) v = azrange(g.theta, nw(g, pv, 0) * GBK_D2R,
-                                             nw(g, pv, g.nrnodes) * GBK_D2R);
-            else { bad = 1; v = NAN; }
-        } else {   // K_VH, K_DH, K_WP: the only implemented kind (uid 1) is 1
-            if (uid == 1) v = 1.f;
-            else { bad = 1; v = NAN; }
-        }
-        tv_set(out, i, v);
+        out[i] = trait_value<KIND>(ts.uids[i], cv, pv, g, sin_incl, cos_incl, z, bad);
+        cv += ts.cc[i];
+        pv += ts.pc[i];
+    }
+}
+
+// the same into register-resident values (the cloud kernels: their trait
+// values stay off the stack)
+template<int KIND>
+__device__ __forceinline__ void eval_set_r(TraitVals& out, const TraitSet& ts, const Ring& g,
+                                           float sin_incl, float cos_incl, float z, int& bad)
+{
+    const float* cv = ts.cv;
+    const float* pv = ts.pv;
+    for (int i = 0; i < ts.n; ++i) {
+        tv_set(out, i, trait_value<KIND>(ts.uids[i], cv, pv, g, sin_incl, cos_incl, z, bad));
         cv += ts.cc[i];
         pv += ts.pc[i];
     }

@@ -277,13 +277,13 @@ __device__ __forceinline__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m,
     if (!disk_info(g.rnidx, rd, nrn, rnodes)) return false;
     TraitVals pt = {0, 0, 0, 0}, ht = {0, 0, 0, 0};
     if (a.spt.uids) {
-        eval_set<K_SP>(pt, a.spt, g, 0, 0, 0, bad);
+        eval_set_r<K_SP>(pt, a.spt, g, 0, 0, 0, bad);
         const float sv = tv_sum(pt, a.spt.n);
         if (!sv) return false;
     }
     float zd = rh_trait_rnd(rng, a.rht.uids[tidx], rhc, rhp, g, bad);
     if (a.zpt.uids) {
-        eval_set<K_ZP>(pt, a.zpt, g, 0, 0, 0, bad);
+        eval_set_r<K_ZP>(pt, a.zpt, g, 0, 0, 0, bad);
         const float zv = tv_sum(pt, a.zpt.n);
         zd += zv;
     }
@@ -308,16 +308,16 @@ __device__ __forceinline__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m,
     if (fx < 0 || fx >= a.sx || fy < 0 || fy >= a.sy || fz < 0 || fz >= a.sz) return false;
     int x = (int)fx, y = (int)fy, z = (int)fz;
     float vv = 0, dv = 0, wv = 1;
-    if (a.vpt.uids) eval_set<K_VP>(pt, a.vpt, g, sinf(incli), cosf(incli), 0, bad);
-    if (a.vht.uids) eval_set<K_VH>(ht, a.vht, g, 0, 0, fabsf(zd), bad);
+    if (a.vpt.uids) eval_set_r<K_VP>(pt, a.vpt, g, sinf(incli), cosf(incli), 0, bad);
+    if (a.vht.uids) eval_set_r<K_VH>(ht, a.vht, g, 0, 0, fabsf(zd), bad);
     vv += tv_dot(pt, &ht, a.vpt.n);
     vv += vsysi;
-    if (a.dpt.uids) eval_set<K_DP>(pt, a.dpt, g, 0, 0, 0, bad);
-    if (a.dht.uids) eval_set<K_DH>(ht, a.dht, g, 0, 0, fabsf(zd), bad);
+    if (a.dpt.uids) eval_set_r<K_DP>(pt, a.dpt, g, 0, 0, 0, bad);
+    if (a.dht.uids) eval_set_r<K_DH>(ht, a.dht, g, 0, 0, fabsf(zd), bad);
     dv += tv_dot(pt, &ht, a.dpt.n);
     dv = fabsf(dv);
     if (a.wpt.uids && a.wdata) {
-        eval_set<K_WP>(pt, a.wpt, g, 0, 0, 0, bad);
+        eval_set_r<K_WP>(pt, a.wpt, g, 0, 0, 0, bad);
         wv *= tv_prod(pt, a.wpt.n);
     }
     float orv = rv;
