@@ -95,6 +95,7 @@ _SIGS = {
     'gbkb200_ctx_set_stream': [c_void_p, c_void_p],
     'gbkb200_ctx_set_sync': [c_void_p, c_int],
     'gbkb200_ctx_set_mcdisk': [c_void_p, ctypes.c_ulonglong, c_int],
+    'gbkb200_ctx_reserve_scratch': [c_void_p, ctypes.c_size_t],
     'gbkb200_ctx_synchronize': [c_void_p],
     'gbkb200_fft_r2c_f32': [c_void_p, c_int3, c_void_p, c_void_p],
     'gbkb200_fft_c2r_f32': [c_void_p, c_int3, c_void_p, c_void_p],
@@ -167,6 +168,9 @@ class Context:
 
     def set_mcdisk(self, seed, mode=0):
         check(_lib.gbkb200_ctx_set_mcdisk(self.handle, int(seed), int(mode)), 'set_mcdisk')
+
+    def reserve_scratch(self, nbytes):
+        check(_lib.gbkb200_ctx_reserve_scratch(self.handle, int(nbytes)), 'reserve_scratch')
 
     def synchronize(self):
         check(_lib.gbkb200_ctx_synchronize(self.handle), 'synchronize')

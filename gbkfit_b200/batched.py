@@ -296,29 +296,60 @@ class BatchedSMDisk:
         one = {k: np.asarray(v)[None] for k, v in params.items()}
         return {k: v[0] for k, v in self.pack(one, 1).items() if v.size}
 
+    def _submit_args(self):
+        """The per-evaluator arguments of gbkb200_batch_submit (built once):
+        the pinned and device input buffers of max_sets sets and the
+        pointers of their per-name views."""
+        a = getattr(self, '_sub', None)
+        if a is not None:
+            return a
+        st = self._e2e_buffers(self.max_sets, 1)
+        hv, hflat, dflat, dv = st['pieces'][0]
+        g = lambda n: c_void_p(dv[n].data_ptr()) if n in dv else None
+        pv = (c_void_p * 9)(*[dv[k].data_ptr() if k in dv else None for k in KINDS])
+        self._sub = a = dict(hv=hv, out=st['chi2'], pv=pv, args=(
+            c_void_p(hflat.data_ptr()), c_void_p(dflat.data_ptr()),
+            ctypes.c_size_t(hflat.numel() * 4), g('vsys'), g('xpos'), g('ypos'), g('posa'),
+            g('incl'), pv, c_void_p(self.chi2.data_ptr()), c_void_p(st['chi2'].data_ptr())))
+        return a
+
     def submit_rows(self, rows):
         """Enqueue one evaluation of len(rows) parameter sets (rows from
-        pack_one) on the evaluator's stream: the rows are gathered into a
-        pinned buffer, copied to the device in one transfer, evaluated, and
-        chi^2 is copied back to pinned memory.  Returns (event, chi2 host
-        tensor view); chi2 is valid once the event has completed.  One
+        pack_one) on the evaluator's stream in one native call: the rows are
+        gathered into a pinned buffer, copied to the device in one transfer,
+        evaluated, and chi^2 is copied back to pinned memory.  Returns (done,
+        chi2 host tensor view): chi2 is valid once done.query() is true.  One
         submission may be in flight per evaluator (the next one reuses its
-        buffers): the caller waits for the event before submitting again."""
+        buffers): the caller waits for it before submitting again."""
         n = len(rows)
         if not 0 < n <= self.max_sets:
             raise ValueError(f"a group of {n} sets (max_sets {self.max_sets})")
-        st = self._e2e_buffers(self.max_sets, 1)
-        hv, hflat, dflat, dv = st['pieces'][0]
-        for name, arr in hv.items():
-            arr[:n] = np.stack([r[name] for r in rows])
-        with torch.cuda.stream(self.stream):
-            dflat.copy_(hflat, non_blocking=True)
-            self.evaluate_device(dv, n)
-            out = st['chi2'][:n]
-            out.copy_(self.chi2[:n], non_blocking=True)
-            ev = torch.cuda.Event()
-            ev.record(self.stream)
-        return ev, out
+        a = self._submit_args()
+        for name, arr in a['hv'].items():
+            if n == 1:
+                arr[0] = rows[0][name]
+            else:
+                arr[:n] = np.stack([r[name] for r in rows])
+        check(_lib.gbkb200_batch_submit(self.handle, c_int(n), *a['args']), 'batch_submit')
+        return self._done, a['out'][:n]
+
+    def submit_cubes(self, cubes, n):
+        """As submit_rows, for n model cubes already enqueued into `cubes` on
+        the evaluator's stream: the convolution, residual and sum, and chi^2
+        copied back to pinned memory.  Returns (done, chi2 host view)."""
+        if not 0 < n <= self.max_sets:
+            raise ValueError(f"a group of {n} sets (max_sets {self.max_sets})")
+        a = self._submit_args()
+        check(_lib.gbkb200_batch_submit_cubes(self.handle, c_int(n), c_void_p(cubes.data_ptr()),
+                                              a['args'][9], a['args'][10]), 'batch_submit_cubes')
+        return self._done, a['out'][:n]
+
+    @property
+    def _done(self):
+        d = getattr(self, '_done_obj', None)
+        if d is None:
+            d = self._done_obj = _Done(self)
+        return d
 
     # ---- given model cubes (direct mode) ---------------------------------------
     def window(self):
@@ -339,21 +370,6 @@ class BatchedSMDisk:
             self.handle, c_int(int(nsets)), c_void_p(cubes.data_ptr()), c_void_p(chi2.data_ptr()),
             c_void_p(model.data_ptr()) if model is not None else None), 'batch_evaluate_cubes')
         return chi2[:nsets]
-
-    def submit_cubes(self, cubes, n):
-        """As submit_rows, for n model cubes already enqueued into `cubes` on
-        the evaluator's stream: the convolution, residual and sum, and chi^2
-        copied back to pinned memory.  Returns (event, chi2 host view)."""
-        if not 0 < n <= self.max_sets:
-            raise ValueError(f"a group of {n} sets (max_sets {self.max_sets})")
-        st = self._e2e_buffers(self.max_sets, 1)
-        with torch.cuda.stream(self.stream):
-            self.evaluate_cubes_device(cubes, n)
-            out = st['chi2'][:n]
-            out.copy_(self.chi2[:n], non_blocking=True)
-            ev = torch.cuda.Event()
-            ev.record(self.stream)
-        return ev, out
 
     def capture(self, bufs, nsets):
         """Capture one evaluate_device call for nsets sets in a CUDA graph."""
@@ -403,6 +419,18 @@ class BatchedSMDisk:
             self.close()
         except Exception:
             pass
+
+
+class _Done:
+    """Completion of an evaluator's last asynchronous submission."""
+
+    def __init__(self, ev):
+        self._ev = ev
+        self._flag = c_int()
+
+    def query(self):
+        check(_lib.gbkb200_batch_query(self._ev.handle, ctypes.byref(self._flag)), 'batch_query')
+        return bool(self._flag.value)
 
 
 def synthetic_data(w, device=0, seed=None):

@@ -364,6 +364,7 @@ struct gbkb200_batch {
     int nper = 0;
     int direct = 0;
     int trim[3] = {0, 0, 0};          // direct mode: taps trimmed from each end (x, y, z)
+    cudaEvent_t done = nullptr;       // recorded at the end of an asynchronous submission
     size_t smemB = 0;
     float* mplanes = nullptr;
     int* xr = nullptr;
@@ -612,6 +613,7 @@ extern "C" int gbkb200_batch_destroy(gbkb200_batch* bt)
     cudaFree(bt->iw);
     cudaFree(bt->counters);
     for (cudaEvent_t e : bt->ev) cudaEventDestroy(e);
+    if (bt->done) cudaEventDestroy(bt->done);
     delete bt;
     return GBKB200_OK;
 }
@@ -944,6 +946,63 @@ extern "C" int gbkb200_batch_evaluate_cubes(gbkb200_batch* bt, int nsets, const 
     stage_mark(bt, 5, false);
     GBK_CUDA_TRY(cudaGetLastError());
     return gbk_finish(bt->ctx);
+}
+
+// chi^2 of nsets sets to pinned host memory and the submission's event
+static int submit_tail(gbkb200_batch* bt, int nsets, const float* chi2_dev, float* chi2_host)
+{
+    cudaStream_t st = bt->ctx->stream;
+    if (nsets > 0 && chi2_host)
+        GBK_CUDA_TRY(cudaMemcpyAsync(chi2_host, chi2_dev, (size_t)nsets * sizeof(float),
+                                     cudaMemcpyDeviceToHost, st));
+    if (!bt->done) GBK_CUDA_TRY(cudaEventCreateWithFlags(&bt->done, cudaEventDisableTiming));
+    GBK_CUDA_TRY(cudaEventRecord(bt->done, st));
+    return GBKB200_OK;
+}
+
+extern "C" int gbkb200_batch_submit(gbkb200_batch* bt, int nsets, const void* in_host,
+                                    void* in_dev, size_t in_bytes, const float* vsys,
+                                    const float* xpos, const float* ypos, const float* posa,
+                                    const float* incl, const float* const pvalues[9],
+                                    float* chi2_dev, float* chi2_host)
+{
+    if (!bt || (in_bytes > 0 && (!in_host || !in_dev))) return GBKB200_ERR_INVALID_ARG;
+    if (in_bytes > 0)
+        GBK_CUDA_TRY(cudaMemcpyAsync(in_dev, in_host, in_bytes, cudaMemcpyHostToDevice,
+                                     bt->ctx->stream));
+    int rc = gbkb200_batch_evaluate(bt, nsets, vsys, xpos, ypos, posa, incl, pvalues, chi2_dev,
+                                    nullptr);
+    if (rc) return rc;
+    return submit_tail(bt, nsets, chi2_dev, chi2_host);
+}
+
+extern "C" int gbkb200_batch_submit_cubes(gbkb200_batch* bt, int nsets, const float* cubes,
+                                          float* chi2_dev, float* chi2_host)
+{
+    int rc = gbkb200_batch_evaluate_cubes(bt, nsets, cubes, chi2_dev, nullptr);
+    if (rc) return rc;
+    return submit_tail(bt, nsets, chi2_dev, chi2_host);
+}
+
+extern "C" int gbkb200_batch_query(const gbkb200_batch* bt, int* done)
+{
+    if (!bt || !done) return GBKB200_ERR_INVALID_ARG;
+    if (!bt->done) {
+        *done = 1;
+        return GBKB200_OK;
+    }
+    const cudaError_t e = cudaEventQuery(bt->done);
+    if (e == cudaSuccess) {
+        *done = 1;
+        return GBKB200_OK;
+    }
+    if (e == cudaErrorNotReady) {
+        (void)cudaGetLastError();
+        *done = 0;
+        return GBKB200_OK;
+    }
+    GBK_CUDA_TRY(e);
+    return GBKB200_OK;
 }
 
 extern "C" int gbkb200_batch_set_timing(gbkb200_batch* bt, int enable)

@@ -78,6 +78,22 @@ extern "C" int gbkb200_ctx_set_mcdisk(gbkb200_ctx* ctx, unsigned long long seed,
     return GBKB200_OK;
 }
 
+extern "C" int gbkb200_ctx_reserve_scratch(gbkb200_ctx* ctx, size_t bytes)
+{
+    if (!ctx) return GBKB200_ERR_INVALID_ARG;
+    if (ctx->mc_scratch_bytes >= bytes) return GBKB200_OK;
+    GBK_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (ctx->mc_scratch) cudaFree(ctx->mc_scratch);
+    ctx->mc_scratch = nullptr;
+    ctx->mc_scratch_bytes = 0;
+    if (cudaMalloc(&ctx->mc_scratch, bytes) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return GBKB200_ERR_OOM;
+    }
+    ctx->mc_scratch_bytes = bytes;
+    return GBKB200_OK;
+}
+
 extern "C" int gbkb200_ctx_synchronize(gbkb200_ctx* ctx)
 {
     if (!ctx) return GBKB200_ERR_INVALID_ARG;

@@ -152,7 +152,10 @@ struct Philox {
         if (j == 0) block(k >> 2);
         const unsigned v = j == 0 ? w0 : j == 1 ? w1 : j == 2 ? w2 : w3;
         ++k;
-        return (float)(((double)(v >> 8) + 0.5) * (1.0 / 16777216.0));
+        // ((v >> 8) + 0.5) / 2^24 rounded to float: the odd integer
+        // 2 (v >> 8) + 1 < 2^25 rounded to float, times 2^-25 (exact), is the
+        // same single rounding
+        return __uint2float_rn(((v >> 8) << 1) | 1u) * 0x1p-25f;
     }
 };
 
@@ -206,10 +209,39 @@ __device__ __forceinline__ float rh_trait_rnd(Philox& rng, int uid, const float*
     }
 }
 
+// The projection values that are the same for every cloud of a call: centre
+// and systemic velocity of a disk that is not loose, angles of a disk that is
+// not tilted (evaluated once per thread, with the expressions of the
+// per-cloud path)
+struct McConst {
+    float vsys, xpos, ypos;
+    float s_i, c_i, s_p, c_p;      // sincos(-incl), sincos(-posa)
+    float sin_incl, cos_incl;
+};
+
+__device__ __forceinline__ McConst mc_const(const DiskArgs& a)
+{
+    McConst k{};
+    if (!a.loose) {
+        k.vsys = a.vsys ? a.vsys[0] : 0.f;
+        k.xpos = a.xpos[0];
+        k.ypos = a.ypos[0];
+    }
+    if (!a.tilted) {
+        const float posai = a.posa[0] * GBK_D2R, incli = a.incl[0] * GBK_D2R;
+        sincosf(-incli, &k.s_i, &k.c_i);
+        sincosf(-posai, &k.s_p, &k.c_p);
+        k.sin_incl = sinf(incli);
+        k.cos_incl = cosf(incli);
+    }
+    return k;
+}
+
 // gmodels.hpp:325-608 up to the splat: sample one cloud and return its
 // voxel and line.  false if the cloud is discarded.
-__device__ __forceinline__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m, int ci, int& xo,
-                                             int& yo, int& zo, SpaxelOut& o, int& bad)
+__device__ __forceinline__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m,
+                                             const McConst& mk, int ci, int& xo, int& yo,
+                                             int& zo, SpaxelOut& o, int& bad)
 {
     Philox rng;
     rng.ci = (unsigned)ci;
@@ -287,19 +319,26 @@ __device__ __forceinline__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m,
         const float zv = tv_sum(pt, a.zpt.n);
         zd += zv;
     }
-    float vsysi = a.vsys ? (a.loose ? lerp(rd, g.rnidx, rnodes, a.vsys, 0) : a.vsys[0]) : 0.f;
-    float xposi = a.loose ? lerp(rd, g.rnidx, rnodes, a.xpos, 0) : a.xpos[0];
-    float yposi = a.loose ? lerp(rd, g.rnidx, rnodes, a.ypos, 0) : a.ypos[0];
-    float posai = a.tilted ? lerp(rd, g.rnidx, rnodes, a.posa, 0) : a.posa[0];
-    float incli = a.tilted ? lerp(rd, g.rnidx, rnodes, a.incl, 0) : a.incl[0];
-    posai *= GBK_D2R;
-    incli *= GBK_D2R;
+    float vsysi = mk.vsys, xposi = mk.xpos, yposi = mk.ypos;
+    if (a.loose) {
+        vsysi = a.vsys ? lerp(rd, g.rnidx, rnodes, a.vsys, 0) : 0.f;
+        xposi = lerp(rd, g.rnidx, rnodes, a.xpos, 0);
+        yposi = lerp(rd, g.rnidx, rnodes, a.ypos, 0);
+    }
+    float s_i = mk.s_i, c_i = mk.c_i, s_p = mk.s_p, c_p = mk.c_p;
+    float sin_incl = mk.sin_incl, cos_incl = mk.cos_incl;
+    if (a.tilted) {
+        const float posai = lerp(rd, g.rnidx, rnodes, a.posa, 0) * GBK_D2R;
+        const float incli = lerp(rd, g.rnidx, rnodes, a.incl, 0) * GBK_D2R;
+        sincosf(-incli, &s_i, &c_i);
+        sincosf(-posai, &s_p, &c_p);
+        sin_incl = sinf(incli);
+        cos_incl = cosf(incli);
+    }
     // disk -> world (gmodels.hpp:159-165 with negated parameters, :495-496)
-    float xn = xd, yn = yd, zn = zd, s, c;
-    sincosf(-incli, &s, &c);
-    rot_lh_x(yn, zn, s, c);
-    sincosf(-posai, &s, &c);
-    rot_lh_z(xn, yn, s, c);
+    float xn = xd, yn = yd, zn = zd;
+    rot_lh_x(yn, zn, s_i, c_i);
+    rot_lh_z(xn, yn, s_p, c_p);
     xn -= -xposi;
     yn -= -yposi;
     float fx = rintf((xn - a.zx) / a.stx), fy = rintf((yn - a.zy) / a.sty);
@@ -308,7 +347,7 @@ __device__ __forceinline__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m,
     if (fx < 0 || fx >= a.sx || fy < 0 || fy >= a.sy || fz < 0 || fz >= a.sz) return false;
     int x = (int)fx, y = (int)fy, z = (int)fz;
     float vv = 0, dv = 0, wv = 1;
-    if (a.vpt.uids) eval_set_r<K_VP>(pt, a.vpt, g, sinf(incli), cosf(incli), 0, bad);
+    if (a.vpt.uids) eval_set_r<K_VP>(pt, a.vpt, g, sin_incl, cos_incl, 0, bad);
     if (a.vht.uids) eval_set_r<K_VH>(ht, a.vht, g, 0, 0, fabsf(zd), bad);
     vv += tv_dot(pt, &ht, a.vpt.n);
     vv += vsysi;
@@ -341,11 +380,12 @@ __device__ __forceinline__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m,
 __global__ void __launch_bounds__(256) mcdisk_kernel(DiskArgs a, McArgs m, int* status)
 {
     int bad = 0;
+    const McConst mk = mc_const(a);
     for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < m.nclouds;
          ci += gridDim.x * blockDim.x) {
         int x, y, z;
         SpaxelOut o;
-        if (!mcdisk_cloud(a, m, ci, x, y, z, o, bad)) continue;
+        if (!mcdisk_cloud(a, m, mk, ci, x, y, z, o, bad)) continue;
         if (a.image) atomicAdd(&a.image[x + (long long)a.sx * y], o.orv);
         int zlo, zhi;
         if (a.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
@@ -384,11 +424,12 @@ __global__ void __launch_bounds__(256) mcdisk_v4_kernel(DiskArgs a, McArgs m, fl
                                                         int nzp, int* status)
 {
     int bad = 0;
+    const McConst mk = mc_const(a);
     for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < m.nclouds;
          ci += gridDim.x * blockDim.x) {
         int x, y, z;
         SpaxelOut o;
-        if (!mcdisk_cloud(a, m, ci, x, y, z, o, bad)) continue;
+        if (!mcdisk_cloud(a, m, mk, ci, x, y, z, o, bad)) continue;
         if (a.image) atomicAdd(&a.image[x + (long long)a.sx * y], o.orv);
         int zlo, zhi;
         if (lines && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
@@ -480,12 +521,13 @@ __device__ __forceinline__ void fixed_add(long long* acc, float v, int k)
 __global__ void __launch_bounds__(256) mcdisk_bound_kernel(DiskArgs a, McArgs m, unsigned* bound)
 {
     int bad = 0;
+    const McConst mk = mc_const(a);
     for (int base = blockIdx.x * blockDim.x; base < m.nclouds; base += gridDim.x * blockDim.x) {
         const int ci = base + threadIdx.x;
         float vc = 0.f, vm = 0.f;
         int x, y, z;
         SpaxelOut o;
-        if (ci < m.nclouds && mcdisk_cloud(a, m, ci, x, y, z, o, bad)) {
+        if (ci < m.nclouds && mcdisk_cloud(a, m, mk, ci, x, y, z, o, bad)) {
             int zlo, zhi;
             if (a.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi))
                 vc = o.orv * (1 / (o.dv * sqrtf(2 * GBK_PI)));
@@ -505,12 +547,13 @@ __global__ void __launch_bounds__(256) mcdisk_fixed_kernel(DiskArgs a, McArgs m,
                                                            int* status)
 {
     int bad = 0;
+    const McConst mk = mc_const(a);
     const int kc = fixed_shift(f.bound[0], m.nclouds), km = fixed_shift(f.bound[1], m.nclouds);
     for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < m.nclouds;
          ci += gridDim.x * blockDim.x) {
         int x, y, z;
         SpaxelOut o;
-        if (!mcdisk_cloud(a, m, ci, x, y, z, o, bad)) continue;
+        if (!mcdisk_cloud(a, m, mk, ci, x, y, z, o, bad)) continue;
         const long long sp = x + (long long)a.sx * y;
         if (f.image) fixed_add(&f.image[sp], o.orv, km);
         int zlo, zhi;

@@ -128,8 +128,9 @@ class Dataset:
             # fast mode: the clouds' lines go through a channel-contiguous
             # scratch cube of the window held by the evaluator's context
             self.batched.ctx.set_mcdisk(mc_seed, 0)
-            self.footprint += (self.mc_cubes.numel() * 4 + self.mc_d.numel() +
-                               4 * wx * wy * ((wz + 3) // 4 * 4))
+            scratch = 4 * wx * wy * ((wz + 3) // 4 * 4)
+            self.batched.ctx.reserve_scratch(scratch)
+            self.footprint += self.mc_cubes.numel() * 4 + self.mc_d.numel() + scratch
 
     def request_layout(self):
         """Byte offsets of one in-flight request's device buffers (padded

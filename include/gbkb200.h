@@ -71,6 +71,9 @@ int gbkb200_ctx_set_sync(gbkb200_ctx* ctx, int sync);
  * scube (no scratch).  The assigned maps (wdata, vdata_cmp, ddata_cmp) keep
  * the reference's last-writer-wins race in every mode. */
 int gbkb200_ctx_set_mcdisk(gbkb200_ctx* ctx, unsigned long long seed, int mode);
+/* grows the context's mcdisk scratch to at least `bytes` now (a later call
+ * that needs no more allocates nothing on its stream's path) */
+int gbkb200_ctx_reserve_scratch(gbkb200_ctx* ctx, size_t bytes);
 /* waits for the context's stream, then returns the status raised by kernels
  * since the last call (GBKB200_OK, _BAD_TRAIT or _TIMEOUT) and clears it */
 int gbkb200_ctx_synchronize(gbkb200_ctx* ctx);
@@ -378,6 +381,22 @@ int gbkb200_batch_window(const gbkb200_batch* b, int offset[3], int size[3]);
  * in gbkb200_batch_evaluate (GBKB200_ERR_UNSUPPORTED in FFT mode). */
 int gbkb200_batch_evaluate_cubes(gbkb200_batch* b, int nsets, const float* cubes, float* chi2,
                                  float* model);
+/* Asynchronous submission (no reference counterpart; the serving loop's
+ * launch): copies in_bytes of packed per-set inputs from pinned host memory
+ * (in_host) to in_dev, evaluates nsets sets as gbkb200_batch_evaluate (the
+ * per-set input pointers point into in_dev), copies chi2 to chi2_host
+ * (pinned, nsets floats) and records the evaluator's completion event, all
+ * on the context's stream; gbkb200_batch_submit_cubes does the same for
+ * given model cubes (gbkb200_batch_evaluate_cubes).  gbkb200_batch_query
+ * sets *done to 1 once the last submission has completed (chi2_host is then
+ * valid), else 0; one submission may be in flight per evaluator. */
+int gbkb200_batch_submit(gbkb200_batch* b, int nsets, const void* in_host, void* in_dev,
+                         size_t in_bytes, const float* vsys, const float* xpos, const float* ypos,
+                         const float* posa, const float* incl, const float* const pvalues[9],
+                         float* chi2_dev, float* chi2_host);
+int gbkb200_batch_submit_cubes(gbkb200_batch* b, int nsets, const float* cubes, float* chi2_dev,
+                               float* chi2_host);
+int gbkb200_batch_query(const gbkb200_batch* b, int* done);
 /* the chosen FFT grid, chunk, the device bytes the evaluator holds (its
  * work space, tables and partials) and the convolution mode (1 = FFT,
  * 2 = direct) */
