@@ -96,6 +96,7 @@ _SIGS = {
     'gbkb200_ctx_set_sync': [c_void_p, c_int],
     'gbkb200_ctx_set_mcdisk': [c_void_p, ctypes.c_ulonglong, c_int],
     'gbkb200_ctx_reserve_scratch': [c_void_p, ctypes.c_size_t],
+    'gbkb200_mcdisk_scratch_bytes': [c_int, c_int, c_int, c_int],
     'gbkb200_ctx_synchronize': [c_void_p],
     'gbkb200_fft_r2c_f32': [c_void_p, c_int3, c_void_p, c_void_p],
     'gbkb200_fft_c2r_f32': [c_void_p, c_int3, c_void_p, c_void_p],
@@ -127,6 +128,7 @@ for _name, _args in _SIGS.items():
     _f = getattr(_lib, _name)
     _f.argtypes = _args
     _f.restype = c_int
+_lib.gbkb200_mcdisk_scratch_bytes.restype = ctypes.c_size_t
 _lib.gbkb200_error_string.argtypes = [c_int]
 _lib.gbkb200_error_string.restype = ctypes.c_char_p
 _lib.gbkb200_last_cuda_error.argtypes = []

@@ -421,8 +421,12 @@ __global__ void __launch_bounds__(256) mcdisk_kernel(DiskArgs a, McArgs m, int* 
 // the scratch cube to scube in the reference's (channel, y, x) layout.  The
 // other outputs are accumulated as in mode 0.
 __global__ void __launch_bounds__(256) mcdisk_v4_kernel(DiskArgs a, McArgs m, float* lines,
-                                                        int nzp, int* status)
+                                                        int nzp, int copies, int* status)
 {
+    // block b adds into copy b % copies of the scratch cube (copies of nsp x
+    // nzp floats): reductions to the same element from many blocks spread
+    // over the copies' L2 lines
+    if (lines) lines += (long long)(blockIdx.x % copies) * a.sx * a.sy * nzp;
     int bad = 0;
     const McConst mk = mc_const(a);
     for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < m.nclouds;
@@ -460,20 +464,26 @@ __global__ void __launch_bounds__(256) mcdisk_v4_kernel(DiskArgs a, McArgs m, fl
     if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
 }
 
-// scube[z][s] += lines[s][z] for spaxels s < nsp, channels z < nz (32 x 32 tiles)
+// scube[z][s] += sum over the copies c of lines[c][s][z] (in copy order) for
+// spaxels s < nsp, channels z < nz (32 x 32 tiles)
 __global__ void __launch_bounds__(256) mc_lines_add_kernel(const float* __restrict__ lines,
                                                            float* __restrict__ scube,
-                                                           long long nsp, int nzp, int nz)
+                                                           long long nsp, int nzp, int nz,
+                                                           int copies)
 {
     __shared__ float tile[32][33];
     const long long s0 = (long long)blockIdx.x * 32;
     const int z0 = blockIdx.y * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const long long cstride = nsp * nzp;
 #pragma unroll
     for (int k = 0; k < 32; k += 8) {
         const long long s = s0 + ty + k;
         const int z = z0 + tx;
-        tile[ty + k][tx] = (s < nsp && z < nz) ? lines[s * nzp + z] : 0.f;
+        float v = 0.f;
+        if (s < nsp && z < nz)
+            for (int c = 0; c < copies; ++c) v += lines[c * cstride + s * nzp + z];
+        tile[ty + k][tx] = v;
     }
     __syncthreads();
 #pragma unroll
@@ -482,6 +492,27 @@ __global__ void __launch_bounds__(256) mc_lines_add_kernel(const float* __restri
         const long long s = s0 + tx;
         if (s < nsp && z < nz) scube[(long long)z * nsp + s] += tile[tx][ty + k];
     }
+}
+
+// Copies of the channel-contiguous line scratch for a call: 1 up to 256
+// clouds per spaxel, doubling per doubling of the density up to 8, and no
+// more than fit in 64 MB (reductions to one element from many blocks queue
+// in its L2 slice; small cubes with many clouds are where that happens)
+static int mc_line_copies(long long nclouds, long long nsp, int nzp)
+{
+    const long long per = nclouds / (nsp > 0 ? nsp : 1);
+    int c = per < 256 ? 1 : per < 512 ? 2 : per < 1024 ? 4 : 8;
+    const long long one = nsp * nzp * (long long)sizeof(float);
+    while (c > 1 && c * one > (64LL << 20)) c >>= 1;
+    return c;
+}
+
+extern "C" size_t gbkb200_mcdisk_scratch_bytes(int nclouds, int spat_size_x, int spat_size_y,
+                                               int spec_size)
+{
+    const long long nsp = (long long)spat_size_x * spat_size_y;
+    const int nzp = (spec_size + 3) & ~3;
+    return (size_t)mc_line_copies(nclouds, nsp, nzp) * nsp * nzp * sizeof(float);
 }
 
 // ---- deterministic mcdisk: 64-bit fixed-point accumulation ------------------
@@ -715,10 +746,11 @@ extern "C" int gbkb200_gmodel_mcdisk_evaluate_f32(gbkb200_ctx* ctx, float cflux,
     // one atomic per channel if the scratch cannot be had); mode 3 and the
     // other outputs: one fp32 atomic per channel and element
     bool vec = (ctx->mc_mode == 0 || ctx->mc_mode == 2) && a.scube;
+    const int copies = mc_line_copies(nclouds, (long long)a.sx * a.sy, (a.spec_size + 3) & ~3);
     if (vec) {
         const long long nsp = (long long)a.sx * a.sy;
         const int nzp = (a.spec_size + 3) & ~3;
-        const size_t need = (size_t)nsp * nzp * sizeof(float);
+        const size_t need = (size_t)copies * nsp * nzp * sizeof(float);
         if (ctx->mc_scratch_bytes < need) {
             if (ctx->mc_scratch) cudaFree(ctx->mc_scratch);
             ctx->mc_scratch = nullptr;
@@ -740,12 +772,14 @@ extern "C" int gbkb200_gmodel_mcdisk_evaluate_f32(gbkb200_ctx* ctx, float cflux,
     if (vec) {
         const long long nsp = (long long)a.sx * a.sy;
         const int nzp = (a.spec_size + 3) & ~3;
-        const size_t need = (size_t)nsp * nzp * sizeof(float);
+        const size_t need = (size_t)copies * nsp * nzp * sizeof(float);
         float* lines = static_cast<float*>(ctx->mc_scratch);
         GBK_CUDA_TRY(cudaMemsetAsync(lines, 0, need, ctx->stream));
-        mcdisk_v4_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, lines, nzp, ctx->d_status);
+        mcdisk_v4_kernel<<<blocks, 256, 0, ctx->stream>>>(a, m, lines, nzp, copies,
+                                                          ctx->d_status);
         const dim3 tg((unsigned)((nsp + 31) / 32), (unsigned)((a.spec_size + 31) / 32));
-        mc_lines_add_kernel<<<tg, 256, 0, ctx->stream>>>(lines, a.scube, nsp, nzp, a.spec_size);
+        mc_lines_add_kernel<<<tg, 256, 0, ctx->stream>>>(lines, a.scube, nsp, nzp, a.spec_size,
+                                                         copies);
         GBK_CUDA_TRY(cudaGetLastError());
         return gbk_finish(ctx);
     }

@@ -128,7 +128,8 @@ class Dataset:
             # fast mode: the clouds' lines go through a channel-contiguous
             # scratch cube of the window held by the evaluator's context
             self.batched.ctx.set_mcdisk(mc_seed, 0)
-            scratch = 4 * wx * wy * ((wz + 3) // 4 * 4)
+            # the fast mode's line scratch at its largest (densest clouds)
+            scratch = int(_lib.gbkb200_mcdisk_scratch_bytes(2 ** 31 - 1, wx, wy, wz))
             self.batched.ctx.reserve_scratch(scratch)
             self.footprint += self.mc_cubes.numel() * 4 + self.mc_d.numel() + scratch
 

@@ -59,8 +59,9 @@ int gbkb200_ctx_set_sync(gbkb200_ctx* ctx, int sync);
 /* seed of the counter-based cloud generator of mcdisk_evaluate and its
  * accumulation mode.  Mode 0 = fast (the default; fp32 atomics, sums depend
  * on the order clouds land in, in the last bits): the lines are accumulated
- * channel-contiguous in a scratch cube held by the context (4 bytes per
- * scube element) with 16-byte vector atomics, then added to scube; when that
+ * channel-contiguous in scratch cubes held by the context (1 to 8 copies of
+ * 4 bytes per scube element, gbkb200_mcdisk_scratch_bytes; each block adds
+ * into one copy) with 16-byte vector atomics, then added to scube; when that
  * scratch cannot be allocated, as mode 3.  Mode 1 = deterministic: the
  * accumulated outputs (scube, image, rdata, ordata and their _cmp forms) are
  * summed in 64-bit fixed point, bit-identical run to run and exact to
@@ -74,6 +75,12 @@ int gbkb200_ctx_set_mcdisk(gbkb200_ctx* ctx, unsigned long long seed, int mode);
 /* grows the context's mcdisk scratch to at least `bytes` now (a later call
  * that needs no more allocates nothing on its stream's path) */
 int gbkb200_ctx_reserve_scratch(gbkb200_ctx* ctx, size_t bytes);
+/* the scratch bytes the fast mcdisk modes use for a call of nclouds clouds
+ * on a spat_size_x x spat_size_y x spec_size spectral cube: copies of the
+ * channel-contiguous line cube (1 to 8, more for denser clouds, at most
+ * 64 MB of copies) */
+size_t gbkb200_mcdisk_scratch_bytes(int nclouds, int spat_size_x, int spat_size_y,
+                                    int spec_size);
 /* waits for the context's stream, then returns the status raised by kernels
  * since the last call (GBKB200_OK, _BAD_TRAIT or _TIMEOUT) and clears it */
 int gbkb200_ctx_synchronize(gbkb200_ctx* ctx);

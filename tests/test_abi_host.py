@@ -230,3 +230,18 @@ def test_imaging_model_parameter_names():
     assert o3[0].disk().tables['rpt']['uids'][0] == T.OPT_OFFSET + T.RPT['exponential']
     assert DModelImage((30, 20)).size() == (30, 20) and DModelImage((30, 20)).keys() == ['image']
     assert DModelLSlit((30, 40)).size() == (30, 1, 40)
+
+
+def test_mcdisk_scratch_copies_rule():
+    """The fast mcdisk modes' line scratch: one channel-contiguous copy up to
+    256 clouds per spaxel, 2/4/8 copies at 256/512/1024 and more, within
+    64 MB of copies."""
+    from gbkfit_b200 import _native
+    f = _native.lib().gbkb200_mcdisk_scratch_bytes
+    one = lambda sx, sy, nz: sx * sy * ((nz + 3) // 4 * 4) * 4
+    assert f(100_000, 65, 68, 47) == one(65, 68, 47)
+    assert f(10_000_000, 65, 68, 47) == 8 * one(65, 68, 47)
+    assert f(10_000_000, 244, 262, 80) == one(244, 262, 80)          # 156 per spaxel
+    assert f(3_000_000, 89, 142, 48) == one(89, 142, 48)              # 237 per spaxel
+    assert f(5_000_000, 89, 142, 48) == 2 * one(89, 142, 48)          # 396
+    assert f(2 ** 31 - 1, 320, 320, 160) == one(320, 320, 160)        # 62.5 MB: one copy fits
