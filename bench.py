@@ -423,7 +423,7 @@ def run_b200(args):
     return out
 
 
-def serving_run(nrequests=10000, slots=8, load=0.8, batch_sets=16):
+def serving_run(nrequests=10000, slots=8, load=0.8, batch_sets=32, mc_sets=8):
     """The serving stream (workloads.serving_stream: 64 datasets, 70 % smdisk /
     30 % mcdisk, sides 32-256 px, 32-192 channels, 1e5-1e7 clouds): capacity
     with every request submitted at once, then Poisson arrivals at `load` x
@@ -431,7 +431,8 @@ def serving_run(nrequests=10000, slots=8, load=0.8, batch_sets=16):
     packing of the request's parameters (in submit).  Every dataset is
     registered with its smdisk disk, so its smdisk requests are coalesced
     into batched launches (direct separable convolution, up to batch_sets
-    sets each)."""
+    sets each) and its mcdisk requests into launches of up to mc_sets
+    cloud cubes on the evaluator's window (the same direct convolution)."""
     import torch
     from gbkfit_b200 import workloads
     from gbkfit_b200.serving import ModelServer, Request
@@ -444,7 +445,7 @@ def serving_run(nrequests=10000, slots=8, load=0.8, batch_sets=16):
     with ModelServer(slots=slots, hbm_budget=40 << 30) as srv:
         for d in st.datasets:
             srv.register(d['key'], d['geom'], d['data'], d['error'], smdisk=d['smdisk'],
-                         batch_sets=batch_sets)
+                         batch_sets=batch_sets, mc_sets=mc_sets)
         [f.result() for f in [srv.submit(r) for r in reqs()[:300]]]     # plans, allocator
         srv.stats(reset=True)
         [f.result() for f in [srv.submit(r) for r in reqs()]]
@@ -463,7 +464,7 @@ def serving_run(nrequests=10000, slots=8, load=0.8, batch_sets=16):
         [f.result() for f in futs]
         s = srv.stats(reset=True)
         resident = srv._resident
-    return dict(requests=nrequests, slots=slots, batch_sets=batch_sets,
+    return dict(requests=nrequests, slots=slots, batch_sets=batch_sets, mc_sets=mc_sets,
                 max_group=s.get('max_group'), capacity_evals_per_s=round(cap, 1),
                 offered_evals_per_s=round(rate, 1), evals_per_s=round(s['evals_per_s'], 1),
                 p50_ms=round(s['p50_ms'], 3), p99_ms=round(s['p99_ms'], 3),
