@@ -675,6 +675,146 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     }
 }
 
+// ka_lines_lsf on two 32-column chunks per warp: lane l evaluates columns
+// 64 q + l and 64 q + 32 + l (chunks 2 q and 2 q + 1) and runs both LSF FIRs
+// as packed FP32 pairs (FFMA2: two lanes of fma, each rounded as fmaf, so
+// every value is the one ka_lines_lsf computes); each chunk keeps its own
+// range-table entries.  Half the multiply-add instructions per spaxel.
+template<int KZ>
+__global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 5 : 4)) ka_lines_lsf2(BatchKernelArgs P, int* status)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int npair = (P.nch + 1) >> 1;
+    const int item = blockIdx.x * (KA_THREADS / 32) + warp;
+    if (item >= P.Wy * npair) return;                    // whole warp
+    const int y = item / npair, c0 = 2 * (item % npair), c1 = c0 + 1;
+    const bool has1 = c1 < P.nch;                        // warp-uniform
+    const int c = blockIdx.y, b = P.set0 + c;
+    const DiskArgs a = set_disk(P, b);
+    const DiskConst kc = disk_const(a);
+    int bad = 0;
+    float amp[2], rinv[2], vv[2];
+    int lo[2], hi[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int x = (c0 + h) * 32 + lane;
+        SpaxelOut o{};
+        lo[h] = INT_MAX;
+        hi[h] = -1;
+        amp[h] = 0.f;
+        rinv[h] = 0.f;
+        const bool on = x < P.Wx && (P.nwfast ? smdisk_spaxel_nw(a, kc, x, y, o)
+                                               : smdisk_spaxel(a, kc, x, y, 0, o, bad));
+        if (on && line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo[h], hi[h])) {
+            amp[h] = o.orv * (1 / (o.dv * sqrtf(2 * GBK_PI)));
+            rinv[h] = 1.4426950408889634f / (2 * o.dv * o.dv);
+        } else {
+            lo[h] = INT_MAX;
+            hi[h] = -1;
+        }
+        vv[h] = o.vv;
+    }
+    const float z0 = a.spec_zero, dz = a.spec_step;
+    const unsigned wlen0 = (unsigned)hi[0] - (unsigned)lo[0];
+    const unsigned wlen1 = (unsigned)hi[1] - (unsigned)lo[1];
+    // the lines of both columns at window channel z (as line_f of ka_lines_lsf)
+    auto line2 = [&](int z, float zf) {
+        const float zv = z0 + zf * dz;
+        const float d0 = zv - vv[0], d1 = zv - vv[1];
+        float e0, e1;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e0) : "f"(-(d0 * d0) * rinv[0]));
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e1) : "f"(-(d1 * d1) * rinv[1]));
+        return make_float2((unsigned)z - (unsigned)lo[0] <= wlen0 ? amp[0] * e0 : 0.f,
+                           (unsigned)z - (unsigned)lo[1] <= wlen1 ? amp[1] * e1 : 0.f);
+    };
+    int olo[2], ohi[2];
+    unsigned olen[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const bool lit = lo[h] <= hi[h];
+        olo[h] = lit ? max(0, lo[h] - KZ + 1) : INT_MAX;
+        ohi[h] = lit ? min(P.Nz - 1, hi[h]) : -1;
+        olen[h] = lit ? (unsigned)(ohi[h] - olo[h]) : 0u;
+    }
+    int zlo = min(olo[0], olo[1]), zhi = max(ohi[0], ohi[1]);
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, s));
+        zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, s));
+    }
+    int* xr0 = P.xr + (((long long)c * P.Wy + y) * P.nch + c0) * P.Nz;
+    int* xr1 = xr0 + P.Nz;                                // chunk c1 (used when has1)
+    for (int zo = lane; zo < P.Nz; zo += 32)
+        if (zo < zlo || zo > zhi) {
+            xr0[zo] = -1;
+            if (has1) xr1[zo] = -1;
+        }
+    if (zlo <= zhi) {
+        float2 lz[KZ];
+#pragma unroll
+        for (int t = 0; t < KZ; ++t) lz[t] = make_float2(P.lsfr[t], P.lsfr[t]);
+        float2 w[KZ];
+#pragma unroll
+        for (int t = 0; t < KZ - 1; ++t) w[t] = line2(zlo + t, (float)(zlo + t));
+        const long long zstride = (long long)P.Wy * P.pitch;
+        float* dp = P.mplanes + ((long long)c * P.Nz * P.Wy + y) * P.pitch + c0 * 32 + lane +
+                    zlo * zstride;
+        unsigned mm0 = 0u, mm1 = 0u;
+        int mz = zlo, own = zlo + lane, fl = min(zlo + 31, zhi);
+        float zf = (float)(zlo + KZ - 1);
+        for (int zb = zlo; zb <= zhi; zb += KZ) {
+#pragma unroll
+            for (int k = 0; k < KZ; ++k) {
+                const int zo = zb + k;
+                if (zo > zhi) break;
+                w[(k + KZ - 1) % KZ] = line2(zo + KZ - 1, zf);
+                zf += 1.f;
+                float2 acc0 = make_float2(0.f, 0.f), acc1 = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int t = 0; t < KZ; t += 2) acc0 = __ffma2_rn(lz[t], w[(k + t) % KZ], acc0);
+#pragma unroll
+                for (int t = 1; t < KZ; t += 2) acc1 = __ffma2_rn(lz[t], w[(k + t) % KZ], acc1);
+                const float2 r = __fadd2_rn(acc0, acc1);
+                dp[0] = r.x;
+                if (has1) dp[32] = r.y;
+                dp += zstride;
+                const unsigned m0 = __ballot_sync(0xffffffffu,
+                                                  (unsigned)zo - (unsigned)olo[0] <= olen[0]);
+                const unsigned m1 = __ballot_sync(0xffffffffu,
+                                                  (unsigned)zo - (unsigned)olo[1] <= olen[1]);
+                if (zo == own) {
+                    mm0 = m0;
+                    mm1 = m1;
+                }
+                if (zo == fl) {
+                    if (own <= zo) {
+                        xr0[own] = mm0 ? ((c0 * 32 + __ffs(mm0) - 1) |
+                                          ((c0 * 32 + 31 - __clz(mm0)) << 16))
+                                       : -1;
+                        if (has1)
+                            xr1[own] = mm1 ? ((c1 * 32 + __ffs(mm1) - 1) |
+                                              ((c1 * 32 + 31 - __clz(mm1)) << 16))
+                                           : -1;
+                    }
+                    mz = zo + 1;
+                    own = mz + lane;
+                    fl = min(mz + 31, zhi);
+                }
+            }
+        }
+    }
+    if (P.counters && lane == 0) {
+        const unsigned long long nc = has1 ? 2 : 1;
+        atomicAdd(&P.counters[GBK_CTR_KA_SPAXEL], 32ull * nc);
+        if (zlo <= zhi) {
+            const unsigned long long n = (unsigned long long)(zhi - zlo + 1) * 32 * nc;
+            atomicAdd(&P.counters[GBK_CTR_KA_FMA], n * KZ);
+            atomicAdd(&P.counters[GBK_CTR_KA_LINE], n + (KZ - 1) * 32ull * nc);
+        }
+    }
+    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
+}
+
 // The LSF FIR of given model cubes (any gmodel's output on the evaluation
 // window, e.g. mcdisk's clouds) into the PSF kernel's input: the same
 // planes and range table as ka_lines_lsf, so that the PSF FIR, residual and
@@ -746,6 +886,8 @@ static_assert(KA_KMAX <= 33 && KB_KMAX <= 33, "coefficient arrays of BatchKernel
 // fill t[Kz / 2] (model kernel) and t[(K - KB_KMIN) / 2] (PSF kernel)
 void ka_register_short(KaFn* t);
 void ka_register_long(KaFn* t);
+// t[Kz / 2]: the two-chunk model kernel (ka_lines_lsf2)
+void ka2_register(KaFn* t);
 // t[Kz / 2]: the LSF FIR of given model cubes
 typedef void (*KcFn)(BatchKernelArgs, const float*);
 void kc_register(KcFn* t);

@@ -367,6 +367,8 @@ typedef struct {
                              * (0-2: 4, 3-5: 5) x epilogue (variant % 3: 0 residual pass,
                              * 1 residual in the y-FIR items, 2 as 1 with the data
                              * prefetched); 0 = the first */
+    int model_pairs;        /* direct mode: 1 = the model kernel runs two 32-column chunks
+                             * per warp as packed FP32 pairs (same values), 0 = one */
 } gbkb200_batch_desc;
 
 int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);

@@ -276,3 +276,37 @@ def test_batched_cubes_match_disk_path(gpu):
     assert abs(z - np.sum(d * d)) <= 1e-5 * np.sum(d * d)
     assert float(m_cube[0].abs().max()) == 0.0
     ev.close()
+
+
+@pytest.mark.parametrize('nodewise', [True, False])
+def test_batched_model_pairs_identical(gpu, nodewise):
+    """The model kernel on two 32-column chunks per warp (packed FP32 pairs,
+    each lane rounded as fmaf) gives bit-identical chi^2 and models, with an
+    odd number of chunks (the last warp's second chunk is absent) and on the
+    generic trait path."""
+    import torch
+    from gbkfit_b200 import traits as T
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    from gbkfit_b200.disk import Disk
+    n = 6
+    w = _small_batch_workload(n)
+    if not nodewise:
+        w.disk = Disk(False, False, w.disk.rnodes, traits=dict(
+            rpt=[T.bpt('nw_uniform')], vpt=[T.vpt('nw_tan_uniform')], dpt=[T.dpt('nw_uniform')],
+            spt=[T.spt('azrange')]))
+        w.params = dict(w.params, spt_p=np.full(n, 30.0), spt_s=np.full(n, 300.0))
+    data, err, _ = synthetic_data(w)
+    out = []
+    for pairs in (0, 1):
+        ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=n, chunk=4, conv='direct',
+                           model_pairs=pairs)
+        bufs = ev.alloc_inputs(n)
+        ev.upload(ev.pack(w.params, n), bufs, n)
+        model = torch.zeros((n,) + tuple(w.geom.size[::-1]), device='cuda')
+        chi2 = ev.evaluate_device(bufs, n, model=model).cpu().numpy().copy()
+        out.append((chi2, model.cpu().numpy()))
+        ev.close()
+    nch = -(-(w.geom.size[0] + 16) // 32)
+    assert nch % 2 == 1
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert np.all(out[0][0] > 0)
