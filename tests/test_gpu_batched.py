@@ -295,6 +295,7 @@ def test_batched_model_pairs_identical(gpu, nodewise):
             rpt=[T.bpt('nw_uniform')], vpt=[T.vpt('nw_tan_uniform')], dpt=[T.dpt('nw_uniform')],
             spt=[T.spt('azrange')]))
         w.params = dict(w.params, spt_p=np.full(n, 30.0), spt_s=np.full(n, 300.0))
+        w.extra = dict(w.extra, truth=dict(w.extra['truth'], spt_p=30.0, spt_s=300.0))
     data, err, _ = synthetic_data(w)
     out = []
     for pairs in (0, 1):
