@@ -234,19 +234,24 @@ class BatchedSMDisk:
               'gbkb200_batch_evaluate')
         return chi2[:nsets]
 
-    def evaluate(self, params, nsets):
+    def evaluate(self, params, nsets, pieces=None):
         """Host parameters -> host chi^2 (numpy), end to end.
 
-        The batch is split into pieces (whole chunks); each piece is packed
-        into its own pinned host buffer, copied to the device in one
-        transfer and evaluated asynchronously while the next piece is
-        packed; chi^2 comes back through a pinned buffer and the call
-        synchronises once."""
+        The batch is split into pieces; each piece is packed into its own
+        pinned host buffer, copied to the device in one transfer and
+        evaluated asynchronously while the next piece is packed; chi^2 comes
+        back through a pinned buffer and the call synchronises once.
+        pieces: how many (default: whole chunks, up to 4); a piece smaller
+        than the chunk is evaluated as a smaller wave."""
         nsets = int(nsets)
         if nsets > self.max_sets:
             raise ValueError(f"nsets {nsets} > max_sets {self.max_sets}")
-        piece = max(self.chunk, -(-nsets // 4))
-        piece = -(-piece // self.chunk) * self.chunk
+        if pieces:
+            piece = max(1, -(-nsets // int(pieces)))
+            piece = min(self.max_sets, -(-piece // 32) * 32)
+        else:
+            piece = max(self.chunk, -(-nsets // 4))
+            piece = -(-piece // self.chunk) * self.chunk
         st = self._e2e_buffers(piece, -(-nsets // piece))
         per_set = {k: (np.ndim(v) > 0 and np.shape(v)[0] == nsets) for k, v in params.items()}
         self.last_h2d_bytes = 0
