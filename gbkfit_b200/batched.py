@@ -241,17 +241,16 @@ class BatchedSMDisk:
         pinned host buffer, copied to the device in one transfer and
         evaluated asynchronously while the next piece is packed; chi^2 comes
         back through a pinned buffer and the call synchronises once.
-        pieces: how many (default: whole chunks, up to 4); a piece smaller
-        than the chunk is evaluated as a smaller wave."""
+        pieces: how many (default: two for 256 sets or more, else one; the
+        second piece's packing overlaps the first's evaluation); a piece
+        smaller than the chunk is evaluated as a smaller wave."""
         nsets = int(nsets)
         if nsets > self.max_sets:
             raise ValueError(f"nsets {nsets} > max_sets {self.max_sets}")
-        if pieces:
-            piece = max(1, -(-nsets // int(pieces)))
-            piece = min(self.max_sets, -(-piece // 32) * 32)
-        else:
-            piece = max(self.chunk, -(-nsets // 4))
-            piece = -(-piece // self.chunk) * self.chunk
+        if pieces is None:
+            pieces = 2 if nsets >= 256 else 1
+        piece = max(1, -(-nsets // int(pieces)))
+        piece = min(self.max_sets, -(-piece // 32) * 32)
         st = self._e2e_buffers(piece, -(-nsets // piece))
         per_set = {k: (np.ndim(v) > 0 and np.shape(v)[0] == nsets) for k, v in params.items()}
         self.last_h2d_bytes = 0
