@@ -156,11 +156,11 @@ __global__ void __launch_bounds__(FFT_THREADS) x_c2r_kernel(const float2* in, fl
 
 // ---- y / z axes: strided columns -------------------------------------------------
 // Column (o, i) of the complex cube: element k at o * so + i + k * sk, for
-// i in [0, inner).  A block holds 16 adjacent columns.  mode 0: one transform
-// (dir inv); mode 1: forward, multiply by spec (same layout) times scale,
-// inverse.
-constexpr int LT = 16;
-
+// i in [0, inner).  A block holds LT adjacent columns (16, or 8 for long
+// lines, whose 16-column blocks would leave two resident blocks per SM).
+// mode 0: one transform (dir inv); mode 1: forward, multiply by spec (same
+// layout) times scale, inverse.
+template<int LT>
 __global__ void __launch_bounds__(FFT_THREADS) lines_kernel(float2* data, int inner, long long so,
                                                             long long sk, AxisDev ax, int inv,
                                                             int mode, const float2* spec,
@@ -275,7 +275,9 @@ static int make_axis(Axis& a, int n)
     return GBKB200_OK;
 }
 
-static size_t lines_smem(int n) { return (size_t)(2 * LT * n + n) * sizeof(float2); }
+static size_t lines_smem(int n, int lt) { return (size_t)(2 * lt * n + n) * sizeof(float2); }
+// columns per lines_kernel block: 16 while a block needs at most 60 KB
+static int lines_tile(int n) { return lines_smem(n, 16) <= 60 * 1024 ? 16 : 8; }
 static size_t rows_smem(int M, int nx)
 {
     int L = std::max(1, std::min(16, 8192 / M));
@@ -291,8 +293,8 @@ static int get_plan(FftState* st, const Size3& s, Plan** out)
     p.nx = s[0]; p.ny = s[1]; p.nz = s[2]; p.hx = p.nx / 2 + 1;
     if (p.nx < 1 || p.ny < 1 || p.nz < 1) return GBKB200_ERR_INVALID_ARG;
     const int M = (p.nx % 2 == 0 && p.nx > 1) ? p.nx / 2 : p.nx;
-    if (rows_smem(M, p.nx) > SMEM_LIMIT || lines_smem(p.ny) > SMEM_LIMIT ||
-        lines_smem(p.nz) > SMEM_LIMIT)
+    if (rows_smem(M, p.nx) > SMEM_LIMIT || lines_smem(p.ny, lines_tile(p.ny)) > SMEM_LIMIT ||
+        lines_smem(p.nz, lines_tile(p.nz)) > SMEM_LIMIT)
         return GBKB200_ERR_UNSUPPORTED;
     int rc;
     if ((rc = make_axis(p.ax, M))) return rc;
@@ -352,16 +354,18 @@ static int launch_lines(const Plan& p, float2* data, int axis, int inv, int mode
 {
     const Axis& a = axis == 1 ? p.ay : p.az;
     if (a.dev.n == 1 && mode == 0) return GBKB200_OK;
-    const int tiles = (p.hx + LT - 1) / LT;
+    const int lt = lines_tile(a.dev.n);
+    const int tiles = (p.hx + lt - 1) / lt;
     long long so, sk;
     int outer;
     if (axis == 1) { outer = p.nz; so = (long long)p.ny * p.hx; sk = p.hx; }
     else { outer = p.ny; so = p.hx; sk = (long long)p.ny * p.hx; }
-    size_t smem = lines_smem(a.dev.n);
-    int rc = set_smem((const void*)lines_kernel, smem);
+    size_t smem = lines_smem(a.dev.n, lt);
+    auto kern = lt == 16 ? lines_kernel<16> : lines_kernel<8>;
+    int rc = set_smem((const void*)kern, smem);
     if (rc) return rc;
-    lines_kernel<<<outer * tiles, FFT_THREADS, smem, st>>>(data, p.hx, so, sk, a.dev, inv, mode,
-                                                           spec, scale);
+    kern<<<outer * tiles, FFT_THREADS, smem, st>>>(data, p.hx, so, sk, a.dev, inv, mode, spec,
+                                                   scale);
     GBK_CUDA_TRY(cudaGetLastError());
     return GBKB200_OK;
 }
