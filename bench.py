@@ -331,8 +331,8 @@ def run_b200(args):
         cfg['band'] = args.band
     if args.psf_variant >= 0:
         cfg['psf_variant'] = args.psf_variant
-    if args.model_pairs >= 0:
-        cfg['model_pairs'] = args.model_pairs
+    if args.model_variant >= 0:
+        cfg['model_variant'] = args.model_variant
     ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=nsets, device=local, **cfg)
     bufs = ev.alloc_inputs(nsets)
     ev.upload(ev.pack(mine, nsets), bufs, nsets)
@@ -922,8 +922,9 @@ def main():
     ap.add_argument('--chunk', type=int, default=0, help='force the sets per wave (default: tuned)')
     ap.add_argument('--psf-variant', type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5],
                     help='PSF kernel variant of the direct mode (default: tuned)')
-    ap.add_argument('--model-pairs', type=int, default=-1, choices=[-1, 0, 1],
-                    help='model kernel on two 32-column chunks per warp (default: tuned)')
+    ap.add_argument('--model-variant', type=int, default=-1, choices=[-1, 0, 1, 2],
+                    help='model kernel of the direct mode: 0 union loop, 1 chunk pairs, '
+                         '2 own windows (default: tuned)')
     ap.add_argument('--band', type=int, default=0,
                     help='force the output rows per PSF block of the direct mode (default: tuned)')
     ap.add_argument('--workload', default='smdisk_batch128',

@@ -11,8 +11,10 @@ Knobs (all change speed only, never results beyond fp32 rounding):
 * ``psf_variant``: PSF kernel sized for 4 or 5 resident blocks per SM, with
   its residual in a separate pass or in the y-FIR items (data loaded after or
   before each item's FIR);
-* ``model_pairs``: the direct mode's model kernel on one or two 32-column
-  chunks per warp (two: packed FP32 pairs, the same values);
+* ``model_variant``: the direct mode's model kernel (0: every lane through
+  the union of its warp's channel windows; 1: two 32-column chunks per warp
+  on packed FP32 pairs; 2: every lane through its own window into a
+  shared-memory tile; the same values);
 * ``rows_k1``: spectral rows per shared-memory group of the model kernel.
 
 Coordinate descent from the defaults; every trial builds an evaluator and
@@ -102,7 +104,7 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
             return dict(fft_size=tuple(c['fft_size']), chunk=c['chunk'], rows_k1=c['rows_k1'],
                         conv=c['conv'], band=c.get('band', 0),
                         psf_variant=c.get('psf_variant', 0),
-                        model_pairs=c.get('model_pairs', 0))
+                        model_variant=c.get('model_variant', 0))
     g = w.geom
     t_end = time.time() + budget_s
     # direct separable convolution (when the PSF is rank 1): chunk, then band
@@ -127,11 +129,13 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
             t = time_config(w, data, err, nsets, cfg)
             if t < best_dt:
                 best_d, best_dt = cfg, t
-        # the model kernel on chunk pairs
-        cfg = dict(best_d, model_pairs=1)
-        t = time_config(w, data, err, nsets, cfg)
-        if t < best_dt:
-            best_d, best_dt = cfg, t
+        # the model kernel's variants
+        base = dict(best_d)
+        for mv in (1, 2):
+            cfg = dict(base, model_variant=mv)
+            t = time_config(w, data, err, nsets, cfg)
+            if t < best_dt:
+                best_d, best_dt = cfg, t
     win = [g.size[i] + g.kernel_size[i] - 1 for i in range(3)]
     cand = [smooth_sizes(win[0], even=True), smooth_sizes(win[1]), smooth_sizes(win[2])]
     best = dict(fft_size=(cand[0][0], cand[1][0], cand[2][0]), chunk=8, rows_k1=16, conv='fft',

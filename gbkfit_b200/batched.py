@@ -38,7 +38,7 @@ class BatchDesc(ctypes.Structure):
         ('max_sets', c_int), ('chunk', c_int), ('rows_k1', c_int), ('rows_k5', c_int),
         ('conv_mode', c_int), ('psf_rank', c_int),
         ('psf_u', ctypes.POINTER(ctypes.c_double)), ('psf_v', ctypes.POINTER(ctypes.c_double)),
-        ('psf_band', c_int), ('psf_variant', c_int), ('model_pairs', c_int),
+        ('psf_band', c_int), ('psf_variant', c_int), ('model_variant', c_int),
     ]
 
 CONV_MODES = dict(auto=0, fft=1, direct=2)
@@ -112,7 +112,7 @@ class BatchedSMDisk:
 
     def __init__(self, disk, geom, data, error=None, mask=None, weight=1.0, max_sets=512,
                  chunk=0, fft_size=(0, 0, 0), rows_k1=0, rows_k5=0, conv='auto', band=0, device=0,
-                 stream=None, psf_variant=0, model_pairs=0):
+                 stream=None, psf_variant=0, model_variant=0):
         if disk.traits['rht']:
             raise ValueError("the batched evaluator takes thin disks only")
         self.disk = disk
@@ -167,7 +167,7 @@ class BatchedSMDisk:
         d.conv_mode = CONV_MODES[conv]
         d.psf_band = int(band)
         d.psf_variant = int(psf_variant)
-        d.model_pairs = int(model_pairs)
+        d.model_variant = int(model_variant)
         rank, fu, fv = separable_factors(psf) if conv != 'fft' else (0, None, None)
         self._fu, self._fv = fu, fv
         d.psf_rank = rank

@@ -364,7 +364,7 @@ struct gbkb200_batch {
     int nper = 0;
     int direct = 0;
     int trim[3] = {0, 0, 0};          // direct mode: taps trimmed from each end (x, y, z)
-    int ka_pairs = 0;                 // direct mode: the model kernel takes chunk pairs
+    int ka_variant = 0;               // direct mode: the model kernel (model_variant)
     cudaEvent_t done = nullptr;       // recorded at the end of an asynchronous submission
     size_t smemB = 0;
     float* mplanes = nullptr;
@@ -420,6 +420,14 @@ static KaFn ka2_fn(int Kz)
     static KaFn t[KA_KMAX / 2 + 1] = {};
     static std::once_flag once;
     std::call_once(once, [] { ka2_register(t); });
+    return t[Kz / 2];
+}
+
+static KaFn ka3_fn(int Kz)
+{
+    static KaFn t[KA_KMAX / 2 + 1] = {};
+    static std::once_flag once;
+    std::call_once(once, [] { ka3_register(t); });
     return t[Kz / 2];
 }
 
@@ -551,9 +559,10 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     k_iw<<<592, 256, 0, bt->ctx->stream>>>(P, bt->iw, (long long)P.Nz * P.Ny * P.Nx);
     GBK_CUDA_TRY(cudaGetLastError());
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
-    if (d->model_pairs != 0 && d->model_pairs != 1) return GBKB200_ERR_INVALID_ARG;
-    bt->ka = d->model_pairs ? ka2_fn(P.Kz) : ka_fn(P.Kz);
-    bt->ka_pairs = d->model_pairs;
+    if (d->model_variant < 0 || d->model_variant > 2) return GBKB200_ERR_INVALID_ARG;
+    bt->ka = d->model_variant == 1 ? ka2_fn(P.Kz) : d->model_variant == 2 ? ka3_fn(P.Kz)
+                                                                           : ka_fn(P.Kz);
+    bt->ka_variant = d->model_variant;
     bt->kb = kb_fn(P.K, d->psf_variant);
     {
         const int rc = gbk_raise_smem_limit(reinterpret_cast<const void*>(bt->kb), bt->smemB);
@@ -854,7 +863,7 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
             const int cn = std::min(bt->chunk, nsets - s0);
             P.set0 = s0;
             stage_mark(bt, 0, true);
-            const int items = P.Wy * (bt->ka_pairs ? (P.nch + 1) / 2 : P.nch);
+            const int items = P.Wy * (bt->ka_variant == 1 ? (P.nch + 1) / 2 : P.nch);
             bt->ka<<<dim3((items + KA_THREADS / 32 - 1) / (KA_THREADS / 32), cn), KA_THREADS, 0,
                      st>>>(P, bt->ctx->d_status);
             stage_mark(bt, 0, false);

@@ -279,11 +279,12 @@ def test_batched_cubes_match_disk_path(gpu):
 
 
 @pytest.mark.parametrize('nodewise', [True, False])
-def test_batched_model_pairs_identical(gpu, nodewise):
-    """The model kernel on two 32-column chunks per warp (packed FP32 pairs,
-    each lane rounded as fmaf) gives bit-identical chi^2 and models, with an
-    odd number of chunks (the last warp's second chunk is absent) and on the
-    generic trait path."""
+def test_batched_model_variant_identical(gpu, nodewise):
+    """The model kernel's variants give bit-identical chi^2 and models: two
+    32-column chunks per warp (packed FP32 pairs, each lane rounded as fmaf;
+    an odd number of chunks, so the last warp's second chunk is absent) and
+    every lane through its own channel window into a shared-memory tile; on
+    the node-wise fast path and the generic trait path."""
     import torch
     from gbkfit_b200 import traits as T
     from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
@@ -298,9 +299,9 @@ def test_batched_model_pairs_identical(gpu, nodewise):
         w.extra = dict(w.extra, truth=dict(w.extra['truth'], spt_p=30.0, spt_s=300.0))
     data, err, _ = synthetic_data(w)
     out = []
-    for pairs in (0, 1):
+    for variant in (0, 1, 2):
         ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=n, chunk=4, conv='direct',
-                           model_pairs=pairs)
+                           model_variant=variant)
         bufs = ev.alloc_inputs(n)
         ev.upload(ev.pack(w.params, n), bufs, n)
         model = torch.zeros((n,) + tuple(w.geom.size[::-1]), device='cuda')
@@ -309,5 +310,6 @@ def test_batched_model_pairs_identical(gpu, nodewise):
         ev.close()
     nch = -(-(w.geom.size[0] + 16) // 32)
     assert nch % 2 == 1
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
     assert np.all(out[0][0] > 0)
