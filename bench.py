@@ -922,9 +922,9 @@ def main():
     ap.add_argument('--chunk', type=int, default=0, help='force the sets per wave (default: tuned)')
     ap.add_argument('--psf-variant', type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5],
                     help='PSF kernel variant of the direct mode (default: tuned)')
-    ap.add_argument('--model-variant', type=int, default=-1, choices=[-1, 0, 1, 2],
-                    help='model kernel of the direct mode: 0 union loop, 1 chunk pairs, '
-                         '2 own windows (default: tuned)')
+    ap.add_argument('--model-variant', type=int, default=-1, choices=[-1, 0, 1],
+                    help='model kernel of the direct mode: 0 one chunk per warp, 1 chunk '
+                         'pairs (default: tuned)')
     ap.add_argument('--band', type=int, default=0,
                     help='force the output rows per PSF block of the direct mode (default: tuned)')
     ap.add_argument('--workload', default='smdisk_batch128',

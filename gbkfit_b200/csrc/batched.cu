@@ -423,14 +423,6 @@ static KaFn ka2_fn(int Kz)
     return t[Kz / 2];
 }
 
-static KaFn ka3_fn(int Kz)
-{
-    static KaFn t[KA_KMAX / 2 + 1] = {};
-    static std::once_flag once;
-    std::call_once(once, [] { ka3_register(t); });
-    return t[Kz / 2];
-}
-
 static KcFn kc_fn(int Kz)
 {
     static KcFn t[KA_KMAX / 2 + 1] = {};
@@ -559,9 +551,8 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     k_iw<<<592, 256, 0, bt->ctx->stream>>>(P, bt->iw, (long long)P.Nz * P.Ny * P.Nx);
     GBK_CUDA_TRY(cudaGetLastError());
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
-    if (d->model_variant < 0 || d->model_variant > 2) return GBKB200_ERR_INVALID_ARG;
-    bt->ka = d->model_variant == 1 ? ka2_fn(P.Kz) : d->model_variant == 2 ? ka3_fn(P.Kz)
-                                                                           : ka_fn(P.Kz);
+    if (d->model_variant != 0 && d->model_variant != 1) return GBKB200_ERR_INVALID_ARG;
+    bt->ka = d->model_variant == 1 ? ka2_fn(P.Kz) : ka_fn(P.Kz);
     bt->ka_variant = d->model_variant;
     bt->kb = kb_fn(P.K, d->psf_variant);
     {

@@ -675,167 +675,6 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     }
 }
 
-// ka_lines_lsf with each lane stepping only through its own output window
-// [olo, ohi] (the planes its line reaches) instead of the union of its warp's
-// windows: the lanes' planes go into a shared-memory tile of TILE planes x
-// 32 columns (conflict-free: lane l writes column l), then the warp copies the
-// union's planes out as coalesced 128-byte row chunks and takes the range
-// ballots; outside its window a lane's value is 0, as ka_lines_lsf computes it.
-// Warps whose union exceeds TILE planes take ka_lines_lsf's loop.  Every value
-// is computed with ka_lines_lsf's expressions in its order.
-constexpr int KA3_TILE = 40;
-
-template<int KZ>
-__global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf3(BatchKernelArgs P, int* status)
-{
-    __shared__ float s_tile[KA_THREADS / 32][KA3_TILE * 32];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int item = blockIdx.x * (KA_THREADS / 32) + warp;
-    if (item >= P.Wy * P.nch) return;                    // whole warp
-    const int y = item / P.nch, chunk = item % P.nch;
-    const int c = blockIdx.y, b = P.set0 + c;
-    const DiskArgs a = set_disk(P, b);
-    const DiskConst kc = disk_const(a);
-    int bad = 0;
-    const int x = chunk * 32 + lane;
-    SpaxelOut o{};
-    int lo = INT_MAX, hi = -1;
-    float amp = 0.f, rinv = 0.f;
-    const bool on = x < P.Wx && (P.nwfast ? smdisk_spaxel_nw(a, kc, x, y, o)
-                                           : smdisk_spaxel(a, kc, x, y, 0, o, bad));
-    if (on && line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo, hi)) {
-        amp = o.orv * (1 / (o.dv * sqrtf(2 * GBK_PI)));
-        rinv = 1.4426950408889634f / (2 * o.dv * o.dv);
-    } else {
-        lo = INT_MAX;
-        hi = -1;
-    }
-    const float v = o.vv, z0 = a.spec_zero, dz = a.spec_step;
-    const unsigned wlen = (unsigned)hi - (unsigned)lo;
-    auto line_f = [&](int z, float zf) {
-        const float d = (z0 + zf * dz) - v;
-        float e;
-        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-(d * d) * rinv));
-        return (unsigned)z - (unsigned)lo <= wlen ? amp * e : 0.f;
-    };
-    const bool lit = lo <= hi;
-    const int olo = lit ? max(0, lo - KZ + 1) : INT_MAX, ohi = lit ? min(P.Nz - 1, hi) : -1;
-    const unsigned olen = lit ? (unsigned)(ohi - olo) : 0u;
-    int zlo = olo, zhi = ohi;
-#pragma unroll
-    for (int s = 16; s > 0; s >>= 1) {
-        zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, s));
-        zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, s));
-    }
-    int* xr = P.xr + (((long long)c * P.Wy + y) * P.nch + chunk) * P.Nz;
-    for (int zo = lane; zo < P.Nz; zo += 32)
-        if (zo < zlo || zo > zhi) xr[zo] = -1;
-    // executed output planes and line values of this lane (counters)
-    unsigned long long nfma = 0, nline = 0;
-    if (zlo <= zhi) {
-        float lz[KZ];
-#pragma unroll
-        for (int t = 0; t < KZ; ++t) lz[t] = P.lsfr[t];
-        const long long zstride = (long long)P.Wy * P.pitch;
-        float* dp = P.mplanes + ((long long)c * P.Nz * P.Wy + y) * P.pitch + x + zlo * zstride;
-        unsigned mm = 0u;
-        int mz = zlo, own = zlo + lane, fl = min(zlo + 31, zhi);
-        if (zhi - zlo < KA3_TILE) {
-            float* T = s_tile[warp];
-            if (lit) {
-                // the lane's own planes [olo, ohi]
-                float w[KZ];
-#pragma unroll
-                for (int t = 0; t < KZ - 1; ++t) w[t] = line_f(olo + t, (float)(olo + t));
-                float zf = (float)(olo + KZ - 1);
-                for (int zb = olo; zb <= ohi; zb += KZ) {
-#pragma unroll
-                    for (int k = 0; k < KZ; ++k) {
-                        const int zo = zb + k;
-                        if (zo > ohi) break;
-                        w[(k + KZ - 1) % KZ] = line_f(zo + KZ - 1, zf);
-                        zf += 1.f;
-                        float acc0 = 0.f, acc1 = 0.f;
-#pragma unroll
-                        for (int t = 0; t < KZ; t += 2) acc0 += lz[t] * w[(k + t) % KZ];
-#pragma unroll
-                        for (int t = 1; t < KZ; t += 2) acc1 += lz[t] * w[(k + t) % KZ];
-                        T[(zo - zlo) * 32 + lane] = acc0 + acc1;
-                    }
-                }
-                nfma = (unsigned long long)(ohi - olo + 1);
-                nline = nfma + (KZ - 1);
-            }
-            __syncwarp();
-            for (int zo = zlo; zo <= zhi; ++zo) {
-                const bool in = (unsigned)zo - (unsigned)olo <= olen;   // false for unlit lanes
-                *dp = in ? T[(zo - zlo) * 32 + lane] : 0.f;              // plane zo
-                dp += zstride;
-                const unsigned m = __ballot_sync(0xffffffffu, in);
-                if (zo == own) mm = m;
-                if (zo == fl) {
-                    if (own <= zo)
-                        xr[own] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
-                                        ((chunk * 32 + 31 - __clz(mm)) << 16))
-                                     : -1;
-                    mz = zo + 1;
-                    own = mz + lane;
-                    fl = min(mz + 31, zhi);
-                }
-            }
-        } else {
-            // a wide union: ka_lines_lsf's loop over it
-            float w[KZ];
-#pragma unroll
-            for (int t = 0; t < KZ - 1; ++t) w[t] = line_f(zlo + t, (float)(zlo + t));
-            float zf = (float)(zlo + KZ - 1);
-            for (int zb = zlo; zb <= zhi; zb += KZ) {
-#pragma unroll
-                for (int k = 0; k < KZ; ++k) {
-                    const int zo = zb + k;
-                    if (zo > zhi) break;
-                    w[(k + KZ - 1) % KZ] = line_f(zo + KZ - 1, zf);
-                    zf += 1.f;
-                    float acc0 = 0.f, acc1 = 0.f;
-#pragma unroll
-                    for (int t = 0; t < KZ; t += 2) acc0 += lz[t] * w[(k + t) % KZ];
-#pragma unroll
-                    for (int t = 1; t < KZ; t += 2) acc1 += lz[t] * w[(k + t) % KZ];
-                    *dp = acc0 + acc1;
-                    dp += zstride;
-                    const unsigned m = __ballot_sync(0xffffffffu,
-                                                     (unsigned)zo - (unsigned)olo <= olen);
-                    if (zo == own) mm = m;
-                    if (zo == fl) {
-                        if (own <= zo)
-                            xr[own] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
-                                            ((chunk * 32 + 31 - __clz(mm)) << 16))
-                                         : -1;
-                        mz = zo + 1;
-                        own = mz + lane;
-                        fl = min(mz + 31, zhi);
-                    }
-                }
-            }
-            nfma = (unsigned long long)(zhi - zlo + 1);
-            nline = nfma + (KZ - 1);
-        }
-    }
-    if (P.counters) {
-#pragma unroll
-        for (int s = 16; s > 0; s >>= 1) {
-            nfma += __shfl_xor_sync(0xffffffffu, nfma, s);
-            nline += __shfl_xor_sync(0xffffffffu, nline, s);
-        }
-        if (lane == 0) {
-            atomicAdd(&P.counters[GBK_CTR_KA_SPAXEL], 32ull);
-            atomicAdd(&P.counters[GBK_CTR_KA_FMA], nfma * KZ);
-            atomicAdd(&P.counters[GBK_CTR_KA_LINE], nline);
-        }
-    }
-    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
-}
-
 // ka_lines_lsf on two 32-column chunks per warp: lane l evaluates columns
 // 64 q + l and 64 q + 32 + l (chunks 2 q and 2 q + 1) and runs both LSF FIRs
 // as packed FP32 pairs (FFMA2: two lanes of fma, each rounded as fmaf, so
@@ -1049,8 +888,6 @@ void ka_register_short(KaFn* t);
 void ka_register_long(KaFn* t);
 // t[Kz / 2]: the two-chunk model kernel (ka_lines_lsf2)
 void ka2_register(KaFn* t);
-// t[Kz / 2]: the own-window model kernel (ka_lines_lsf3)
-void ka3_register(KaFn* t);
 // t[Kz / 2]: the LSF FIR of given model cubes
 typedef void (*KcFn)(BatchKernelArgs, const float*);
 void kc_register(KcFn* t);

@@ -367,11 +367,10 @@ typedef struct {
                              * (0-2: 4, 3-5: 5) x epilogue (variant % 3: 0 residual pass,
                              * 1 residual in the y-FIR items, 2 as 1 with the data
                              * prefetched); 0 = the first */
-    int model_variant;      /* direct mode, the model kernel (all give the same values):
+    int model_variant;      /* direct mode, the model kernel (both give the same values):
                              * 0 = a warp per 32-column chunk stepping every lane through
                              * the union of the lanes' channel windows; 1 = two chunks per
-                             * warp on packed FP32 pairs; 2 = each lane through its own
-                             * window into a shared-memory tile, copied out by plane */
+                             * warp on packed FP32 pairs */
 } gbkb200_batch_desc;
 
 int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);
