@@ -967,9 +967,25 @@ static int submit_tail(gbkb200_batch* bt, int nsets, const float* chi2_dev, floa
     if (nsets > 0 && chi2_host)
         GBK_CUDA_TRY(cudaMemcpyAsync(chi2_host, chi2_dev, (size_t)nsets * sizeof(float),
                                      cudaMemcpyDeviceToHost, st));
+    // the kernels' status word, read by gbkb200_batch_take_status once done
+    GBK_CUDA_TRY(cudaMemcpyAsync(bt->ctx->h_status, bt->ctx->d_status, sizeof(int),
+                                 cudaMemcpyDeviceToHost, st));
     if (!bt->done) GBK_CUDA_TRY(cudaEventCreateWithFlags(&bt->done, cudaEventDisableTiming));
     GBK_CUDA_TRY(cudaEventRecord(bt->done, st));
     return GBKB200_OK;
+}
+
+extern "C" int gbkb200_batch_take_status(gbkb200_batch* bt)
+{
+    if (!bt) return GBKB200_ERR_INVALID_ARG;
+    const int s = *bt->ctx->h_status;
+    if (!s) return GBKB200_OK;
+    // cleared for the next submission (enqueued after the completed one)
+    *bt->ctx->h_status = 0;
+    GBK_CUDA_TRY(cudaMemsetAsync(bt->ctx->d_status, 0, sizeof(int), bt->ctx->stream));
+    if (s & GBK_STATUS_BAD_TRAIT) return GBKB200_ERR_BAD_TRAIT;
+    if (s & GBK_STATUS_TIMEOUT) return GBKB200_ERR_TIMEOUT;
+    return GBKB200_ERR_INVALID_ARG;
 }
 
 extern "C" int gbkb200_batch_submit(gbkb200_batch* bt, int nsets, const void* in_host,

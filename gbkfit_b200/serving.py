@@ -599,6 +599,8 @@ class ModelServer:
     def _complete_group(self, ds):
         ev, out, reqs = ds.group
         chi2 = out.numpy().copy()
+        # a kernel of the group raised the status word (unknown trait uid)
+        rc = _lib.gbkb200_batch_take_status(ds.batched.handle)
         now = time.perf_counter()
         with self._cv:
             ds.group = None
@@ -610,7 +612,10 @@ class ModelServer:
             if ds.released and ds.holders == 0:
                 self._release(ds)
         for r, c in zip(reqs, chi2):
-            r.future.set_result(dict(chi2=float(c)))
+            if rc:
+                r.future.set_exception(_native.NativeError(rc, 'serving group'))
+            else:
+                r.future.set_result(dict(chi2=float(c)))
 
     def _launch(self, slot, req, need):
         ds = req.ds

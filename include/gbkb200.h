@@ -408,6 +408,10 @@ int gbkb200_batch_submit(gbkb200_batch* b, int nsets, const void* in_host, void*
 int gbkb200_batch_submit_cubes(gbkb200_batch* b, int nsets, const float* cubes, float* chi2_dev,
                                float* chi2_host);
 int gbkb200_batch_query(const gbkb200_batch* b, int* done);
+/* after the last submission completed: GBKB200_OK, or the error of the status
+ * word its kernels raised (GBKB200_ERR_BAD_TRAIT: a model of the submission
+ * met an unknown trait uid), which is then cleared */
+int gbkb200_batch_take_status(gbkb200_batch* b);
 /* the chosen FFT grid, chunk, the device bytes the evaluator holds (its
  * work space, tables and partials) and the convolution mode (1 = FFT,
  * 2 = direct) */

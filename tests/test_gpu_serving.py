@@ -217,3 +217,31 @@ def test_coalesced_mcdisk_matches_fft_path(gpu):
         assert not any(r.cube for r in reqs)
     for c, f in zip(got, fft):
         assert abs(c - f) <= 1e-4 * abs(f), (c, f)
+
+
+def test_coalesced_group_reports_unknown_trait(gpu):
+    """An mcdisk request whose height trait has an unknown uid: the kernels
+    raise the status word, its coalesced group's futures fail with
+    GBKB200_ERR_BAD_TRAIT (no GPU fault: the cloud is discarded), the status
+    is cleared, and the dataset's next group completes normally."""
+    import copy
+    from gbkfit_b200 import traits as T
+    from gbkfit_b200._native import NativeError
+    from gbkfit_b200.disk import Disk
+    from gbkfit_b200.serving import ModelServer, Request
+    stream = _small_stream(n=40, seed=31)
+    q = [q for q in stream.requests if q['kind'] == 'mcdisk'][0]
+    d = stream.datasets[q['dataset']]
+    good = d['mcdisk']
+    bad_rht = copy.copy(T.bht('sech2'))
+    bad_rht._uid = 77
+    bad = Disk(False, False, good.rnodes, traits=dict(good.traits, rht=[bad_rht]))
+    with ModelServer(slots=2) as srv:
+        _register_coalesced(srv, stream)
+        f = srv.submit(Request(q['dataset'], 'mcdisk', bad, q['params'], cflux=q['cflux'],
+                               thick=True))
+        with pytest.raises(NativeError, match='unknown trait uid'):
+            f.result(timeout=300)
+        ok = srv.submit(Request(q['dataset'], 'mcdisk', good, q['params'], cflux=q['cflux'],
+                                thick=True)).result(timeout=300)
+        assert np.isfinite(ok['chi2']) and ok['chi2'] > 0
