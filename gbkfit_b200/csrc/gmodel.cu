@@ -217,11 +217,39 @@ struct McConst {
     float vsys, xpos, ypos;
     float s_i, c_i, s_p, c_p;      // sincos(-incl), sincos(-posa)
     float sin_incl, cos_incl;
+    float ix, iy, iz, ispec;       // 1 / the grid steps
 };
+
+// 1 / (sigma sqrt(2 pi)) and log2(e) / (2 sigma^2) of a cloud's line from
+// one reciprocal of sigma
+__device__ __forceinline__ void mc_line_consts(float dv, float& amp, float& rinv)
+{
+    const float r = 1.f / dv;
+    amp = r * 0.3989422804014327f;
+    rinv = 0.7213475204444817f * r * r;
+}
+
+// line_window with the reciprocal of the channel width
+__device__ __forceinline__ bool mc_line_window(float v, float d, int nz, float istep, float zero,
+                                               int& zlo, int& zhi)
+{
+    if (!isfinite(v) || !isfinite(d)) return false;
+    const float zmin = v - d * GBK_LINE_WIDTH, zmax = v + d * GBK_LINE_WIDTH;
+    float a = rintf((zmin - zero) * istep), b = rintf((zmax - zero) * istep);
+    a = a < 0.f ? 0.f : a;
+    b = (float)(nz - 1) < b ? (float)(nz - 1) : b;
+    zlo = (int)a;
+    zhi = (int)b;
+    return zlo <= zhi;
+}
 
 __device__ __forceinline__ McConst mc_const(const DiskArgs& a)
 {
     McConst k{};
+    k.ix = 1.f / a.stx;
+    k.iy = 1.f / a.sty;
+    k.iz = 1.f / a.stz;
+    k.ispec = 1.f / a.spec_step;
     if (!a.loose) {
         k.vsys = a.vsys ? a.vsys[0] : 0.f;
         k.xpos = a.xpos[0];
@@ -341,8 +369,8 @@ __device__ __forceinline__ bool mcdisk_cloud(const DiskArgs& a, const McArgs& m,
     rot_lh_z(xn, yn, s_p, c_p);
     xn -= -xposi;
     yn -= -yposi;
-    float fx = rintf((xn - a.zx) / a.stx), fy = rintf((yn - a.zy) / a.sty);
-    float fz = rintf((zn - a.zz) / a.stz);
+    float fx = rintf((xn - a.zx) * mk.ix), fy = rintf((yn - a.zy) * mk.iy);
+    float fz = rintf((zn - a.zz) * mk.iz);
     if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) return false;
     if (fx < 0 || fx >= a.sx || fy < 0 || fy >= a.sy || fz < 0 || fz >= a.sz) return false;
     int x = (int)fx, y = (int)fy, z = (int)fz;
@@ -388,9 +416,10 @@ __global__ void __launch_bounds__(256) mcdisk_kernel(DiskArgs a, McArgs m, int* 
         if (!mcdisk_cloud(a, m, mk, ci, x, y, z, o, bad)) continue;
         if (a.image) atomicAdd(&a.image[x + (long long)a.sx * y], o.orv);
         int zlo, zhi;
-        if (a.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
-            const float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
-            const float rinv = 1.4426950408889634f / (2 * o.dv * o.dv);
+        if (a.scube &&
+            mc_line_window(o.vv, o.dv, a.spec_size, mk.ispec, a.spec_zero, zlo, zhi)) {
+            float amp, rinv;
+            mc_line_consts(o.dv, amp, rinv);
             float* col = a.scube + (x + (long long)a.sx * y);
             long long plane = (long long)a.sx * a.sy;
             for (int zs = zlo; zs <= zhi; ++zs) {
@@ -436,9 +465,9 @@ __global__ void __launch_bounds__(256) mcdisk_v4_kernel(DiskArgs a, McArgs m, fl
         if (!mcdisk_cloud(a, m, mk, ci, x, y, z, o, bad)) continue;
         if (a.image) atomicAdd(&a.image[x + (long long)a.sx * y], o.orv);
         int zlo, zhi;
-        if (lines && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
-            const float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
-            const float rinv = 1.4426950408889634f / (2 * o.dv * o.dv);
+        if (lines && mc_line_window(o.vv, o.dv, a.spec_size, mk.ispec, a.spec_zero, zlo, zhi)) {
+            float amp, rinv;
+            mc_line_consts(o.dv, amp, rinv);
             float* col = lines + (x + (long long)a.sx * y) * nzp;
             for (int z4 = zlo & ~3; z4 <= zhi; z4 += 4) {
                 float v[4];
@@ -560,8 +589,11 @@ __global__ void __launch_bounds__(256) mcdisk_bound_kernel(DiskArgs a, McArgs m,
         SpaxelOut o;
         if (ci < m.nclouds && mcdisk_cloud(a, m, mk, ci, x, y, z, o, bad)) {
             int zlo, zhi;
-            if (a.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi))
-                vc = o.orv * (1 / (o.dv * sqrtf(2 * GBK_PI)));
+            float amp, rinv;
+            mc_line_consts(o.dv, amp, rinv);
+            if (a.scube &&
+                mc_line_window(o.vv, o.dv, a.spec_size, mk.ispec, a.spec_zero, zlo, zhi))
+                vc = o.orv * amp;
             vm = fmaxf(fabsf(o.orv), fabsf(o.rv));
         }
         atomic_max_abs(&bound[0], vc);
@@ -588,9 +620,9 @@ __global__ void __launch_bounds__(256) mcdisk_fixed_kernel(DiskArgs a, McArgs m,
         const long long sp = x + (long long)a.sx * y;
         if (f.image) fixed_add(&f.image[sp], o.orv, km);
         int zlo, zhi;
-        if (f.scube && line_window(o.vv, o.dv, a.spec_size, a.spec_step, a.spec_zero, zlo, zhi)) {
-            const float amp = 1 / (o.dv * sqrtf(2 * GBK_PI));
-            const float rinv = 1.4426950408889634f / (2 * o.dv * o.dv);
+        if (f.scube && mc_line_window(o.vv, o.dv, a.spec_size, mk.ispec, a.spec_zero, zlo, zhi)) {
+            float amp, rinv;
+            mc_line_consts(o.dv, amp, rinv);
             const long long plane = (long long)a.sx * a.sy;
             for (int zs = zlo; zs <= zhi; ++zs) {
                 const float zv = a.spec_zero + zs * a.spec_step;
