@@ -10,7 +10,7 @@ Knobs (all change speed only, never results beyond fp32 rounding):
   resident blocks, more halo rows);
 * ``psf_variant``: PSF kernel sized for 4 or 5 resident blocks per SM, with
   its residual in a separate pass or in the y-FIR items (data loaded after or
-  before each item's FIR);
+  before each item's FIR), or persistent over all (set, plane) items;
 * ``model_variant``: the direct mode's model kernel (0: one 32-column chunk
   per warp; 1: two chunks per warp on packed FP32 pairs; the same values);
 * ``rows_k1``: spectral rows per shared-memory group of the model kernel.
@@ -122,7 +122,7 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
                 best_d, best_dt = cfg, t
         # the PSF kernel's variants (resident blocks per SM x epilogue)
         base = dict(best_d)
-        for variant in range(1, 6):
+        for variant in range(1, 7):
             cfg = dict(base, psf_variant=variant)
             t = time_config(w, data, err, nsets, cfg)
             if t < best_dt:

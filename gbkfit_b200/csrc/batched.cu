@@ -365,6 +365,7 @@ struct gbkb200_batch {
     int direct = 0;
     int trim[3] = {0, 0, 0};          // direct mode: taps trimmed from each end (x, y, z)
     int ka_variant = 0;               // direct mode: the model kernel (model_variant)
+    int kb_grid = 0;                  // persistent PSF kernel: blocks of a launch (else 0)
     cudaEvent_t done = nullptr;       // recorded at the end of an asynchronous submission
     size_t smemB = 0;
     float* mplanes = nullptr;
@@ -405,6 +406,20 @@ static void stage_mark(gbkb200_batch* bt, int stage, bool begin)
     }
 }
 
+// the PSF kernel over cn sets: a block per (set, plane, band), or the
+// persistent variant's resident wave over all of them
+static void launch_kb(const gbkb200_batch* bt, BatchKernelArgs& P, int cn, cudaStream_t st)
+{
+    if (bt->kb_grid > 0) {
+        P.kb_cn = cn;
+        const long long items = (long long)cn * P.Nz * P.nbands;
+        const int grid = (int)std::min<long long>(items, bt->kb_grid);
+        bt->kb<<<grid, KB_THREADS, bt->smemB, st>>>(P);
+    } else {
+        bt->kb<<<dim3(cn, P.Nz * P.nbands), KB_THREADS, bt->smemB, st>>>(P);
+    }
+}
+
 static KaFn ka_fn(int Kz)
 {
     static KaFn t[KA_KMAX / 2 + 1] = {};
@@ -438,6 +453,7 @@ static KbFn kb_fn(int K, int variant)
     std::call_once(once, [] {
         kb_register4(t);
         kb_register5(t + 3);
+        kb_register_pf(t + 6);
     });
     return t[variant][(K - KB_KMIN) / 2];
 }
@@ -511,18 +527,24 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     // otherwise 54 KB (four blocks per SM)
     int bpmax = 4 * (2 * ((P.Nx + 7) / 8 - 1) + NW);
     bpmax += ((4 - bpmax % 32) + 32) % 32;
-    const long long xr_bytes = (long long)(P.band + P.K - 1) * P.nch * sizeof(int);
+    // range entries of the band's input rows (the persistent variant 6: two
+    // buffers, each rounded to 4 entries)
+    const bool pf = d->psf_variant == 6;
+    const long long xr_slot = ((long long)(P.band + P.K - 1) * P.nch + 3) & ~3LL;
+    const long long xr_bytes = pf ? 2 * xr_slot * (long long)sizeof(int)
+                                  : (long long)(P.band + P.K - 1) * P.nch * sizeof(int);
     const long long need_min = (long long)(P.K + 15) * bpmax;
     const long long need_all = (long long)(P.band + P.K + 7) * bpmax;
     // PSF kernel variant: 0-2 sized for 4 resident blocks per SM, 3-5 for 5,
-    // epilogue (variant % 3) as in kb_psf_residual; shared memory per block:
-    // 55 KB for 4 blocks per SM, 43 KB for 5
+    // epilogue (variant % 3) as in kb_psf_residual, 6 = 0 as a persistent
+    // kernel; shared memory per block: 55 KB for 4 blocks per SM, 43 KB for 5
     if (d->psf_variant < 0 || d->psf_variant >= KB_VARIANTS) return GBKB200_ERR_INVALID_ARG;
-    const int blocks = d->psf_variant >= 3 ? 5 : 4;
+    const int blocks = (d->psf_variant >= 3 && d->psf_variant <= 5) ? 5 : 4;
     const long long budget = blocks == 5 ? 43LL * 1024 : 55LL * 1024;
     const long long cap = std::max(need_min, std::min(need_all, (budget - xr_bytes) / 4));
     if (cap * (long long)sizeof(float) + xr_bytes > 227LL * 1024) return GBKB200_ERR_UNSUPPORTED;
     P.cap = (int)cap;
+    P.xr_slot = pf ? (int)xr_slot : 0;
     bt->smemB = (size_t)cap * sizeof(float) + (size_t)xr_bytes;
     std::vector<float> vr(P.K, 0.f), ur(P.K, 0.f), lr(P.Kz);
     for (int s = 0; s < P.Kx; ++s) vr[s] = (float)d->psf_v[d->kernel_size[0] - 1 - tx - s];
@@ -558,6 +580,14 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     {
         const int rc = gbk_raise_smem_limit(reinterpret_cast<const void*>(bt->kb), bt->smemB);
         if (rc) return rc;
+    }
+    if (pf) {
+        // one resident wave of blocks
+        int per_sm = 0, nsm = 0;
+        GBK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, reinterpret_cast<const void*>(bt->kb), KB_THREADS, bt->smemB));
+        GBK_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, bt->ctx->device));
+        bt->kb_grid = std::max(1, per_sm) * std::max(1, nsm);
     }
     bt->nper = P.Nz * P.nbands;
     if (cudaMalloc(&bt->partials, (size_t)bt->max_sets * bt->nper * sizeof(double)) != cudaSuccess)
@@ -866,7 +896,7 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
             }
             stage_mark(bt, 1, false);
             stage_mark(bt, 4, true);
-            bt->kb<<<dim3(cn, P.Nz * P.nbands), KB_THREADS, bt->smemB, st>>>(P);
+            launch_kb(bt, P, cn, st);
             stage_mark(bt, 4, false);
         }
         stage_mark(bt, 5, true);
@@ -950,7 +980,7 @@ extern "C" int gbkb200_batch_evaluate_cubes(gbkb200_batch* bt, int nsets, const 
         }
         stage_mark(bt, 1, false);
         stage_mark(bt, 4, true);
-        bt->kb<<<dim3(cn, P.Nz * P.nbands), KB_THREADS, bt->smemB, st>>>(P);
+        launch_kb(bt, P, cn, st);
         stage_mark(bt, 4, false);
     }
     stage_mark(bt, 5, true);

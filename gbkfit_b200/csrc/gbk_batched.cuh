@@ -36,6 +36,8 @@ struct BatchKernelArgs {
     int pitch;            // row pitch of the LSF-convolved planes in HBM (floats, % 32 == 0)
     int cap;              // shared-memory floats of a PSF block (rows of one pass)
     int band, nbands;     // output rows per PSF block, bands per plane
+    int xr_slot;          // persistent PSF kernel: ints per range-entry buffer (% 4 == 0)
+    int kb_cn;            // persistent PSF kernel: sets of the launch
     // FIR coefficients in the parameter block (constant bank, uniform loads)
     float vr[33];         // (K): PSF x factor, reversed, zero-padded
     float ur[33];         // (K): PSF y factor, reversed, zero-padded
@@ -220,6 +222,12 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
 __device__ __forceinline__ void cp_async_wait_all()
 {
     asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -255,34 +263,66 @@ constexpr int KB_NX_MAX = 512;  // widest data cube of the direct mode
 // pass's rows reading shared memory; 1: the residual in each y-FIR item's
 // epilogue (no write-back, no barriers between items), its data loaded after
 // the item's FIR; 2: as 1, with the item's data requested before its FIR.
-template<int K, int MINB, int EPI>
+template<int K, int MINB, int EPI, bool PF>
 __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelArgs P)
 {
     constexpr int NW = (K + 7 + 3) / 4;     // float4 slots of one 8-output x window
     constexpr int NWARPS = KB_THREADS / 32;
     extern __shared__ float4 sm4[];
     float* S = reinterpret_cast<float*>(sm4);                   // (rows of a pass, bp)
-    int* s_xr = reinterpret_cast<int*>(S + P.cap);              // (in1 - ob0, nch) entries
+    // (in1 - ob0, nch) range entries of an item; PF: two buffers of xr_slot ints
+    int* const s_xr0 = reinterpret_cast<int*>(S + P.cap);
     __shared__ float warp_part[NWARPS];
     __shared__ int s_box[4];
-    // sets vary fastest: the blocks in flight share a few planes of the data
-    const int zo = blockIdx.y / P.nbands, band = blockIdx.y % P.nbands;
-    const int c = blockIdx.x, b = P.set0 + c;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ld = P.Nx + 1;
+    // PF (persistent): block i takes items i, i + grid, ... of cn x Nz x nbands,
+    // sets fastest; the next item's range entries are copied into the other
+    // buffer (cp.async) while this item runs.  Otherwise one item per block:
+    // blockIdx.x the set, blockIdx.y the (plane, band) - sets vary fastest, so
+    // the blocks in flight share a few planes of the data.
+    const int nit = PF ? P.kb_cn * P.Nz * P.nbands : 1;
+    auto entries = [&](int it, const int*& src, int& n, int& ob0_) {
+        const int c_ = PF ? it % P.kb_cn : blockIdx.x;
+        const int yi = PF ? it / P.kb_cn : blockIdx.y;
+        const int zo_ = yi / P.nbands, band_ = yi % P.nbands;
+        ob0_ = band_ * P.band;
+        const int ob1_ = min(P.Ny, ob0_ + P.band), in1_ = min(P.Wy, ob1_ + K - 1);
+        src = P.xrt + (((long long)c_ * P.Nz + zo_) * P.Wy + ob0_) * P.nch;
+        n = (in1_ - ob0_) * P.nch;
+    };
+    auto prefetch = [&](int it, int* dst) {
+        const int* src;
+        int n, o;
+        entries(it, src, n, o);
+        for (int i = threadIdx.x; i < n; i += KB_THREADS) cp_async4(dst + i, src + i);
+    };
+    int buf = 0;
+    if (PF && (int)blockIdx.x < nit) prefetch(blockIdx.x, s_xr0);
+    for (int it = PF ? (int)blockIdx.x : 0; it < nit; it += PF ? (int)gridDim.x : 1) {
+    int* const s_xr = s_xr0 + buf * P.xr_slot;
+    const int c = PF ? it % P.kb_cn : (int)blockIdx.x, b = P.set0 + c;
+    const int yi = PF ? it / P.kb_cn : (int)blockIdx.y;
+    const int zo = yi / P.nbands, band = yi % P.nbands;
     const int ob0 = band * P.band, ob1 = min(P.Ny, ob0 + P.band);  // output rows [ob0, ob1)
     const int in1 = min(P.Wy, ob1 + K - 1);                        // input rows [ob0, in1)
     const long long prow = ((long long)c * P.Nz + zo) * P.Wy;
     const int* xr = P.xrt + prow * P.nch;                          // (y, chunk) at [y nch + chunk]
-    const int ld = P.Nx + 1;
     const double* T = P.sat + (long long)zo * (P.Ny + 1) * ld;
+    if (PF) cp_async_wait_all();          // this item's entries (this thread's copies)
     if (threadIdx.x == 0) {
         s_box[0] = INT_MAX; s_box[1] = -1; s_box[2] = INT_MAX; s_box[3] = -1;
     }
     __syncthreads();
+    // the next item's entries, into the other buffer (its last reader, the
+    // item before this one, has finished)
+    if (PF && it + (int)gridDim.x < nit) prefetch(it + gridDim.x, s_xr0 + (buf ^ 1) * P.xr_slot);
+    do {
     // bounding box of the nonzero input row chunks
     {
         int y0 = INT_MAX, y1 = -1, x0 = INT_MAX, x1 = -1;
         // the entries of rows [ob0, in1), eight loads in flight per thread
+        // (PF: already in s_xr)
         const int* src = xr + ob0 * P.nch;
         const int n = (in1 - ob0) * P.nch;
         for (int i0 = 0; i0 < n; i0 += 8 * KB_THREADS) {
@@ -290,8 +330,12 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 const int i = i0 + u * KB_THREADS + threadIdx.x;
-                v[u] = i < n ? src[i] : -1;
-                if (i < n) s_xr[i] = v[u];
+                if (PF) {
+                    v[u] = i < n ? s_xr[i] : -1;
+                } else {
+                    v[u] = i < n ? src[i] : -1;
+                    if (i < n) s_xr[i] = v[u];
+                }
             }
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
@@ -329,7 +373,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
                  i += KB_THREADS)
                 model[i] = 0.f;
         if (threadIdx.x == 0) P.partials[part] = sat_box(T, ld, ob0, ob1, 0, P.Nx);
-        return;
+        break;
     }
     // output box: x in 8-column strips [g_lo, g_hi], rows [yo_lo, yb_end) in 8-row groups
     const int g_lo = max(0, x0 - K + 1) >> 3, g_hi = min(P.Nx - 1, x1) >> 3;
@@ -673,6 +717,10 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
             atomicAdd(&P.counters[GBK_CTR_KB_VOX], c_v);
         }
     }
+    } while (0);
+    if (PF) __syncthreads();   // before the next item reuses the shared memory
+    buf ^= 1;
+    }
 }
 
 // ka_lines_lsf on two 32-column chunks per warp: lane l evaluates columns
@@ -892,8 +940,10 @@ void ka2_register(KaFn* t);
 typedef void (*KcFn)(BatchKernelArgs, const float*);
 void kc_register(KcFn* t);
 // t[v][(K - KB_KMIN) / 2] for the PSF kernel variant v = 3 * (MINB == 5) + EPI
-constexpr int KB_VARIANTS = 6;
+// (v = 6: MINB 4, EPI 0, persistent with prefetched range entries)
+constexpr int KB_VARIANTS = 7;
 void kb_register4(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1]);   // MINB 4, EPI 0-2
 void kb_register5(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1]);   // MINB 5, EPI 0-2
+void kb_register_pf(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1]); // MINB 4, EPI 0, persistent
 
 }  // namespace gbk
