@@ -366,6 +366,7 @@ struct gbkb200_batch {
     int trim[3] = {0, 0, 0};          // direct mode: taps trimmed from each end (x, y, z)
     int ka_variant = 0;               // direct mode: the model kernel (model_variant)
     int kb_grid = 0;                  // persistent PSF kernel: blocks of a launch (else 0)
+    int* kb_work = nullptr;           // persistent PSF kernel: its item counter
     cudaEvent_t done = nullptr;       // recorded at the end of an asynchronous submission
     size_t smemB = 0;
     float* mplanes = nullptr;
@@ -414,6 +415,7 @@ static void launch_kb(const gbkb200_batch* bt, BatchKernelArgs& P, int cn, cudaS
         P.kb_cn = cn;
         const long long items = (long long)cn * P.Nz * P.nbands;
         const int grid = (int)std::min<long long>(items, bt->kb_grid);
+        cudaMemsetAsync(bt->kb_work, 0, sizeof(int), st);
         bt->kb<<<grid, KB_THREADS, bt->smemB, st>>>(P);
     } else {
         bt->kb<<<dim3(cn, P.Nz * P.nbands), KB_THREADS, bt->smemB, st>>>(P);
@@ -588,6 +590,8 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
             &per_sm, reinterpret_cast<const void*>(bt->kb), KB_THREADS, bt->smemB));
         GBK_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, bt->ctx->device));
         bt->kb_grid = std::max(1, per_sm) * std::max(1, nsm);
+        if (cudaMalloc(&bt->kb_work, sizeof(int)) != cudaSuccess) return GBKB200_ERR_OOM;
+        P.kb_work = bt->kb_work;
     }
     bt->nper = P.Nz * P.nbands;
     if (cudaMalloc(&bt->partials, (size_t)bt->max_sets * bt->nper * sizeof(double)) != cudaSuccess)
@@ -655,6 +659,7 @@ extern "C" int gbkb200_batch_destroy(gbkb200_batch* bt)
     cudaFree(bt->counters);
     for (cudaEvent_t e : bt->ev) cudaEventDestroy(e);
     if (bt->done) cudaEventDestroy(bt->done);
+    cudaFree(bt->kb_work);
     delete bt;
     return GBKB200_OK;
 }

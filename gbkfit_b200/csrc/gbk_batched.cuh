@@ -38,6 +38,7 @@ struct BatchKernelArgs {
     int band, nbands;     // output rows per PSF block, bands per plane
     int xr_slot;          // persistent PSF kernel: ints per range-entry buffer (% 4 == 0)
     int kb_cn;            // persistent PSF kernel: sets of the launch
+    int* kb_work;         // persistent PSF kernel: item counter (zeroed before each launch)
     // FIR coefficients in the parameter block (constant bank, uniform loads)
     float vr[33];         // (K): PSF x factor, reversed, zero-padded
     float ur[33];         // (K): PSF y factor, reversed, zero-padded
@@ -276,9 +277,10 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     __shared__ int s_box[4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ld = P.Nx + 1;
-    // PF (persistent): block i takes items i, i + grid, ... of cn x Nz x nbands,
-    // sets fastest; the next item's range entries are copied into the other
-    // buffer (cp.async) while this item runs.  Otherwise one item per block:
+    // PF (persistent): the blocks take items of cn x Nz x nbands (sets fastest)
+    // from a work counter, one ahead: the next item's range entries are copied
+    // into the other buffer (cp.async) while this item runs.  Otherwise one
+    // item per block:
     // blockIdx.x the set, blockIdx.y the (plane, band) - sets vary fastest, so
     // the blocks in flight share a few planes of the data.
     const int nit = PF ? P.kb_cn * P.Nz * P.nbands : 1;
@@ -297,9 +299,16 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
         entries(it, src, n, o);
         for (int i = threadIdx.x; i < n; i += KB_THREADS) cp_async4(dst + i, src + i);
     };
-    int buf = 0;
-    if (PF && (int)blockIdx.x < nit) prefetch(blockIdx.x, s_xr0);
-    for (int it = PF ? (int)blockIdx.x : 0; it < nit; it += PF ? (int)gridDim.x : 1) {
+    __shared__ int s_next;
+    int buf = 0, it = 0;
+    if (PF) {
+        if (threadIdx.x == 0) s_next = atomicAdd(P.kb_work, 1);
+        __syncthreads();
+        it = s_next;
+        __syncthreads();      // every thread has read s_next before it is rewritten
+        if (it < nit) prefetch(it, s_xr0);
+    }
+    while (it < nit) {
     int* const s_xr = s_xr0 + buf * P.xr_slot;
     const int c = PF ? it % P.kb_cn : (int)blockIdx.x, b = P.set0 + c;
     const int yi = PF ? it / P.kb_cn : (int)blockIdx.y;
@@ -312,11 +321,13 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     if (PF) cp_async_wait_all();          // this item's entries (this thread's copies)
     if (threadIdx.x == 0) {
         s_box[0] = INT_MAX; s_box[1] = -1; s_box[2] = INT_MAX; s_box[3] = -1;
+        if (PF) s_next = atomicAdd(P.kb_work, 1);
     }
     __syncthreads();
     // the next item's entries, into the other buffer (its last reader, the
     // item before this one, has finished)
-    if (PF && it + (int)gridDim.x < nit) prefetch(it + gridDim.x, s_xr0 + (buf ^ 1) * P.xr_slot);
+    const int next = PF ? s_next : nit;
+    if (PF && next < nit) prefetch(next, s_xr0 + (buf ^ 1) * P.xr_slot);
     do {
     // bounding box of the nonzero input row chunks
     {
@@ -720,6 +731,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     } while (0);
     if (PF) __syncthreads();   // before the next item reuses the shared memory
     buf ^= 1;
+    it = next;
     }
 }
 
