@@ -177,8 +177,9 @@ __global__ void __launch_bounds__(512) k1_model_xfft(BatchKernelArgs P, int* sta
         const unsigned long long mhx = fdiv_magic(P.hx);
         for (int e = threadIdx.x; e < gn * P.hx; e += blockDim.x) {
             const int l = fdiv(e, mhx), k = e - l * P.hx;
-            float2 zk = r[l * M + (k % M)];
-            float2 zc = conjf2(r[l * M + ((M - k) % M)]);
+            // k in [0, M]: k mod M and (M - k) mod M without a division
+            float2 zk = r[l * M + (k == M ? 0 : k)];
+            float2 zc = conjf2(r[l * M + (k == 0 ? 0 : M - k)]);
             float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
             float2 od = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
             float2 t = cmul(s_post[k], make_float2(od.y, -od.x));

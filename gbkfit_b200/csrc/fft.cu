@@ -70,8 +70,9 @@ __global__ void __launch_bounds__(FFT_THREADS) x_r2c_kernel(const float* in, flo
         if (row >= rows) continue;
         float2 X;
         if (even) {
-            float2 zk = z[l * M + (k % M)];
-            float2 zc = conjf2(z[l * M + ((M - k) % M)]);
+            // k in [0, M]: k mod M and (M - k) mod M without a division
+            float2 zk = z[l * M + (k == M ? 0 : k)];
+            float2 zc = conjf2(z[l * M + (k == 0 ? 0 : M - k)]);
             float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
             float2 od = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
             // X = E + W^k * (-i) * O

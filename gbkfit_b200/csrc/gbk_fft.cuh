@@ -188,10 +188,14 @@ static __device__ void pass_generic(const float2* src, float2* dst, int n, int R
     }
 }
 
-// All passes of one transform; returns the buffer holding the result.
-static __device__ float2* fft_smem(float2* b0, float2* b1, const AxisDev& ax, int L, int sk, int sl,
-                            bool rows, const float2* tw, bool inv)
+// All passes of one transform; returns the buffer holding the result.  The
+// direction and the line layout are template parameters, so the
+// butterflies' direction selects and the index mapping's branch fold away.
+template<bool INV, bool ROWS>
+static __device__ float2* fft_smem_t(float2* b0, float2* b1, const AxisDev& ax, int L, int sk,
+                                     int sl, const float2* tw)
 {
+    constexpr bool inv = INV, rows = ROWS;
     float2* src = b0;
     float2* dst = b1;
     int Ns = 1;
@@ -215,6 +219,17 @@ static __device__ float2* fft_smem(float2* b0, float2* b1, const AxisDev& ax, in
         Ns *= R;
     }
     return src;
+}
+
+static __device__ __forceinline__ float2* fft_smem(float2* b0, float2* b1, const AxisDev& ax,
+                                                   int L, int sk, int sl, bool rows,
+                                                   const float2* tw, bool inv)
+{
+    if (rows)
+        return inv ? fft_smem_t<true, true>(b0, b1, ax, L, sk, sl, tw)
+                   : fft_smem_t<false, true>(b0, b1, ax, L, sk, sl, tw);
+    return inv ? fft_smem_t<true, false>(b0, b1, ax, L, sk, sl, tw)
+               : fft_smem_t<false, false>(b0, b1, ax, L, sk, sl, tw);
 }
 
 __device__ __forceinline__ void load_twiddles(float2* s_tw, const float2* g_tw, int n)
