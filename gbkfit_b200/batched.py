@@ -415,9 +415,14 @@ class BatchedSMDisk:
         return {n: int(out[i]) for i, n in enumerate(COUNTERS)}
 
     def close(self):
+        """Frees the evaluator's device memory and its native context (with
+        the context's scratch, e.g. the serving loop's mcdisk line cubes)."""
         if getattr(self, 'handle', None):
             _lib.gbkb200_batch_destroy(self.handle)
             self.handle = None
+        ctx = getattr(self, 'ctx', None)
+        if ctx is not None:
+            ctx.close()
 
     def __del__(self):
         try:
