@@ -312,3 +312,21 @@ def test_batched_model_variant_identical(gpu, nodewise):
     for o in out[1:]:
         assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
     assert np.all(out[0][0] > 0)
+
+
+def test_batched_evaluate_pieces_identical(gpu):
+    """End-to-end evaluate() in one, two (the default from 256 sets) or three
+    pieces, smaller than a chunk or not: the same chi^2, bit for bit, as the
+    device-resident evaluation."""
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    n = 300
+    w = _small_batch_workload(n)
+    data, err, _ = synthetic_data(w)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=n, chunk=128, conv='direct')
+    bufs = ev.alloc_inputs(n)
+    ev.upload(ev.pack(w.params, n), bufs, n)
+    ref = ev.evaluate_device(bufs, n).cpu().numpy().copy()
+    for pieces in (None, 1, 3):
+        got = ev.evaluate(w.params, n, pieces=pieces)
+        assert np.array_equal(got, ref), pieces
+    ev.close()
