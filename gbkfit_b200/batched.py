@@ -297,9 +297,27 @@ class BatchedSMDisk:
     # ---- asynchronous groups (serving) ----------------------------------------
     def pack_one(self, params):
         """One parameter set (host dict) -> {name: float32 row} in the layout
-        of the evaluator's inputs (what pack() gives for one set)."""
-        one = {k: np.asarray(v)[None] for k, v in params.items()}
-        return {k: v[0] for k, v in self.pack(one, 1).items() if v.size}
+        of the evaluator's inputs: the values pack() gives for one set, filled
+        from a per-disk plan of the rows (the serving loop packs every
+        request with it)."""
+        plan = getattr(self, '_row_plan', None)
+        if plan is None:
+            plan = self._row_plan = row_plan(self.disk)
+        out = {}
+        for name, entries, width in plan:
+            row = np.empty(width, np.float32)
+            off = 0
+            for pname, size, nw, interp in entries:
+                v = params[pname]
+                if nw:
+                    vals = interp(np.asarray(v, np.float64)[None])[0]
+                    n = vals.shape[0]
+                else:
+                    vals, n = np.asarray(v, np.float64).reshape(size), size
+                row[off:off + n] = vals
+                off += n
+            out[name] = row
+        return out
 
     def _submit_args(self):
         """The per-evaluator arguments of gbkb200_batch_submit (built once):
@@ -441,6 +459,33 @@ class _Done:
     def query(self):
         check(_lib.gbkb200_batch_query(self._ev.handle, ctypes.byref(self._flag)), 'batch_query')
         return bool(self._flag.value)
+
+
+def row_plan(disk):
+    """The per-set input rows of a disk's batched evaluation: [(name,
+    [(parameter, size, node-wise, interpolation), ...], row width)] for the
+    common parameters and each kind's trait parameters, in Disk.pack_batch's
+    order; node-wise values go through the same node -> sub-node
+    interpolation as pack_batch for one set."""
+    from .disk import _interp, _linear_matrix
+    if disk.interp == 'linear':
+        # pack_batch's linear interpolation of a batch: y @ W, W fixed per disk
+        W = _linear_matrix(disk.rnodes, disk.subrnodes)
+        interp = lambda y: y @ W
+    else:
+        interp = lambda y: _interp(disk.interp, disk.rnodes, y, disk.subrnodes)
+    plan = []
+    for name in ('vsys', 'xpos', 'ypos', 'posa', 'incl'):
+        if name in disk.pdescs:
+            nw = disk.pdescs[name][1]
+            plan.append((name, [(name, 1, nw, interp)], disk.common_size(name)))
+    for kind in KINDS:
+        tab = disk.tables[kind]
+        if tab is None or not tab['npv']:
+            continue
+        plan.append((kind, [(pname, size, nw, interp) for pname, size, nw in tab['plist']],
+                     tab['npv']))
+    return plan
 
 
 def synthetic_data(w, device=0, seed=None):

@@ -79,3 +79,40 @@ def test_request_blob_and_argument_block():
         else:
             assert a.kind == 0 and a.off_csum == -1 and a.off_hasordint == -1
     assert kinds == {'smdisk', 'mcdisk'}
+
+
+def test_pack_one_plan_equals_pack():
+    """BatchedSMDisk.pack_one (filled from a per-disk row plan) gives the rows
+    of pack() for one set, value for value, for node-wise, smooth, mixture,
+    loose and tilted disks."""
+    from gbkfit_b200 import traits as T
+    from gbkfit_b200.batched import BatchedSMDisk
+    from gbkfit_b200.disk import Disk
+    from tests import trait_catalogue as C
+
+    class _Ev:
+        def __init__(self, disk):
+            self.disk = disk
+
+    disks = []
+    disks.append(Disk(True, True, C.RNODES, traits=dict(
+        rpt=[T.bpt('exponential'), T.bpt('mixture_gauss', nblobs=2)],
+        vpt=[T.vpt('tan_arctan')], dpt=[T.dpt('nw_uniform')])))
+    cases = [c for c in C.cases() if not c[3]][:12]
+    items = [(d, C._params(d)) for d in [C.disk_of(c) for c in cases]]
+    for d in disks:                     # loose and tilted: node-wise centre and angles
+        params = C._params(d)
+        params.update({k: np.full(len(C.RNODES), float(params[k]) + 0.1 * i)
+                       for i, k in enumerate(('vsys', 'xpos', 'ypos', 'posa', 'incl'))})
+        items.append((d, params))
+    st = _stream()
+    items += [(st.datasets[q['dataset']]['smdisk'], q['params']) for q in st.requests
+              if q['kind'] == 'smdisk']
+    for d, params in items:
+        ev = _Ev(d)
+        one = {k: np.asarray(v)[None] for k, v in params.items()}
+        ref = {k: v[0] for k, v in BatchedSMDisk.pack(ev, one, 1).items() if v.size}
+        got = BatchedSMDisk.pack_one(ev, params)
+        assert sorted(got) == sorted(ref)
+        for k in ref:
+            assert got[k].dtype == np.float32 and np.array_equal(got[k], ref[k]), k
