@@ -326,3 +326,46 @@ def test_mcdisk_deterministic_mode(be, oracle_built):
         assert rel_err(fast[k], a[k]) <= 1e-4, (k, rel_err(fast[k], a[k]))
     assert rel_err(fast['scube'], a['scube']) <= 1e-5
     assert abs(a['scube'].sum() - fast['scube'].sum()) <= 1e-5 * abs(a['scube'].sum())
+
+
+def test_mcdisk_dense_clouds_replicated_scratch(be, oracle_built):
+    """Dense clouds (over 1,000 per spaxel on the 64x64 padded grid of a
+    48x48 cube): the fast mode's
+    line scratch is replicated 8 times (gbkb200_mcdisk_scratch_bytes) and the
+    copies are summed by the transpose-add; the cube and maps agree with the
+    deterministic mode and with one atomic per channel (mode 3)."""
+    import torch
+    from gbkfit_b200 import _native, psflsf, workloads
+    w = workloads.mcdisk_cube256(nclouds=3_000_000)
+    w.geom = workloads.Geometry((48, 48, 32), (1, 1, 10), (0, 0, 15.5), (0, 0, 0),
+                                psflsf.PSFGauss(1.0), w.geom.lsf)
+    w.params = dict(w.params, xpos=24.0, ypos=24.0, bpt_s=6.0)
+    w.disk = workloads.Disk(False, False, np.linspace(0, 30, 21), traits=w.disk.traits)
+    cflux = 4.8e-5                    # about 4.5e6 clouds, 1,100 per spaxel
+    csum = w.disk.ncloudscsum(w.params, cflux)
+    n = int(csum[-1])
+    hoi = w.disk.hasordint()
+    g = w.geometry_args(spat_z=32)
+    nx, ny, sz = g['spat_size']
+    nz = g['spec_size']
+    copies = _native.lib().gbkb200_mcdisk_scratch_bytes(n, nx, ny, nz) // (
+        nx * ny * ((nz + 3) // 4 * 4) * 4)
+    assert copies == 8, (n, copies)
+    pd = upload(w.disk.pack(w.params), 'cuda')
+
+    def run(mode):
+        be['gmodel'].set_mcdisk(seed=11, mode=mode)
+        outs = dict(scube=torch.zeros((nz, ny, nx), device='cuda'),
+                    rdata=torch.zeros((sz, ny, nx), device='cuda'))
+        gpu_mcdisk(be['gmodel'], cflux, n, torch.from_numpy(csum).cuda(),
+                   torch.from_numpy(hoi).cuda(), pd, g, outs)
+        return {k: v.cpu().numpy() for k, v in outs.items()}
+
+    fast, det, scalar = run(0), run(1), run(3)
+    be['gmodel'].set_mcdisk(seed=42, mode=0)
+    assert det['scube'].sum() > 0
+    for o in (fast, scalar):
+        assert rel_err(o['scube'], det['scube']) <= 1e-5
+        assert rel_err(o['rdata'], det['rdata']) <= 1e-4
+    assert abs(fast['scube'].astype(np.float64).sum() - det['scube'].astype(np.float64).sum()) \
+        <= 1e-5 * det['scube'].astype(np.float64).sum()
