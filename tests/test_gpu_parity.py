@@ -330,10 +330,10 @@ def test_mcdisk_deterministic_mode(be, oracle_built):
 
 def test_mcdisk_dense_clouds_replicated_scratch(be, oracle_built):
     """Dense clouds (over 1,000 per spaxel on the 64x64 padded grid of a
-    48x48 cube): the fast mode's
-    line scratch is replicated 8 times (gbkb200_mcdisk_scratch_bytes) and the
-    copies are summed by the transpose-add; the cube and maps agree with the
-    deterministic mode and with one atomic per channel (mode 3)."""
+    48x48 cube): the fast mode's line scratch is replicated 8 times
+    (gbkb200_mcdisk_scratch_bytes) and the copies are summed by the
+    transpose-add; the cube and maps agree with the deterministic mode and
+    with one atomic per channel (mode 3)."""
     import torch
     from gbkfit_b200 import _native, psflsf, workloads
     w = workloads.mcdisk_cube256(nclouds=3_000_000)
