@@ -69,7 +69,6 @@ def direct_flops_per_eval(geom):
 NCU_DRAM_BYTES_PER_SET = {
     'kb_psf_residual': 289.1e6 / 128,
     'ka_lines_lsf': 211.5e6 / 128,
-    'k_xr_transpose': 36.5e6 / 128,
 }
 
 # FLOPs of one residual voxel computed from the model: (m - d), x w, r^2 sum
@@ -389,7 +388,7 @@ def run_b200(args):
     out = None
     if rank == 0:
         n_chunks = (nsets + ev.chunk - 1) // ev.chunk
-        per_chunk = 3 if ev.conv_mode == 'direct' else 5
+        per_chunk = 2 if ev.conv_mode == 'direct' else 5
         plain = plain_per_call(w, data, err) if args.plain else None
         serving = serving_run() if args.serving else None
         cpu = cpu_baseline(w, data, err) if args.cpu_baseline else None

@@ -71,7 +71,7 @@ COUNTERS = ('lsf_fma', 'lines', 'psf_x_fma', 'psf_y_fma', 'residual_voxels', 'sp
 
 # per-stage kernel names of gbkb200_batch_timing, by convolution mode
 STAGE_KERNELS = {
-    'direct': {0: 'ka_lines_lsf', 1: 'k_xr_transpose', 4: 'kb_psf_residual', 5: 'k6_sum'},
+    'direct': {0: 'ka_lines_lsf', 4: 'kb_psf_residual', 5: 'k6_sum'},
     'fft': {0: 'k1_model_xfft', 1: 'k_lines (y forward)', 2: 'k_lines (z convolution)',
             3: 'k_lines (y inverse)', 4: 'k5_c2r_residual', 5: 'k6_sum'},
 }

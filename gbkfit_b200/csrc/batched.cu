@@ -35,29 +35,6 @@
 
 namespace gbk {
 
-// The model kernel's range table (row chunk-major, written per warp) to the
-// plane-major layout the PSF kernel reads: a 32 x 32 tiled transpose per set.
-__global__ void __launch_bounds__(256) k_xr_transpose(const int* __restrict__ src,
-                                                      int* __restrict__ dst, int R, int Nz)
-{
-    __shared__ int tile[32][33];
-    const int c = blockIdx.z, r0 = blockIdx.x * 32, z0 = blockIdx.y * 32;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int* s = src + (long long)c * R * Nz;
-    int* d = dst + (long long)c * Nz * R;
-#pragma unroll
-    for (int k = 0; k < 32; k += 8) {
-        const int r = r0 + ty + k, z = z0 + tx;
-        if (r < R && z < Nz) tile[ty + k][tx] = s[(long long)r * Nz + z];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 32; k += 8) {
-        const int z = z0 + ty + k, r = r0 + tx;
-        if (r < R && z < Nz) d[(long long)z * R + r] = tile[tx][ty + k];
-    }
-}
-
 // per-voxel residual factor of the direct path: mask * weight / error
 __global__ void k_iw(BatchKernelArgs P, float* iw, long long n)
 {
@@ -371,7 +348,6 @@ struct gbkb200_batch {
     cudaEvent_t done = nullptr;       // recorded at the end of an asynchronous submission
     size_t smemB = 0;
     float* mplanes = nullptr;
-    int* xr = nullptr;
     int* xrt = nullptr;
     double* sat = nullptr;
     float* iw = nullptr;
@@ -561,14 +537,12 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
         P.ur2[i] = make_float2(P.ur[i], P.ur[i]);
     }
     if (cudaMalloc(&bt->mplanes, nrows * P.pitch * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&bt->xr, nrows * P.nch * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&bt->xrt, nrows * P.nch * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&bt->sat, (size_t)P.Nz * (P.Ny + 1) * (P.Nx + 1) * sizeof(double)) !=
             cudaSuccess ||
         cudaMalloc(&bt->iw, (size_t)P.Nz * P.Ny * P.Nx * sizeof(float)) != cudaSuccess)
         return GBKB200_ERR_OOM;
     P.mplanes = bt->mplanes;
-    P.xr = bt->xr;
     P.xrt = bt->xrt;
     P.sat = bt->sat;
     P.iw = bt->iw;
@@ -653,7 +627,6 @@ extern "C" int gbkb200_batch_destroy(gbkb200_batch* bt)
     cudaFree(bt->work);
     cudaFree(bt->partials);
     cudaFree(bt->mplanes);
-    cudaFree(bt->xr);
     cudaFree(bt->xrt);
     cudaFree(bt->sat);
     cudaFree(bt->iw);
@@ -848,7 +821,7 @@ extern "C" int gbkb200_batch_info(const gbkb200_batch* bt, int fft_size[3], int*
         size_t b = (size_t)bt->max_sets * bt->nper * sizeof(double);
         if (bt->direct) {
             const size_t nrows = (size_t)bt->chunk * P.Nz * P.Wy;
-            b += nrows * P.pitch * sizeof(float) + 2 * nrows * P.nch * sizeof(int) +
+            b += nrows * P.pitch * sizeof(float) + nrows * P.nch * sizeof(int) +
                  (size_t)P.Nz * (P.Ny + 1) * (P.Nx + 1) * sizeof(double) +
                  (size_t)P.Nz * P.Ny * P.Nx * sizeof(float);
         } else {
@@ -894,13 +867,6 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
             bt->ka<<<dim3((items + KA_THREADS / 32 - 1) / (KA_THREADS / 32), cn), KA_THREADS, 0,
                      st>>>(P, bt->ctx->d_status);
             stage_mark(bt, 0, false);
-            stage_mark(bt, 1, true);
-            {
-                const int R = P.Wy * P.nch;
-                k_xr_transpose<<<dim3((R + 31) / 32, (P.Nz + 31) / 32, cn), 256, 0, st>>>(
-                    P.xr, P.xrt, R, P.Nz);
-            }
-            stage_mark(bt, 1, false);
             stage_mark(bt, 4, true);
             launch_kb(bt, P, cn, st);
             stage_mark(bt, 4, false);
@@ -978,13 +944,6 @@ extern "C" int gbkb200_batch_evaluate_cubes(gbkb200_batch* bt, int nsets, const 
         kc<<<dim3((P.Wy * P.nch + KA_THREADS / 32 - 1) / (KA_THREADS / 32), cn), KA_THREADS, 0,
              st>>>(P, cubes);
         stage_mark(bt, 0, false);
-        stage_mark(bt, 1, true);
-        {
-            const int R = P.Wy * P.nch;
-            k_xr_transpose<<<dim3((R + 31) / 32, (P.Nz + 31) / 32, cn), 256, 0, st>>>(
-                P.xr, P.xrt, R, P.Nz);
-        }
-        stage_mark(bt, 1, false);
         stage_mark(bt, 4, true);
         launch_kb(bt, P, cn, st);
         stage_mark(bt, 4, false);

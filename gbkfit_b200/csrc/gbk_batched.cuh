@@ -47,9 +47,9 @@ struct BatchKernelArgs {
     float* mplanes;       // (chunk, Nz, Wy, pitch): written where xr is not empty
     int nch;              // 32-column chunks per window row, ceil(Wx / 32)
     int nwfast;           // the disk's traits are exactly rpt/vpt/dpt uid 101 (smdisk_spaxel_nw)
-    int* xr;              // (chunk, Wy, nch, Nz): nonzero x range (xmin | xmax << 16) of
-                          // each plane row chunk (4-aligned around it is written), or -1
-    int* xrt;             // (chunk, Nz, Wy, nch): the same, plane-major (read by the PSF kernel)
+    int* xrt;             // (chunk, Nz, Wy, nch): nonzero x range (xmin | xmax << 16) of
+                          // each plane row chunk (4-aligned around it is written), or -1;
+                          // written by the model kernel, read by the PSF kernel
     const double* sat;    // (Nz, Ny + 1, Nx + 1): summed-area table of the zero-model r^2
     // executed-work counters (null unless enabled): what the direct-mode kernels
     // actually compute, for the roofline of the measured launches
@@ -157,10 +157,13 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
         zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, s));
         zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, s));
     }
-    int* xr = P.xr + (((long long)c * P.Wy + y) * P.nch + chunk) * P.Nz;
+    // the range table, plane-major (set, plane, row, chunk) as the PSF kernel
+    // reads it: this warp's entry of plane z at xr[z * xs]
+    const long long xs = (long long)P.Wy * P.nch;
+    int* xr = P.xrt + ((long long)c * P.Nz * P.Wy + y) * P.nch + chunk;
     // planes outside [zlo, zhi] are empty for this chunk
     for (int zo = lane; zo < P.Nz; zo += 32)
-        if (zo < zlo || zo > zhi) xr[zo] = -1;
+        if (zo < zlo || zo > zhi) xr[zo * xs] = -1;
     if (zlo <= zhi) {
         float lz[KZ];
 #pragma unroll
@@ -196,9 +199,9 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
                 if (zo == own) mm = m;
                 if (zo == fl) {
                     if (own <= zo)
-                        xr[own] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
-                                        ((chunk * 32 + 31 - __clz(mm)) << 16))
-                                     : -1;
+                        xr[own * xs] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
+                                             ((chunk * 32 + 31 - __clz(mm)) << 16))
+                                          : -1;
                     mz = zo + 1;
                     own = mz + lane;
                     fl = min(mz + 31, zhi);
@@ -802,12 +805,14 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 5 : 4)) ka_lines_lsf2(
         zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, s));
         zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, s));
     }
-    int* xr0 = P.xr + (((long long)c * P.Wy + y) * P.nch + c0) * P.Nz;
-    int* xr1 = xr0 + P.Nz;                                // chunk c1 (used when has1)
+    // the range table, plane-major: the chunks' entries of plane z at [z * xs]
+    const long long xs = (long long)P.Wy * P.nch;
+    int* xr0 = P.xrt + ((long long)c * P.Nz * P.Wy + y) * P.nch + c0;
+    int* xr1 = xr0 + 1;                                   // chunk c1 (used when has1)
     for (int zo = lane; zo < P.Nz; zo += 32)
         if (zo < zlo || zo > zhi) {
-            xr0[zo] = -1;
-            if (has1) xr1[zo] = -1;
+            xr0[zo * xs] = -1;
+            if (has1) xr1[zo * xs] = -1;
         }
     if (zlo <= zhi) {
         float2 lz[KZ];
@@ -848,13 +853,13 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 5 : 4)) ka_lines_lsf2(
                 }
                 if (zo == fl) {
                     if (own <= zo) {
-                        xr0[own] = mm0 ? ((c0 * 32 + __ffs(mm0) - 1) |
-                                          ((c0 * 32 + 31 - __clz(mm0)) << 16))
-                                       : -1;
+                        xr0[own * xs] = mm0 ? ((c0 * 32 + __ffs(mm0) - 1) |
+                                               ((c0 * 32 + 31 - __clz(mm0)) << 16))
+                                            : -1;
                         if (has1)
-                            xr1[own] = mm1 ? ((c1 * 32 + __ffs(mm1) - 1) |
-                                              ((c1 * 32 + 31 - __clz(mm1)) << 16))
-                                           : -1;
+                            xr1[own * xs] = mm1 ? ((c1 * 32 + __ffs(mm1) - 1) |
+                                                   ((c1 * 32 + 31 - __clz(mm1)) << 16))
+                                                : -1;
                     }
                     mz = zo + 1;
                     own = mz + lane;
@@ -903,7 +908,9 @@ __global__ void __launch_bounds__(KA_THREADS) kc_cube_lsf(BatchKernelArgs P,
     float w[KZ];
 #pragma unroll
     for (int t = 0; t < KZ - 1; ++t) w[t] = ld(t);
-    int* xr = P.xr + (((long long)c * P.Wy + y) * P.nch + chunk) * P.Nz;
+    // the range table, plane-major: this warp's entry of plane z at xr[z * xs]
+    const long long xs = (long long)P.Wy * P.nch;
+    int* xr = P.xrt + ((long long)c * P.Nz * P.Wy + y) * P.nch + chunk;
     const long long zstride = (long long)P.Wy * P.pitch;
     float* dp = P.mplanes + ((long long)c * P.Nz * P.Wy + y) * P.pitch + x;
     unsigned mm = 0u;
@@ -928,9 +935,9 @@ __global__ void __launch_bounds__(KA_THREADS) kc_cube_lsf(BatchKernelArgs P,
             if ((zo & 31) == 31 || zo == P.Nz - 1) {
                 const int own = (zo & ~31) + lane;
                 if (own <= zo)
-                    xr[own] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
-                                    ((chunk * 32 + 31 - __clz(mm)) << 16))
-                                 : -1;
+                    xr[own * xs] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
+                                         ((chunk * 32 + 31 - __clz(mm)) << 16))
+                                      : -1;
             }
         }
     }

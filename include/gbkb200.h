@@ -424,8 +424,8 @@ int gbkb200_batch_destroy(gbkb200_batch* b);
 /* Per-stage device timing (no reference counterpart; a measurement aid).
  * With timing enabled, evaluate records a CUDA event pair around every kernel
  * launch; do not capture evaluate into a graph while it is enabled.  Stages:
- * 0 model + lines (direct: LSF FIR too; FFT: x r2c), 1 y FFT (direct: the
- * range-table transpose), 2 z FFT convolution, 3 inverse y FFT, 4 PSF FIR or
+ * 0 model + lines (direct: LSF FIR too; FFT: x r2c), 1 y FFT, 2 z FFT
+ * convolution, 3 inverse y FFT (FFT mode only), 4 PSF FIR or
  * x c2r + residual, 5 chi^2 sum.
  * gbkb200_batch_timing synchronizes the stream, returns the summed
  * milliseconds and launch counts per stage since the last call, and resets. */
