@@ -44,12 +44,11 @@ struct BatchKernelArgs {
     float ur[33];         // (K): PSF y factor, reversed, zero-padded
     float lsfr[33];       // (Kz): LSF reversed
     float2 ur2[33];       // (K): ur duplicated into packed pairs (FFMA2 operands)
-    float* mplanes;       // (chunk, Nz, Wy, pitch): row chunks written whole where xrt is not -1
+    float* mplanes;       // (chunk, Nz, Wy, pitch): written where xr is not empty
     int nch;              // 32-column chunks per window row, ceil(Wx / 32)
     int nwfast;           // the disk's traits are exactly rpt/vpt/dpt uid 101 (smdisk_spaxel_nw)
     int* xrt;             // (chunk, Nz, Wy, nch): nonzero x range (xmin | xmax << 16) of
-                          // each plane row chunk (the whole chunk is written, zeros
-                          // outside the range), or -1 (not written);
+                          // each plane row chunk (4-aligned around it is written), or -1;
                           // written by the model kernel, read by the PSF kernel
     const double* sat;    // (Nz, Ny + 1, Nx + 1): summed-area table of the zero-model r^2
     // executed-work counters (null unless enabled): what the direct-mode kernels
@@ -429,11 +428,10 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
                     const int* vrow = s_xr + (y - ob0) * P.nch;
                     float4* d = reinterpret_cast<float4*>(S) + (y - ys) * bp4;
                     const float4* g = src + (long long)y * (P.pitch / 4);
-                    // a row chunk with a range entry was written whole by the
-                    // model kernel (zeros outside its range): copy all of it
                     for (int j = ti; j < nsl; j += tc) {
                         const int sl = sl0 + j, ch = sl >> 3;
-                        if (ch < P.nch && vrow[ch] >= 0)
+                        const int v = ch < P.nch ? vrow[ch] : -1;
+                        if (v >= 0 && sl >= (v & 0xffff) >> 2 && sl <= (v >> 16) >> 2)
                             cp_async16(d + j, g + sl);
                         else
                             d[j] = make_float4(0.f, 0.f, 0.f, 0.f);
