@@ -67,7 +67,7 @@ def direct_flops_per_eval(geom):
 # wave of this workload, divided by 128; a launch of n sets moves about n times
 # this (the traffic grows with the sets processed).  Not measured by this run.
 NCU_DRAM_BYTES_PER_SET = {
-    'kb_psf_residual': 289.1e6 / 128,
+    'kb_psf_residual': 289.5e6 / 128,
     'ka_lines_lsf': 211.5e6 / 128,
 }
 
