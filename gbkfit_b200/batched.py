@@ -241,22 +241,32 @@ class BatchedSMDisk:
         pinned host buffer, copied to the device in one transfer and
         evaluated asynchronously while the next piece is packed; chi^2 comes
         back through a pinned buffer and the call synchronises once.
-        pieces: how many (default: two for 256 sets or more, else one; the
-        second piece's packing overlaps the first's evaluation); a piece
-        smaller than the chunk is evaluated as a smaller wave."""
+        pieces: how many equal pieces, or the sizes of the pieces (default:
+        two for 256 sets or more, else one; the second piece's packing
+        overlaps the first's evaluation); a piece smaller than the chunk is
+        evaluated as a smaller wave."""
         nsets = int(nsets)
         if nsets > self.max_sets:
             raise ValueError(f"nsets {nsets} > max_sets {self.max_sets}")
         if pieces is None:
             pieces = 2 if nsets >= 256 else 1
-        piece = max(1, -(-nsets // int(pieces)))
-        piece = min(self.max_sets, -(-piece // 32) * 32)
-        st = self._e2e_buffers(piece, -(-nsets // piece))
+        if np.ndim(pieces) == 0:
+            piece = max(1, -(-nsets // int(pieces)))
+            piece = min(self.max_sets, -(-piece // 32) * 32)
+            sizes = [min(piece, nsets - lo) for lo in range(0, nsets, piece)] or [0]
+        else:
+            sizes = [int(s) for s in pieces]
+            if sum(sizes) != nsets or min(sizes) < 1:
+                raise ValueError(f"piece sizes {sizes} do not make {nsets} sets")
+        bounds = np.concatenate([[0], np.cumsum(sizes)]).astype(int)
+        st = self._e2e_buffers(max(sizes), len(sizes))
         per_set = {k: (np.ndim(v) > 0 and np.shape(v)[0] == nsets) for k, v in params.items()}
         self.last_h2d_bytes = 0
         with torch.cuda.stream(self.stream):
-            for j, lo in enumerate(range(0, nsets, piece)):
-                hi = min(nsets, lo + piece)
+            for j in range(len(sizes)):
+                lo, hi = int(bounds[j]), int(bounds[j + 1])
+                if hi <= lo:
+                    continue
                 sub = {k: (v[lo:hi] if per_set[k] else v) for k, v in params.items()}
                 hv, hflat, dflat, dv = st['pieces'][j]
                 for name, arr in self.pack(sub, hi - lo).items():

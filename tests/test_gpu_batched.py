@@ -316,8 +316,8 @@ def test_batched_model_variant_identical(gpu, nodewise):
 
 def test_batched_evaluate_pieces_identical(gpu):
     """End-to-end evaluate() in one, two (the default from 256 sets) or three
-    pieces, smaller than a chunk or not: the same chi^2, bit for bit, as the
-    device-resident evaluation."""
+    equal pieces or pieces of given sizes, smaller than a chunk or not: the
+    same chi^2, bit for bit, as the device-resident evaluation."""
     from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
     n = 300
     w = _small_batch_workload(n)
@@ -326,7 +326,7 @@ def test_batched_evaluate_pieces_identical(gpu):
     bufs = ev.alloc_inputs(n)
     ev.upload(ev.pack(w.params, n), bufs, n)
     ref = ev.evaluate_device(bufs, n).cpu().numpy().copy()
-    for pieces in (None, 1, 3):
+    for pieces in (None, 1, 3, (100, 200), (64, 236)):
         got = ev.evaluate(w.params, n, pieces=pieces)
         assert np.array_equal(got, ref), pieces
     ev.close()
