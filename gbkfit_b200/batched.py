@@ -242,14 +242,19 @@ class BatchedSMDisk:
         evaluated asynchronously while the next piece is packed; chi^2 comes
         back through a pinned buffer and the call synchronises once.
         pieces: how many equal pieces, or the sizes of the pieces (default:
-        two for 256 sets or more, else one; the second piece's packing
-        overlaps the first's evaluation); a piece smaller than the chunk is
-        evaluated as a smaller wave."""
+        for 256 sets or more a first piece of an eighth of the sets, at least
+        32, then the rest: the device starts early and the large second
+        piece's packing overlaps the first's evaluation; else one piece); a
+        piece smaller than the chunk is evaluated as a smaller wave."""
         nsets = int(nsets)
         if nsets > self.max_sets:
             raise ValueError(f"nsets {nsets} > max_sets {self.max_sets}")
         if pieces is None:
-            pieces = 2 if nsets >= 256 else 1
+            if nsets >= 256:
+                first = max(32, nsets // 8 // 32 * 32)
+                pieces = (first, nsets - first)
+            else:
+                pieces = 1
         if np.ndim(pieces) == 0:
             piece = max(1, -(-nsets // int(pieces)))
             piece = min(self.max_sets, -(-piece // 32) * 32)
