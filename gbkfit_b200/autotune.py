@@ -122,7 +122,7 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
                 best_d, best_dt = cfg, t
         # the PSF kernel's variants (resident blocks per SM x epilogue)
         base = dict(best_d)
-        for variant in range(1, 7):
+        for variant in range(1, 8):
             cfg = dict(base, psf_variant=variant)
             t = time_config(w, data, err, nsets, cfg)
             if t < best_dt:

@@ -344,6 +344,7 @@ struct gbkb200_batch {
     int trim[3] = {0, 0, 0};          // direct mode: taps trimmed from each end (x, y, z)
     int ka_variant = 0;               // direct mode: the model kernel (model_variant)
     int kb_grid = 0;                  // persistent PSF kernel: blocks of a launch (else 0)
+    int kb_threads = KB_THREADS;      // threads of a PSF-kernel block
     int* kb_work = nullptr;           // persistent PSF kernel: its item counter
     cudaEvent_t done = nullptr;       // recorded at the end of an asynchronous submission
     size_t smemB = 0;
@@ -393,9 +394,9 @@ static void launch_kb(const gbkb200_batch* bt, BatchKernelArgs& P, int cn, cudaS
         const long long items = (long long)cn * P.Nz * P.nbands;
         const int grid = (int)std::min<long long>(items, bt->kb_grid);
         cudaMemsetAsync(bt->kb_work, 0, sizeof(int), st);
-        bt->kb<<<grid, KB_THREADS, bt->smemB, st>>>(P);
+        bt->kb<<<grid, bt->kb_threads, bt->smemB, st>>>(P);
     } else {
-        bt->kb<<<dim3(cn, P.Nz * P.nbands), KB_THREADS, bt->smemB, st>>>(P);
+        bt->kb<<<dim3(cn, P.Nz * P.nbands), bt->kb_threads, bt->smemB, st>>>(P);
     }
 }
 
@@ -433,6 +434,7 @@ static KbFn kb_fn(int K, int variant)
         kb_register4(t);
         kb_register5(t + 3);
         kb_register_pf(t + 6);
+        kb_register_wide(t + 7);
     });
     return t[variant][(K - KB_KMIN) / 2];
 }
@@ -518,8 +520,11 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     // epilogue (variant % 3) as in kb_psf_residual, 6 = 0 as a persistent
     // kernel; shared memory per block: 55 KB for 4 blocks per SM, 43 KB for 5
     if (d->psf_variant < 0 || d->psf_variant >= KB_VARIANTS) return GBKB200_ERR_INVALID_ARG;
+    const bool wide = d->psf_variant == 7;
     const int blocks = (d->psf_variant >= 3 && d->psf_variant <= 5) ? 5 : 4;
-    const long long budget = blocks == 5 ? 43LL * 1024 : 55LL * 1024;
+    // variant 7: 256-thread blocks, two per SM, 110 KB each
+    const long long budget = wide ? 110LL * 1024 : blocks == 5 ? 43LL * 1024 : 55LL * 1024;
+    bt->kb_threads = wide ? 256 : KB_THREADS;
     const long long cap = std::max(need_min, std::min(need_all, (budget - xr_bytes) / 4));
     if (cap * (long long)sizeof(float) + xr_bytes > 227LL * 1024) return GBKB200_ERR_UNSUPPORTED;
     P.cap = (int)cap;
@@ -562,7 +567,7 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
         // one resident wave of blocks
         int per_sm = 0, nsm = 0;
         GBK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, reinterpret_cast<const void*>(bt->kb), KB_THREADS, bt->smemB));
+            &per_sm, reinterpret_cast<const void*>(bt->kb), bt->kb_threads, bt->smemB));
         GBK_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, bt->ctx->device));
         bt->kb_grid = std::max(1, per_sm) * std::max(1, nsm);
         if (cudaMalloc(&bt->kb_work, sizeof(int)) != cudaSuccess) return GBKB200_ERR_OOM;

@@ -7,51 +7,51 @@ namespace gbk {
 
 void kb_register4(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1])
 {
-    t[0][0] = kb_psf_residual<5, 4, 0, false>;
-    t[0][1] = kb_psf_residual<7, 4, 0, false>;
-    t[0][2] = kb_psf_residual<9, 4, 0, false>;
-    t[0][3] = kb_psf_residual<11, 4, 0, false>;
-    t[0][4] = kb_psf_residual<13, 4, 0, false>;
-    t[0][5] = kb_psf_residual<15, 4, 0, false>;
-    t[0][6] = kb_psf_residual<17, 4, 0, false>;
-    t[0][7] = kb_psf_residual<19, 4, 0, false>;
-    t[0][8] = kb_psf_residual<21, 4, 0, false>;
-    t[0][9] = kb_psf_residual<23, 4, 0, false>;
-    t[0][10] = kb_psf_residual<25, 4, 0, false>;
-    t[0][11] = kb_psf_residual<27, 4, 0, false>;
-    t[0][12] = kb_psf_residual<29, 4, 0, false>;
-    t[0][13] = kb_psf_residual<31, 4, 0, false>;
-    t[0][14] = kb_psf_residual<33, 4, 0, false>;
-    t[1][0] = kb_psf_residual<5, 4, 1, false>;
-    t[1][1] = kb_psf_residual<7, 4, 1, false>;
-    t[1][2] = kb_psf_residual<9, 4, 1, false>;
-    t[1][3] = kb_psf_residual<11, 4, 1, false>;
-    t[1][4] = kb_psf_residual<13, 4, 1, false>;
-    t[1][5] = kb_psf_residual<15, 4, 1, false>;
-    t[1][6] = kb_psf_residual<17, 4, 1, false>;
-    t[1][7] = kb_psf_residual<19, 4, 1, false>;
-    t[1][8] = kb_psf_residual<21, 4, 1, false>;
-    t[1][9] = kb_psf_residual<23, 4, 1, false>;
-    t[1][10] = kb_psf_residual<25, 4, 1, false>;
-    t[1][11] = kb_psf_residual<27, 4, 1, false>;
-    t[1][12] = kb_psf_residual<29, 4, 1, false>;
-    t[1][13] = kb_psf_residual<31, 4, 1, false>;
-    t[1][14] = kb_psf_residual<33, 4, 1, false>;
-    t[2][0] = kb_psf_residual<5, 4, 2, false>;
-    t[2][1] = kb_psf_residual<7, 4, 2, false>;
-    t[2][2] = kb_psf_residual<9, 4, 2, false>;
-    t[2][3] = kb_psf_residual<11, 4, 2, false>;
-    t[2][4] = kb_psf_residual<13, 4, 2, false>;
-    t[2][5] = kb_psf_residual<15, 4, 2, false>;
-    t[2][6] = kb_psf_residual<17, 4, 2, false>;
-    t[2][7] = kb_psf_residual<19, 4, 2, false>;
-    t[2][8] = kb_psf_residual<21, 4, 2, false>;
-    t[2][9] = kb_psf_residual<23, 4, 2, false>;
-    t[2][10] = kb_psf_residual<25, 4, 2, false>;
-    t[2][11] = kb_psf_residual<27, 4, 2, false>;
-    t[2][12] = kb_psf_residual<29, 4, 2, false>;
-    t[2][13] = kb_psf_residual<31, 4, 2, false>;
-    t[2][14] = kb_psf_residual<33, 4, 2, false>;
+    t[0][0] = kb_psf_residual<5, 4, 0, false, KB_THREADS>;
+    t[0][1] = kb_psf_residual<7, 4, 0, false, KB_THREADS>;
+    t[0][2] = kb_psf_residual<9, 4, 0, false, KB_THREADS>;
+    t[0][3] = kb_psf_residual<11, 4, 0, false, KB_THREADS>;
+    t[0][4] = kb_psf_residual<13, 4, 0, false, KB_THREADS>;
+    t[0][5] = kb_psf_residual<15, 4, 0, false, KB_THREADS>;
+    t[0][6] = kb_psf_residual<17, 4, 0, false, KB_THREADS>;
+    t[0][7] = kb_psf_residual<19, 4, 0, false, KB_THREADS>;
+    t[0][8] = kb_psf_residual<21, 4, 0, false, KB_THREADS>;
+    t[0][9] = kb_psf_residual<23, 4, 0, false, KB_THREADS>;
+    t[0][10] = kb_psf_residual<25, 4, 0, false, KB_THREADS>;
+    t[0][11] = kb_psf_residual<27, 4, 0, false, KB_THREADS>;
+    t[0][12] = kb_psf_residual<29, 4, 0, false, KB_THREADS>;
+    t[0][13] = kb_psf_residual<31, 4, 0, false, KB_THREADS>;
+    t[0][14] = kb_psf_residual<33, 4, 0, false, KB_THREADS>;
+    t[1][0] = kb_psf_residual<5, 4, 1, false, KB_THREADS>;
+    t[1][1] = kb_psf_residual<7, 4, 1, false, KB_THREADS>;
+    t[1][2] = kb_psf_residual<9, 4, 1, false, KB_THREADS>;
+    t[1][3] = kb_psf_residual<11, 4, 1, false, KB_THREADS>;
+    t[1][4] = kb_psf_residual<13, 4, 1, false, KB_THREADS>;
+    t[1][5] = kb_psf_residual<15, 4, 1, false, KB_THREADS>;
+    t[1][6] = kb_psf_residual<17, 4, 1, false, KB_THREADS>;
+    t[1][7] = kb_psf_residual<19, 4, 1, false, KB_THREADS>;
+    t[1][8] = kb_psf_residual<21, 4, 1, false, KB_THREADS>;
+    t[1][9] = kb_psf_residual<23, 4, 1, false, KB_THREADS>;
+    t[1][10] = kb_psf_residual<25, 4, 1, false, KB_THREADS>;
+    t[1][11] = kb_psf_residual<27, 4, 1, false, KB_THREADS>;
+    t[1][12] = kb_psf_residual<29, 4, 1, false, KB_THREADS>;
+    t[1][13] = kb_psf_residual<31, 4, 1, false, KB_THREADS>;
+    t[1][14] = kb_psf_residual<33, 4, 1, false, KB_THREADS>;
+    t[2][0] = kb_psf_residual<5, 4, 2, false, KB_THREADS>;
+    t[2][1] = kb_psf_residual<7, 4, 2, false, KB_THREADS>;
+    t[2][2] = kb_psf_residual<9, 4, 2, false, KB_THREADS>;
+    t[2][3] = kb_psf_residual<11, 4, 2, false, KB_THREADS>;
+    t[2][4] = kb_psf_residual<13, 4, 2, false, KB_THREADS>;
+    t[2][5] = kb_psf_residual<15, 4, 2, false, KB_THREADS>;
+    t[2][6] = kb_psf_residual<17, 4, 2, false, KB_THREADS>;
+    t[2][7] = kb_psf_residual<19, 4, 2, false, KB_THREADS>;
+    t[2][8] = kb_psf_residual<21, 4, 2, false, KB_THREADS>;
+    t[2][9] = kb_psf_residual<23, 4, 2, false, KB_THREADS>;
+    t[2][10] = kb_psf_residual<25, 4, 2, false, KB_THREADS>;
+    t[2][11] = kb_psf_residual<27, 4, 2, false, KB_THREADS>;
+    t[2][12] = kb_psf_residual<29, 4, 2, false, KB_THREADS>;
+    t[2][13] = kb_psf_residual<31, 4, 2, false, KB_THREADS>;
+    t[2][14] = kb_psf_residual<33, 4, 2, false, KB_THREADS>;
 }
 
 }  // namespace gbk

@@ -267,11 +267,11 @@ constexpr int KB_NX_MAX = 512;  // widest data cube of the direct mode
 // pass's rows reading shared memory; 1: the residual in each y-FIR item's
 // epilogue (no write-back, no barriers between items), its data loaded after
 // the item's FIR; 2: as 1, with the item's data requested before its FIR.
-template<int K, int MINB, int EPI, bool PF>
-__global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelArgs P)
+template<int K, int MINB, int EPI, bool PF, int NT>
+__global__ void __launch_bounds__(NT, MINB) kb_psf_residual(BatchKernelArgs P)
 {
     constexpr int NW = (K + 7 + 3) / 4;     // float4 slots of one 8-output x window
-    constexpr int NWARPS = KB_THREADS / 32;
+    constexpr int NWARPS = NT / 32;
     extern __shared__ float4 sm4[];
     float* S = reinterpret_cast<float*>(sm4);                   // (rows of a pass, bp)
     // (in1 - ob0, nch) range entries of an item; PF: two buffers of xr_slot ints
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
         const int* src;
         int n, o;
         entries(it, src, n, o);
-        for (int i = threadIdx.x; i < n; i += KB_THREADS) cp_async4(dst + i, src + i);
+        for (int i = threadIdx.x; i < n; i += NT) cp_async4(dst + i, src + i);
     };
     __shared__ int s_next;
     int buf = 0, it = 0;
@@ -339,11 +339,11 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
         // (PF: already in s_xr)
         const int* src = xr + ob0 * P.nch;
         const int n = (in1 - ob0) * P.nch;
-        for (int i0 = 0; i0 < n; i0 += 8 * KB_THREADS) {
+        for (int i0 = 0; i0 < n; i0 += 8 * NT) {
             int v[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                const int i = i0 + u * KB_THREADS + threadIdx.x;
+                const int i = i0 + u * NT + threadIdx.x;
                 if (PF) {
                     v[u] = i < n ? s_xr[i] : -1;
                 } else {
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 if (v[u] >= 0) {
-                    const int y = ob0 + (i0 + u * KB_THREADS + (int)threadIdx.x) / P.nch;
+                    const int y = ob0 + (i0 + u * NT + (int)threadIdx.x) / P.nch;
                     y0 = min(y0, y);
                     y1 = max(y1, y);
                     x0 = min(x0, v[u] & 0xffff);
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     if (y1 < 0) {   // nothing reaches this band: the model is 0 on it
         if (model)
             for (long long i = (long long)ob0 * P.Nx + threadIdx.x; i < (long long)ob1 * P.Nx;
-                 i += KB_THREADS)
+                 i += NT)
                 model[i] = 0.f;
         if (threadIdx.x == 0) P.partials[part] = sat_box(T, ld, ob0, ob1, 0, P.Nx);
         break;
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
         }
         // load rows [ly0, ly1]: each row chunk's nonzero range, zeros elsewhere
         if (ly0 <= ly1) {
-            const int tc = min(nsl, KB_THREADS), tr = KB_THREADS / tc;
+            const int tc = min(nsl, NT), tr = NT / tc;
             const int ti = threadIdx.x % tc, ty = threadIdx.x / tc;
             if (ty < tr) {
                 for (int y = ly0 + ty; y <= ly1; y += tr) {
@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
         }
         // the other rows that the y FIR reads: zeros in its strips
         {
-            const int tc = min(ns4, KB_THREADS), tr = KB_THREADS / tc;
+            const int tc = min(ns4, NT), tr = NT / tc;
             const int ti = threadIdx.x % tc, ty = threadIdx.x / tc;
             if (ty < tr) {
                 for (int y = ys + ty; y < rend; y += tr) {
@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
             // y FIR in place: model(yo, xo) = sum_t ur[t] S[yo + t][xo], written to S row yo.
             // Packed FP32 pairs (FFMA2: two lanes of fma, each rounded as fmaf),
             // columns (x, x+1) and (x+2, x+3) of a float4 per instruction.  Items
-            // (8-row group, float4 column) in ascending order, KB_THREADS x kIt
+            // (8-row group, float4 column) in ascending order, NT x kIt
             // per round, loads before the round's barrier and stores after it: a
             // column's group is written only after every lower group of that
             // column, the only readers of its rows, has loaded them.
@@ -516,11 +516,11 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     #pragma unroll
                 for (int t = 0; t < K; ++t) u2[t] = make_float2(P.ur[t], P.ur[t]);
                 const int nitems = ng * ns4;
-                for (int gr0 = 0; gr0 < nitems; gr0 += KB_THREADS * kIt) {
+                for (int gr0 = 0; gr0 < nitems; gr0 += NT * kIt) {
                     float2 acc[kIt][8][2];
     #pragma unroll
                     for (int it = 0; it < kIt; ++it) {
-                        const int item = gr0 + threadIdx.x + it * KB_THREADS;
+                        const int item = gr0 + threadIdx.x + it * NT;
     #pragma unroll
                         for (int q = 0; q < 8; ++q) {
                             acc[it][q][0] = make_float2(0.f, 0.f);
@@ -547,7 +547,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
                     __syncthreads();
     #pragma unroll
                     for (int it = 0; it < kIt; ++it) {
-                        const int item = gr0 + threadIdx.x + it * KB_THREADS;
+                        const int item = gr0 + threadIdx.x + it * NT;
                         if (item < nitems) {
                             const int rb = 8 * (item / ns4), s4 = item % ns4;
     #pragma unroll
@@ -566,14 +566,14 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
                 // flat float4 index over the pass, stepped without divisions
                 const int nv = (xb_end - xb0) >> 2;        // xb0 and xb_end are multiples of 4
                 const int n = (ye - ys) * nv;
-                const int dq = KB_THREADS / nv, dr = KB_THREADS % nv;
+                const int dq = NT / nv, dr = NT % nv;
                 int row = threadIdx.x / nv, col = threadIdx.x % nv;
                 // running offsets: si in S (float4), vi in the data plane (float)
                 int si = row * bp4 + col, vi = pbase + (ys + row) * P.Nx + xb0 + 4 * col;
                 const int dsi = dq * bp4 + dr, dvi = dq * P.Nx + 4 * dr;
                 float2 s2 = make_float2(0.f, 0.f);
     #pragma unroll 4
-                for (int i = threadIdx.x; i < n; i += KB_THREADS) {
+                for (int i = threadIdx.x; i < n; i += NT) {
                     const float4 m = reinterpret_cast<const float4*>(S)[si];
                     const float4 o = *reinterpret_cast<const float4*>(P.obs + vi);
                     const float4 w = *reinterpret_cast<const float4*>(P.iw + vi);
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
                 sum += s2.x + s2.y;
             } else {
                 const int nw = xb_end - xb0, n = (ye - ys) * nw;
-                for (int i = threadIdx.x; i < n; i += KB_THREADS) {
+                for (int i = threadIdx.x; i < n; i += NT) {
                     const int row = i / nw, col = i % nw;
                     const int yo = ys + row, xo = xb0 + col;
                     const float m = S[row * bp + col];
@@ -620,7 +620,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
                 const int nitems = ng * ns4;
                 const bool vec = (P.Nx & 3) == 0;
                 float2 s2 = make_float2(0.f, 0.f);
-                for (int item = threadIdx.x; item < nitems; item += KB_THREADS) {
+                for (int item = threadIdx.x; item < nitems; item += NT) {
                     const int rb = 8 * (item / ns4), s4 = item % ns4;
                     float2 acc[8][2];
     #pragma unroll
@@ -712,7 +712,7 @@ __global__ void __launch_bounds__(KB_THREADS, MINB) kb_psf_residual(BatchKernelA
     if (model) {
         const int bw = P.Nx;
         for (long long i = (long long)ob0 * bw + threadIdx.x; i < (long long)ob1 * bw;
-             i += KB_THREADS) {
+             i += NT) {
             const int yo = (int)(i / bw), xo = (int)(i % bw);
             if (yo < yo_lo || yo >= yb_end || xo < xb0 || xo >= xb_end) model[i] = 0.f;
         }
@@ -959,10 +959,12 @@ void ka2_register(KaFn* t);
 typedef void (*KcFn)(BatchKernelArgs, const float*);
 void kc_register(KcFn* t);
 // t[v][(K - KB_KMIN) / 2] for the PSF kernel variant v = 3 * (MINB == 5) + EPI
-// (v = 6: MINB 4, EPI 0, persistent with prefetched range entries)
-constexpr int KB_VARIANTS = 7;
+// (v = 6: MINB 4, EPI 0, persistent with prefetched range entries; v = 7:
+// 256-thread blocks, MINB 2, EPI 0)
+constexpr int KB_VARIANTS = 8;
 void kb_register4(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1]);   // MINB 4, EPI 0-2
 void kb_register5(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1]);   // MINB 5, EPI 0-2
 void kb_register_pf(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1]); // MINB 4, EPI 0, persistent
+void kb_register_wide(KbFn (*t)[(KB_KMAX - KB_KMIN) / 2 + 1]); // 256 threads, MINB 2, EPI 0
 
 }  // namespace gbk

@@ -363,12 +363,14 @@ typedef struct {
     const double* psf_u;    /* host: (psf_rank, kernel_size[1]) */
     const double* psf_v;    /* host: (psf_rank, kernel_size[0]) */
     int psf_band;           /* direct mode: output rows per PSF block (0 = automatic) */
-    int psf_variant;        /* direct mode: PSF kernel variant 0-6: resident blocks per SM
+    int psf_variant;        /* direct mode: PSF kernel variant 0-7: resident blocks per SM
                              * (0-2: 4, 3-5: 5) x epilogue (variant % 3: 0 residual pass,
                              * 1 residual in the y-FIR items, 2 as 1 with the data
                              * prefetched); 6 = 0 as a persistent kernel (one resident
                              * wave of blocks over all items, each item's range entries
-                             * copied in while the previous item runs); 0 = the first */
+                             * copied in while the previous item runs); 7 = 0 on
+                             * 256-thread blocks with twice the shared memory (2 blocks
+                             * per SM); 0 = the first */
     int model_variant;      /* direct mode, the model kernel (both give the same values):
                              * 0 = a warp per 32-column chunk stepping every lane through
                              * the union of the lanes' channel windows; 1 = two chunks per

@@ -91,7 +91,8 @@ def test_headline_set_vs_fp64_oracle(headline, oracle_built, i):
                                  dict(chunk=512, band=64, psf_variant=2),
                                  dict(chunk=512, model_variant=1),
                                  dict(chunk=512, psf_variant=6), dict(chunk=512, band=48, psf_variant=6),
-                                 dict(chunk=128, psf_variant=6)])
+                                 dict(chunk=128, psf_variant=6), dict(chunk=512, psf_variant=7),
+                                 dict(chunk=512, band=48, psf_variant=7)])
 def test_headline_tuner_shapes_agree(headline, cfg):
     """The other direct-mode shapes of the autotuner's search give the same
     results: chi^2 of all 512 sets within 1e-6 relative, sampled cubes
