@@ -465,6 +465,9 @@ class ModelServer:
 
     # ---- scheduler -------------------------------------------------------------
     SCAN = 64   # queued requests the scheduler looks at per pass
+    # clouds of one coalesced mcdisk launch at most (beyond its first
+    # request): the launch's requests all complete with its slowest splat
+    MC_GROUP_CLOUDS = 15_000_000
 
     def _run(self):
         try:
@@ -525,11 +528,15 @@ class ModelServer:
                     cube = req.cube
                     cap = ds.mc_sets if cube else ds.batched.max_sets
                     group = [i]
+                    clouds = req.nclouds if cube else 0
                     for j in range(i + 1, len(q)):
                         if len(group) >= cap:
                             break
                         if j not in taken and q[j].ds is ds and q[j].cube == cube and (
                                 cube or q[j].rows is not None):
+                            if cube and clouds + q[j].nclouds > self.MC_GROUP_CLOUDS:
+                                continue
+                            clouds += q[j].nclouds if cube else 0
                             group.append(j)
                     taken.update(group)
                     launches.append((ds, 'group', [q[j] for j in group]))
