@@ -410,6 +410,14 @@ static KaFn ka_fn(int Kz)
     return t[Kz / 2];
 }
 
+static KaFn ka_t_fn(int Kz)
+{
+    static KaFn t[KA_KMAX / 2 + 1] = {};
+    static std::once_flag once;
+    std::call_once(once, [] { ka_t_register(t); });
+    return t[Kz / 2];
+}
+
 static KaFn ka2_fn(int Kz)
 {
     static KaFn t[KA_KMAX / 2 + 1] = {};
@@ -555,8 +563,11 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     k_iw<<<592, 256, 0, bt->ctx->stream>>>(P, bt->iw, (long long)P.Nz * P.Ny * P.Nx);
     GBK_CUDA_TRY(cudaGetLastError());
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
-    if (d->model_variant != 0 && d->model_variant != 1) return GBKB200_ERR_INVALID_ARG;
-    bt->ka = d->model_variant == 1 ? ka2_fn(P.Kz) : ka_fn(P.Kz);
+    if (d->model_variant < 0 || d->model_variant > 2) return GBKB200_ERR_INVALID_ARG;
+    // variant 2 keeps a plane's entries of its 4 rows in shared memory
+    if (d->model_variant == 2 && (long long)P.Nz * 16 > 32 * 1024) return GBKB200_ERR_UNSUPPORTED;
+    bt->ka = d->model_variant == 1 ? ka2_fn(P.Kz) : d->model_variant == 2 ? ka_t_fn(P.Kz)
+                                                                         : ka_fn(P.Kz);
     bt->ka_variant = d->model_variant;
     bt->kb = kb_fn(P.K, d->psf_variant);
     {
@@ -868,9 +879,12 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
             const int cn = std::min(bt->chunk, nsets - s0);
             P.set0 = s0;
             stage_mark(bt, 0, true);
+            // variant 2: a block per (4 rows, chunk); otherwise a warp per item
             const int items = P.Wy * (bt->ka_variant == 1 ? (P.nch + 1) / 2 : P.nch);
-            bt->ka<<<dim3((items + KA_THREADS / 32 - 1) / (KA_THREADS / 32), cn), KA_THREADS, 0,
-                     st>>>(P, bt->ctx->d_status);
+            const int blocks = bt->ka_variant == 2 ? (P.Wy + 3) / 4 * P.nch
+                                                   : (items + KA_THREADS / 32 - 1) / (KA_THREADS / 32);
+            const size_t smem = bt->ka_variant == 2 ? (size_t)P.Nz * 16 : 0;
+            bt->ka<<<dim3(blocks, cn), KA_THREADS, smem, st>>>(P, bt->ctx->d_status);
             stage_mark(bt, 0, false);
             stage_mark(bt, 4, true);
             launch_kb(bt, P, cn, st);

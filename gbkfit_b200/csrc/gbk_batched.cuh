@@ -47,9 +47,11 @@ struct BatchKernelArgs {
     float* mplanes;       // (chunk, Nz, Wy, pitch): written where xr is not empty
     int nch;              // 32-column chunks per window row, ceil(Wx / 32)
     int nwfast;           // the disk's traits are exactly rpt/vpt/dpt uid 101 (smdisk_spaxel_nw)
-    int* xrt;             // (chunk, Nz, Wy, nch): nonzero x range (xmin | xmax << 16) of
-                          // each plane row chunk (4-aligned around it is written), or -1;
-                          // written by the model kernel, read by the PSF kernel
+    int* xrt;             // (chunk, Nz, Wy, nch): the nonzero columns of each plane row
+                          // chunk as a 32-bit mask (bit j: column 32 chunk + j; 0: the
+                          // chunk is zero).  Every column of a 4-column group with a set
+                          // bit is written; written by the model kernel, read by the
+                          // PSF kernel
     const double* sat;    // (Nz, Ny + 1, Nx + 1): summed-area table of the zero-model r^2
     // executed-work counters (null unless enabled): what the direct-mode kernels
     // actually compute, for the roofline of the measured launches
@@ -95,8 +97,8 @@ constexpr int KA_THREADS = 128;        // 4 independent (row, chunk) warps per b
 //
 // Sparsity: a line is exactly zero outside its +-5 sigma channel window and
 // off the disk, so each LSF-convolved plane is nonzero only in a band of
-// rows and columns.  The model kernel records each plane row's nonzero x
-// range; the PSF kernel convolves only the bounding box of its plane (sums
+// rows and columns.  The model kernel records each plane row chunk's nonzero
+// columns; the PSF kernel convolves only the bounding box of its plane (sums
 // of exact zeros are exact zeros, so results do not change) and takes the
 // residual outside the box, where the model is exactly 0, from a summed-area
 // table of ((0 - data) / error * mask * weight)^2 built once per data cube.
@@ -106,7 +108,7 @@ constexpr int KA_THREADS = 128;        // 4 independent (row, chunk) warps per b
 // LSF-convolved spectral column over the warp's output channel range: a
 // sliding window of KZ line values in registers (compile-time rotation, KZ
 // taps per output), each output plane row chunk stored as one coalesced
-// 128-byte segment.  Per plane the chunk's nonzero x range is stored.
+// 128-byte segment.  Per plane the chunk's nonzero-column mask is stored.
 template<int KZ>
 __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(BatchKernelArgs P, int* status)
 {
@@ -163,7 +165,7 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
     int* xr = P.xrt + ((long long)c * P.Nz * P.Wy + y) * P.nch + chunk;
     // planes outside [zlo, zhi] are empty for this chunk
     for (int zo = lane; zo < P.Nz; zo += 32)
-        if (zo < zlo || zo > zhi) xr[zo * xs] = -1;
+        if (zo < zlo || zo > zhi) xr[zo * xs] = 0;
     if (zlo <= zhi) {
         float lz[KZ];
 #pragma unroll
@@ -198,16 +200,135 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
                                                  (unsigned)zo - (unsigned)olo <= olen);
                 if (zo == own) mm = m;
                 if (zo == fl) {
-                    if (own <= zo)
-                        xr[own * xs] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
-                                             ((chunk * 32 + 31 - __clz(mm)) << 16))
-                                          : -1;
+                    if (own <= zo) xr[own * xs] = (int)mm;
                     mz = zo + 1;
                     own = mz + lane;
                     fl = min(mz + 31, zhi);
                 }
             }
         }
+    }
+    if (P.counters && lane == 0) {
+        atomicAdd(&P.counters[GBK_CTR_KA_SPAXEL], 32ull);
+        if (zlo <= zhi) {
+            const unsigned long long n = (unsigned long long)(zhi - zlo + 1) * 32;
+            atomicAdd(&P.counters[GBK_CTR_KA_FMA], n * KZ);
+            atomicAdd(&P.counters[GBK_CTR_KA_LINE], n + (KZ - 1) * 32ull);
+        }
+    }
+    if (bad) atomicOr(status, GBK_STATUS_BAD_TRAIT);
+}
+
+// KA on compact spaxel tiles: a block per (set, 4 window rows, 32-column
+// chunk), its warp w on the 4 x 8 tile of columns [32 chunk + 8 w, + 8); lane
+// l takes spaxel (32 chunk + 8 w + (l & 7), 4 rg + (l >> 3)).  The lines of
+// nearby spaxels have close channel windows, and a 4 x 8 tile spans fewer
+// velocities than a 32-spaxel row, so the warp's channel range (the union of
+// its lanes' output ranges) is shorter: ~1.57 instead of ~2.11 times the
+// lanes' own ranges for the 128 x 128 x 96 batch workload.  Each plane row
+// store is a 32-byte segment.  A warp's ballot of plane zo holds four rows'
+// 8-column masks; each goes into byte w of that row chunk's entry (columns
+// 8 w .. 8 w + 7) in shared memory (Nz x 4 entries, zero where no warp
+// writes), and the block stores whole entries once all four warps are done.
+// The lines, the LSF FIR and its order of operations are those of
+// ka_lines_lsf (identical values).
+template<int KZ>
+__global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf_t(BatchKernelArgs P, int* status)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rg = blockIdx.x / P.nch, chunk = blockIdx.x % P.nch;   // grid: ceil(Wy / 4) nch
+    extern __shared__ unsigned s_ent[];                               // (Nz, 4 rows)
+    for (int i = threadIdx.x; i < 4 * P.Nz; i += KA_THREADS) s_ent[i] = 0u;
+    __syncthreads();
+    const int y = 4 * rg + (lane >> 3), x = chunk * 32 + 8 * warp + (lane & 7);
+    const bool row_ok = y < P.Wy;
+    const int c = blockIdx.y, b = P.set0 + c;
+    const DiskArgs a = set_disk(P, b);
+    const DiskConst kc = disk_const(a);
+    int bad = 0;
+    SpaxelOut o{};
+    int lo = INT_MAX, hi = -1;
+    float amp = 0.f, rinv = 0.f;
+    const bool on = row_ok && x < P.Wx &&
+                    (P.nwfast ? smdisk_spaxel_nw(a, kc, x, y, o) : smdisk_spaxel(a, kc, x, y, 0, o, bad));
+    if (on && line_window(o.vv, o.dv, P.Wz, a.spec_step, a.spec_zero, lo, hi)) {
+        amp = o.orv * (1 / (o.dv * sqrtf(2 * GBK_PI)));
+        rinv = 1.4426950408889634f / (2 * o.dv * o.dv);
+    } else {
+        lo = INT_MAX;
+        hi = -1;
+    }
+    const float v = o.vv, z0 = a.spec_zero, dz = a.spec_step;
+    const unsigned wlen = (unsigned)hi - (unsigned)lo;
+    auto line_f = [&](int z, float zf) {
+        const float d = (z0 + zf * dz) - v;
+        float e;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-(d * d) * rinv));
+        return (unsigned)z - (unsigned)lo <= wlen ? amp * e : 0.f;
+    };
+    auto line = [&](int z) { return line_f(z, (float)z); };
+    const bool lit = lo <= hi;
+    const int olo = lit ? max(0, lo - KZ + 1) : INT_MAX, ohi = lit ? min(P.Nz - 1, hi) : -1;
+    const unsigned olen = lit ? (unsigned)(ohi - olo) : 0u;
+    int zlo = olo, zhi = ohi;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, s));
+        zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, s));
+    }
+    // byte `warp` of the entries of plane z, rows 4 rg + r (r < 4)
+    auto put = [&](int z, unsigned m) {
+        unsigned char* e = reinterpret_cast<unsigned char*>(s_ent + 4 * z) + warp;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) e[4 * r] = (unsigned char)(m >> (8 * r));
+    };
+    if (zlo <= zhi) {
+        float lz[KZ];
+#pragma unroll
+        for (int t = 0; t < KZ; ++t) lz[t] = P.lsfr[t];
+        float w[KZ];
+#pragma unroll
+        for (int t = 0; t < KZ - 1; ++t) w[t] = line(zlo + t);
+        const long long zstride = (long long)P.Wy * P.pitch;
+        float* dp = P.mplanes + ((long long)c * P.Nz * P.Wy + (row_ok ? y : 0)) * P.pitch + x +
+                    zlo * zstride;
+        unsigned mm = 0u;
+        int mz = zlo, own = zlo + lane, fl = min(zlo + 31, zhi);
+        float zf = (float)(zlo + KZ - 1);
+        for (int zb = zlo; zb <= zhi; zb += KZ) {
+#pragma unroll
+            for (int k = 0; k < KZ; ++k) {
+                const int zo = zb + k;
+                if (zo > zhi) break;
+                w[(k + KZ - 1) % KZ] = line_f(zo + KZ - 1, zf);
+                zf += 1.f;
+                float acc0 = 0.f, acc1 = 0.f;
+#pragma unroll
+                for (int t = 0; t < KZ; t += 2) acc0 += lz[t] * w[(k + t) % KZ];
+#pragma unroll
+                for (int t = 1; t < KZ; t += 2) acc1 += lz[t] * w[(k + t) % KZ];
+                if (row_ok) *dp = acc0 + acc1;      // plane zo
+                dp += zstride;
+                const unsigned m = __ballot_sync(0xffffffffu,
+                                                 (unsigned)zo - (unsigned)olo <= olen);
+                if (zo == own) mm = m;
+                if (zo == fl) {
+                    if (own <= zo) put(own, mm);
+                    mz = zo + 1;
+                    own = mz + lane;
+                    fl = min(mz + 31, zhi);
+                }
+            }
+        }
+    }
+    // the block's entries: every plane of its rows in the window
+    __syncthreads();
+    const int nrow = min(4, P.Wy - 4 * rg);
+    const long long xs = (long long)P.Wy * P.nch;
+    int* xr = P.xrt + ((long long)c * P.Nz * P.Wy + 4 * rg) * P.nch + chunk;
+    for (int i = threadIdx.x; i < nrow * P.Nz; i += KA_THREADS) {
+        const int z = i / nrow, r = i - z * nrow;
+        xr[z * xs + r * P.nch] = (int)s_ent[4 * z + r];
     }
     if (P.counters && lane == 0) {
         atomicAdd(&P.counters[GBK_CTR_KA_SPAXEL], 32ull);
@@ -248,7 +369,7 @@ __device__ __forceinline__ double sat_box(const double* T, int ld, int y0, int y
 // finds the bounding box of the band's nonzero input row chunks and works
 // through its output rows in passes whose input rows fit the block's shared
 // memory (box-relative row pitch; usually one pass):
-//   - the rows' nonzero segments are loaded from HBM (cp.async), the rest of
+//   - the rows' nonzero 4-column groups are loaded from HBM (cp.async), the rest of
 //     the rows that the y FIR reads is zeroed;
 //   - x FIR in place, a warp per row, its lanes on consecutive (row, strip)
 //     pairs of its rows, 8 outputs per lane window;
@@ -345,20 +466,21 @@ __global__ void __launch_bounds__(NT, MINB) kb_psf_residual(BatchKernelArgs P)
             for (int u = 0; u < 8; ++u) {
                 const int i = i0 + u * NT + threadIdx.x;
                 if (PF) {
-                    v[u] = i < n ? s_xr[i] : -1;
+                    v[u] = i < n ? s_xr[i] : 0;
                 } else {
-                    v[u] = i < n ? src[i] : -1;
+                    v[u] = i < n ? src[i] : 0;
                     if (i < n) s_xr[i] = v[u];
                 }
             }
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                if (v[u] >= 0) {
-                    const int y = ob0 + (i0 + u * NT + (int)threadIdx.x) / P.nch;
-                    y0 = min(y0, y);
-                    y1 = max(y1, y);
-                    x0 = min(x0, v[u] & 0xffff);
-                    x1 = max(x1, v[u] >> 16);
+                if (v[u] != 0) {
+                    const int i = i0 + u * NT + (int)threadIdx.x;
+                    const int r = i / P.nch, ch = i - r * P.nch;
+                    y0 = min(y0, ob0 + r);
+                    y1 = max(y1, ob0 + r);
+                    x0 = min(x0, ch * 32 + __ffs(v[u]) - 1);
+                    x1 = max(x1, ch * 32 + 31 - __clz(v[u]));
                 }
             }
         }
@@ -419,7 +541,7 @@ __global__ void __launch_bounds__(NT, MINB) kb_psf_residual(BatchKernelArgs P)
             c_y += (unsigned long long)ng * ns4 * 32 * K;
             c_v += (unsigned long long)(ye - ys) * (xb_end - xb0);
         }
-        // load rows [ly0, ly1]: each row chunk's nonzero range, zeros elsewhere
+        // load rows [ly0, ly1]: the 4-column groups that hold a nonzero value, zeros elsewhere
         if (ly0 <= ly1) {
             const int tc = min(nsl, NT), tr = NT / tc;
             const int ti = threadIdx.x % tc, ty = threadIdx.x / tc;
@@ -429,9 +551,11 @@ __global__ void __launch_bounds__(NT, MINB) kb_psf_residual(BatchKernelArgs P)
                     float4* d = reinterpret_cast<float4*>(S) + (y - ys) * bp4;
                     const float4* g = src + (long long)y * (P.pitch / 4);
                     for (int j = ti; j < nsl; j += tc) {
+                        // the slot's 4 columns hold a nonzero value: load them
+                        // (all written), else they are zeros
                         const int sl = sl0 + j, ch = sl >> 3;
-                        const int v = ch < P.nch ? vrow[ch] : -1;
-                        if (v >= 0 && sl >= (v & 0xffff) >> 2 && sl <= (v >> 16) >> 2)
+                        const unsigned v = ch < P.nch ? (unsigned)vrow[ch] : 0u;
+                        if ((v >> (4 * (sl & 7))) & 0xfu)
                             cp_async16(d + j, g + sl);
                         else
                             d[j] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -811,8 +935,8 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 5 : 4)) ka_lines_lsf2(
     int* xr1 = xr0 + 1;                                   // chunk c1 (used when has1)
     for (int zo = lane; zo < P.Nz; zo += 32)
         if (zo < zlo || zo > zhi) {
-            xr0[zo * xs] = -1;
-            if (has1) xr1[zo * xs] = -1;
+            xr0[zo * xs] = 0;
+            if (has1) xr1[zo * xs] = 0;
         }
     if (zlo <= zhi) {
         float2 lz[KZ];
@@ -853,13 +977,8 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 5 : 4)) ka_lines_lsf2(
                 }
                 if (zo == fl) {
                     if (own <= zo) {
-                        xr0[own * xs] = mm0 ? ((c0 * 32 + __ffs(mm0) - 1) |
-                                               ((c0 * 32 + 31 - __clz(mm0)) << 16))
-                                            : -1;
-                        if (has1)
-                            xr1[own * xs] = mm1 ? ((c1 * 32 + __ffs(mm1) - 1) |
-                                                   ((c1 * 32 + 31 - __clz(mm1)) << 16))
-                                                : -1;
+                        xr0[own * xs] = (int)mm0;
+                        if (has1) xr1[own * xs] = (int)mm1;
                     }
                     mz = zo + 1;
                     own = mz + lane;
@@ -886,7 +1005,7 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 5 : 4)) ka_lines_lsf2(
 // sum run unchanged.  cubes: (sets, Wz, Wy, Wx), set b = P.set0 + slot;
 // one warp per (window row y, 32-column chunk), a lane per column, the
 // channel axis walked with a KZ-deep register window (each cube value is
-// read once).  A plane row chunk's range covers its nonzero outputs (all
+// read once).  A plane row chunk's mask marks its nonzero outputs (all
 // outputs are written), so the PSF kernel skips exactly the zero ones.
 template<int KZ>
 __global__ void __launch_bounds__(KA_THREADS) kc_cube_lsf(BatchKernelArgs P,
@@ -934,10 +1053,7 @@ __global__ void __launch_bounds__(KA_THREADS) kc_cube_lsf(BatchKernelArgs P,
             if ((zo & 31) == lane) mm = m;
             if ((zo & 31) == 31 || zo == P.Nz - 1) {
                 const int own = (zo & ~31) + lane;
-                if (own <= zo)
-                    xr[own * xs] = mm ? ((chunk * 32 + __ffs(mm) - 1) |
-                                         ((chunk * 32 + 31 - __clz(mm)) << 16))
-                                      : -1;
+                if (own <= zo) xr[own * xs] = (int)mm;
             }
         }
     }
@@ -955,6 +1071,8 @@ void ka_register_short(KaFn* t);
 void ka_register_long(KaFn* t);
 // t[Kz / 2]: the two-chunk model kernel (ka_lines_lsf2)
 void ka2_register(KaFn* t);
+// t[Kz / 2]: the model kernel on 4 x 8 spaxel tiles (ka_lines_lsf_t)
+void ka_t_register(KaFn* t);
 // t[Kz / 2]: the LSF FIR of given model cubes
 typedef void (*KcFn)(BatchKernelArgs, const float*);
 void kc_register(KcFn* t);

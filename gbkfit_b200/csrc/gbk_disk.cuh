@@ -92,9 +92,12 @@ static __device__ bool smdisk_spaxel(const DiskArgs& a, const DiskConst& kc, int
     if (a.rht.uids) eval_set<K_RH>(ht, a.rht, g, 0, 0, fabsf(zn), bad);
     for (int i = 0; i < a.rpt.n; ++i) rv += pt[i] * (thin ? 1.f : ht[i]);
     if (!rv) return false;
-    if (thin) rv /= cosf(incli);
+    // cos_in and sin_in are sincosf(incli): the values cosf(incli) and
+    // sinf(incli) of gmodels.hpp, computed once per set (per spaxel only
+    // when the disk is tilted)
+    if (thin) rv /= cos_in;
     else rv *= a.stz;
-    if (a.vpt.uids) eval_set<K_VP>(pt, a.vpt, g, sinf(incli), cosf(incli), 0, bad);
+    if (a.vpt.uids) eval_set<K_VP>(pt, a.vpt, g, sin_in, cos_in, 0, bad);
     if (a.vht.uids) eval_set<K_VH>(ht, a.vht, g, 0, 0, fabsf(zn), bad);
     for (int i = 0; i < a.vpt.n; ++i) vv += pt[i] * (thin ? 1.f : ht[i]);
     vv += vsysi;
@@ -140,8 +143,8 @@ __device__ __forceinline__ bool smdisk_spaxel_nw(const DiskArgs& a, const DiskCo
     float rv = 0;
     rv += lerp(r, k, a.rnodes, a.rpt.pv, 0) * 1.f;
     if (!rv) return false;
-    rv /= cosf(kc.incli);
-    const float mtan = cosf(theta) * sinf(kc.incli);
+    rv /= kc.cos_in;                                     // cosf(incli), once per set
+    const float mtan = cosf(theta) * kc.sin_in;
     const float vt = r == 0 ? 0.f : lerp(r, k, a.rnodes, a.vpt.pv, 0) * mtan;
     float vv = 0;
     vv += vt * 1.f;

@@ -371,10 +371,11 @@ typedef struct {
                              * copied in while the previous item runs); 7 = 0 on
                              * 256-thread blocks with twice the shared memory (2 blocks
                              * per SM); 0 = the first */
-    int model_variant;      /* direct mode, the model kernel (both give the same values):
+    int model_variant;      /* direct mode, the model kernel (all give the same values):
                              * 0 = a warp per 32-column chunk stepping every lane through
                              * the union of the lanes' channel windows; 1 = two chunks per
-                             * warp on packed FP32 pairs */
+                             * warp on packed FP32 pairs; 2 = a warp per 4 x 8 spaxel tile
+                             * (shorter channel unions) */
 } gbkb200_batch_desc;
 
 int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);

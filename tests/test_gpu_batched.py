@@ -278,18 +278,21 @@ def test_batched_cubes_match_disk_path(gpu):
     ev.close()
 
 
-@pytest.mark.parametrize('nodewise', [True, False])
-def test_batched_model_variant_identical(gpu, nodewise):
+@pytest.mark.parametrize('nodewise,ny', [(True, 60), (False, 60), (True, 62)])
+def test_batched_model_variant_identical(gpu, nodewise, ny):
     """The model kernel on two 32-column chunks per warp (packed FP32 pairs,
-    each lane rounded as fmaf) gives bit-identical chi^2 and models, with an
-    odd number of chunks (the last warp's second chunk is absent), on the
-    node-wise fast path and the generic trait path."""
+    each lane rounded as fmaf) and on 4 x 8 spaxel tiles give bit-identical
+    chi^2 and models, with an odd number of chunks (the last warp's second
+    chunk is absent), on the node-wise fast path and the generic trait path,
+    and with a window height that is not a multiple of 4 (the last row
+    group of the tiles is partial: 62 + 16 rows)."""
     import torch
     from gbkfit_b200 import traits as T
+    from gbkfit_b200 import workloads
     from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
     from gbkfit_b200.disk import Disk
     n = 6
-    w = _small_batch_workload(n)
+    w = workloads.smdisk_batch128(nsets=n, size=(64, ny, 48), nnodes=16)
     if not nodewise:
         w.disk = Disk(False, False, w.disk.rnodes, traits=dict(
             rpt=[T.bpt('nw_uniform')], vpt=[T.vpt('nw_tan_uniform')], dpt=[T.dpt('nw_uniform')],
@@ -298,7 +301,7 @@ def test_batched_model_variant_identical(gpu, nodewise):
         w.extra = dict(w.extra, truth=dict(w.extra['truth'], spt_p=30.0, spt_s=300.0))
     data, err, _ = synthetic_data(w)
     out = []
-    for variant in (0, 1):
+    for variant in (0, 1, 2):
         ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=n, chunk=4, conv='direct',
                            model_variant=variant)
         bufs = ev.alloc_inputs(n)
