@@ -170,8 +170,9 @@ def barrier(world):
 def roofline_direct(kernels, counters, steps, nsets, clocks, geom, ms_step):
     """Roofline of the dominant direct-mode kernel (the PSF FIR + residual
     kernel): the FLOPs it executed (PSF x and y FIR multiply-adds and residual
-    voxels, counted inside the kernel over the timed launches) per launch,
-    divided by its average launch time (CUDA events on its stream), against
+    voxels, counted inside the kernel over a second pass of the same launches)
+    per launch, divided by its average launch time (CUDA events on its stream,
+    measured in a pass without the counters), against
     the FP32 CUDA-core peak at the sampled clock.  The kernel computes in
     FP32 on CUDA cores and moves little DRAM traffic (see `hbm_view`)."""
     peak, mhz = fp32_peak_tflops(clocks)
@@ -202,7 +203,8 @@ def roofline_direct(kernels, counters, steps, nsets, clocks, geom, ms_step):
         executed_flops_per_launch=int(fl_kb), ms_per_launch=k['ms_per_launch'],
         sets_per_launch=sets_per_launch,
         basis='PSF x and y FIR multiply-adds (2 FLOP each) and residual voxels (3 FLOP each) '
-              'executed by the kernel, counted in-kernel over the timed launches',
+              'executed by the kernel, counted in-kernel over a second pass of the same '
+              'launches (the timed pass runs without the counters)',
         traffic=round(traffic), traffic_unit='DRAM bytes per launch',
         traffic_source='ncu capture of a 128-set wave of this workload, scaled to the '
                        'sets of one launch (not measured by this run)',
@@ -368,13 +370,21 @@ def run_b200(args):
     assert np.all(np.isfinite(chi2)) and np.all(chi2 > 0)
 
     # per-kernel device time: the same evaluation launched without the graph,
-    # with a CUDA event pair around every launch on the evaluator's stream
-    ev.set_timing(True)
+    # with a CUDA event pair around every launch on the evaluator's stream and
+    # no work counters; then one more pass with the counters for the executed
+    # work (their atomic adds would lengthen the timed launches)
+    ev.set_timing(True, counters=False)
     ev.stage_times()
     for i in range(args.steps):
         flush.fill_(float(i))
         ev.evaluate_device(bufs, nsets)
     stages = ev.stage_times()
+    ev.set_timing(True, counters=True)
+    ev.work_counters()
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        ev.evaluate_device(bufs, nsets)
+    ev.stage_times()
     counters = ev.work_counters()
     ev.set_timing(False)
     tsum = sum(t for t, _ in stages.values())
@@ -921,9 +931,10 @@ def main():
     ap.add_argument('--chunk', type=int, default=0, help='force the sets per wave (default: tuned)')
     ap.add_argument('--psf-variant', type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5, 6, 7],
                     help='PSF kernel variant of the direct mode (default: tuned)')
-    ap.add_argument('--model-variant', type=int, default=-1, choices=[-1, 0, 1, 2],
+    ap.add_argument('--model-variant', type=int, default=-1, choices=[-1, 0, 1, 2, 3],
                     help='model kernel of the direct mode: 0 one chunk per warp, 1 chunk '
-                         'pairs, 2 4x8 spaxel tiles (default: tuned)')
+                         'pairs, 2 4x8 spaxel tiles, 3 tiles with transposed range masks '
+                         '(default: tuned)')
     ap.add_argument('--band', type=int, default=0,
                     help='force the output rows per PSF block of the direct mode (default: tuned)')
     ap.add_argument('--workload', default='smdisk_batch128',

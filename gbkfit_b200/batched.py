@@ -428,9 +428,12 @@ class BatchedSMDisk:
         self._graph.replay()
         return self.chi2
 
-    def set_timing(self, enable):
-        """Per-stage CUDA-event timing of subsequent (uncaptured) evaluations."""
-        check(_lib.gbkb200_batch_set_timing(self.handle, int(bool(enable))), 'batch_set_timing')
+    def set_timing(self, enable, counters=True):
+        """Per-stage CUDA-event timing of subsequent (uncaptured) evaluations;
+        with ``counters`` the direct-mode kernels also count their executed
+        work (atomic adds that lengthen the timed launches)."""
+        mode = 0 if not enable else (1 if counters else 2)
+        check(_lib.gbkb200_batch_set_timing(self.handle, mode), 'batch_set_timing')
 
     def stage_times(self):
         """{kernel name: (summed ms, launches)} since the last call (synchronises)."""
@@ -442,7 +445,7 @@ class BatchedSMDisk:
 
     def work_counters(self):
         """{counter: executed work} of the direct-mode kernels since the last
-        call, counted while timing is enabled (synchronises)."""
+        call, counted while timing is enabled with counters (synchronises)."""
         out = (ctypes.c_ulonglong * 8)()
         check(_lib.gbkb200_batch_counters(self.handle, out), 'batch_counters')
         return {n: int(out[i]) for i, n in enumerate(COUNTERS)}

@@ -356,6 +356,7 @@ struct gbkb200_batch {
     void (*ka)(BatchKernelArgs, int*) = nullptr;
     // per-stage timing: event pairs recorded around launches while enabled
     int timing = 0;
+    int count = 0;                            // work counters on (timing mode 1)
     unsigned long long* counters = nullptr;   // device, GBK_CTR_N (direct mode, timing on)
     std::vector<cudaEvent_t> ev;      // 2 per record
     std::vector<int> ev_stage;
@@ -410,12 +411,15 @@ static KaFn ka_fn(int Kz)
     return t[Kz / 2];
 }
 
-static KaFn ka_t_fn(int Kz)
+static KaFn ka_t_fn(int Kz, bool tm)
 {
-    static KaFn t[KA_KMAX / 2 + 1] = {};
+    static KaFn t[2][KA_KMAX / 2 + 1] = {};
     static std::once_flag once;
-    std::call_once(once, [] { ka_t_register(t); });
-    return t[Kz / 2];
+    std::call_once(once, [] {
+        ka_t_register(t[0], false);
+        ka_t_register(t[1], true);
+    });
+    return t[tm ? 1 : 0][Kz / 2];
 }
 
 static KaFn ka2_fn(int Kz)
@@ -563,11 +567,14 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     k_iw<<<592, 256, 0, bt->ctx->stream>>>(P, bt->iw, (long long)P.Nz * P.Ny * P.Nx);
     GBK_CUDA_TRY(cudaGetLastError());
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
-    if (d->model_variant < 0 || d->model_variant > 2) return GBKB200_ERR_INVALID_ARG;
-    // variant 2 keeps a plane's entries of its 4 rows in shared memory
-    if (d->model_variant == 2 && (long long)P.Nz * 16 > 32 * 1024) return GBKB200_ERR_UNSUPPORTED;
-    bt->ka = d->model_variant == 1 ? ka2_fn(P.Kz) : d->model_variant == 2 ? ka_t_fn(P.Kz)
-                                                                         : ka_fn(P.Kz);
+    if (d->model_variant < 0 || d->model_variant > 3) return GBKB200_ERR_INVALID_ARG;
+    // variants 2 and 3 (4 x 8 tiles) keep a plane's entries of its 4 rows in
+    // shared memory; 3 forms the masks by bit transposes
+    const bool tiles = d->model_variant >= 2;
+    if (tiles && (long long)P.Nz * 16 > 32 * 1024) return GBKB200_ERR_UNSUPPORTED;
+    bt->ka = d->model_variant == 1 ? ka2_fn(P.Kz)
+             : tiles               ? ka_t_fn(P.Kz, d->model_variant == 3)
+                                   : ka_fn(P.Kz);
     bt->ka_variant = d->model_variant;
     bt->kb = kb_fn(P.K, d->psf_variant);
     {
@@ -870,7 +877,7 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
     }
     P.model = model;
     P.lim_model = model ? (long long)nsets * P.Nz * P.Ny * P.Nx : 0;
-    P.counters = bt->timing ? bt->counters : nullptr;
+    P.counters = bt->count ? bt->counters : nullptr;
     const long long set_stride = (long long)P.Wz * P.Py * P.hx;
     const long long lim_spec = (long long)P.Pz * P.Py * P.hx;
     const int tiles = (P.hx + BLT - 1) / BLT;
@@ -879,11 +886,12 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
             const int cn = std::min(bt->chunk, nsets - s0);
             P.set0 = s0;
             stage_mark(bt, 0, true);
-            // variant 2: a block per (4 rows, chunk); otherwise a warp per item
+            // variants 2 and 3: a block per (4 rows, chunk); otherwise a warp per item
+            const bool tiles = bt->ka_variant >= 2;
             const int items = P.Wy * (bt->ka_variant == 1 ? (P.nch + 1) / 2 : P.nch);
-            const int blocks = bt->ka_variant == 2 ? (P.Wy + 3) / 4 * P.nch
-                                                   : (items + KA_THREADS / 32 - 1) / (KA_THREADS / 32);
-            const size_t smem = bt->ka_variant == 2 ? (size_t)P.Nz * 16 : 0;
+            const int blocks = tiles ? (P.Wy + 3) / 4 * P.nch
+                                     : (items + KA_THREADS / 32 - 1) / (KA_THREADS / 32);
+            const size_t smem = tiles ? (size_t)P.Nz * 16 : 0;
             bt->ka<<<dim3(blocks, cn), KA_THREADS, smem, st>>>(P, bt->ctx->d_status);
             stage_mark(bt, 0, false);
             stage_mark(bt, 4, true);
@@ -954,7 +962,7 @@ extern "C" int gbkb200_batch_evaluate_cubes(gbkb200_batch* bt, int nsets, const 
     cudaStream_t st = bt->ctx->stream;
     P.model = model;
     P.lim_model = model ? (long long)nsets * P.Nz * P.Ny * P.Nx : 0;
-    P.counters = bt->timing ? bt->counters : nullptr;
+    P.counters = bt->count ? bt->counters : nullptr;
     const KcFn kc = kc_fn(P.Kz);
     for (int s0 = 0; s0 < nsets; s0 += bt->chunk) {
         const int cn = std::min(bt->chunk, nsets - s0);
@@ -1050,12 +1058,14 @@ extern "C" int gbkb200_batch_query(const gbkb200_batch* bt, int* done)
 extern "C" int gbkb200_batch_set_timing(gbkb200_batch* bt, int enable)
 {
     if (!bt) return GBKB200_ERR_INVALID_ARG;
-    if (enable && !bt->counters) {
+    if (enable < 0 || enable > 2) return GBKB200_ERR_INVALID_ARG;
+    if (enable == 1 && !bt->counters) {
         if (cudaMalloc(&bt->counters, GBK_CTR_N * sizeof(unsigned long long)) != cudaSuccess)
             return GBKB200_ERR_OOM;
         GBK_CUDA_TRY(cudaMemset(bt->counters, 0, GBK_CTR_N * sizeof(unsigned long long)));
     }
     bt->timing = enable ? 1 : 0;
+    bt->count = enable == 1 ? 1 : 0;
     bt->ev_used = 0;
     bt->ev_error = 0;
     return GBKB200_OK;

@@ -109,6 +109,33 @@ constexpr int KA_THREADS = 128;        // 4 independent (row, chunk) warps per b
 // sliding window of KZ line values in registers (compile-time rotation, KZ
 // taps per output), each output plane row chunk stored as one coalesced
 // 128-byte segment.  Per plane the chunk's nonzero-column mask is stored.
+// Warp-wide transpose of a 32 x 32 bit matrix: lane i holds row i (bit j =
+// column j) and receives column i (bit j = row j of lane j).  Five butterfly
+// stages, each exchanging the off-diagonal blocks of the 2s x 2s sub-blocks
+// (s = 16, 8, 4, 2, 1) with the partner lane i ^ s.
+__device__ __forceinline__ unsigned warp_transpose32(unsigned v, int lane)
+{
+    constexpr unsigned M[5] = {0x0000ffffu, 0x00ff00ffu, 0x0f0f0f0fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int s = 16 >> k;
+        const unsigned y = __shfl_xor_sync(0xffffffffu, v, s);
+        v = (lane & s) ? ((v & ~M[k]) | ((y >> s) & M[k])) : ((v & M[k]) | ((y << s) & ~M[k]));
+    }
+    return v;
+}
+
+// The nonzero-lane masks of output planes [mz, mz + 32): lane j receives the
+// mask of plane mz + j, bit l set when lane l's output range [olo, ohi]
+// holds that plane (the per-plane ballots of the range test, for 32 planes
+// at once).  A lane without a line passes olo > ohi.
+__device__ __forceinline__ unsigned plane_masks32(int olo, int ohi, int mz, int lane)
+{
+    const int a = max(olo - mz, 0), e = min(ohi - mz, 31);
+    const unsigned row = a <= e ? ((0xffffffffu >> (31 - e)) & (0xffffffffu << a)) : 0u;
+    return warp_transpose32(row, lane);
+}
+
 template<int KZ>
 __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(BatchKernelArgs P, int* status)
 {
@@ -232,7 +259,11 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
 // writes), and the block stores whole entries once all four warps are done.
 // The lines, the LSF FIR and its order of operations are those of
 // ka_lines_lsf (identical values).
-template<int KZ>
+// TM (transposed masks): no ballot in the channel loop; after it, each group
+// of 32 planes gets its masks at once, every lane forming its output range
+// as a 32-bit row and the warp transposing the 32 rows (plane_masks32): the
+// same masks for a few instructions per group instead of several per plane.
+template<int KZ, bool TM>
 __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf_t(BatchKernelArgs P, int* status)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -309,15 +340,24 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf_t
                 for (int t = 1; t < KZ; t += 2) acc1 += lz[t] * w[(k + t) % KZ];
                 if (row_ok) *dp = acc0 + acc1;      // plane zo
                 dp += zstride;
-                const unsigned m = __ballot_sync(0xffffffffu,
-                                                 (unsigned)zo - (unsigned)olo <= olen);
-                if (zo == own) mm = m;
-                if (zo == fl) {
-                    if (own <= zo) put(own, mm);
-                    mz = zo + 1;
-                    own = mz + lane;
-                    fl = min(mz + 31, zhi);
+                if constexpr (!TM) {
+                    const unsigned m = __ballot_sync(0xffffffffu,
+                                                     (unsigned)zo - (unsigned)olo <= olen);
+                    if (zo == own) mm = m;
+                    if (zo == fl) {
+                        if (own <= zo) put(own, mm);
+                        mz = zo + 1;
+                        own = mz + lane;
+                        fl = min(mz + 31, zhi);
+                    }
                 }
+            }
+        }
+        if constexpr (TM) {
+            // lanes without a line: olo = INT_MAX, ohi = -1 (an empty row)
+            for (int g = zlo; g <= zhi; g += 32) {
+                const unsigned m = plane_masks32(olo, ohi, g, lane);
+                if (g + lane <= zhi) put(g + lane, m);
             }
         }
     }
@@ -1072,7 +1112,7 @@ void ka_register_long(KaFn* t);
 // t[Kz / 2]: the two-chunk model kernel (ka_lines_lsf2)
 void ka2_register(KaFn* t);
 // t[Kz / 2]: the model kernel on 4 x 8 spaxel tiles (ka_lines_lsf_t)
-void ka_t_register(KaFn* t);
+void ka_t_register(KaFn* t, bool tm);
 // t[Kz / 2]: the LSF FIR of given model cubes
 typedef void (*KcFn)(BatchKernelArgs, const float*);
 void kc_register(KcFn* t);

@@ -375,7 +375,9 @@ typedef struct {
                              * 0 = a warp per 32-column chunk stepping every lane through
                              * the union of the lanes' channel windows; 1 = two chunks per
                              * warp on packed FP32 pairs; 2 = a warp per 4 x 8 spaxel tile
-                             * (shorter channel unions) */
+                             * (shorter channel unions); 3 = 2 with the range-table masks
+                             * from one bit transpose per 32 planes instead of a ballot
+                             * per plane */
 } gbkb200_batch_desc;
 
 int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);
@@ -430,6 +432,8 @@ int gbkb200_batch_destroy(gbkb200_batch* b);
  * 0 model + lines (direct: LSF FIR too; FFT: x r2c), 1 y FFT, 2 z FFT
  * convolution, 3 inverse y FFT (FFT mode only), 4 PSF FIR or
  * x c2r + residual, 5 chi^2 sum.
+ * enable: 0 off, 1 timing and the work counters below, 2 timing alone (the
+ * kernels then run without the counters' atomic adds, as in a graph replay).
  * gbkb200_batch_timing synchronizes the stream, returns the summed
  * milliseconds and launch counts per stage since the last call, and resets. */
 #define GBKB200_BATCH_STAGES 6
@@ -437,7 +441,7 @@ int gbkb200_batch_set_timing(gbkb200_batch* b, int enable);
 int gbkb200_batch_timing(gbkb200_batch* b, double ms[GBKB200_BATCH_STAGES],
                          int launches[GBKB200_BATCH_STAGES]);
 /* Executed-work counters of the direct-mode kernels (no reference
- * counterpart; a measurement aid), counted while timing is enabled:
+ * counterpart; a measurement aid), counted while timing mode 1 is enabled:
  * [0] LSF FIR multiply-adds, [1] line values (one exponential each),
  * [2] PSF x FIR multiply-adds, [3] PSF y FIR multiply-adds, [4] residual
  * voxels computed from the model box, [5] spaxel evaluations (one

@@ -281,7 +281,8 @@ def test_batched_cubes_match_disk_path(gpu):
 @pytest.mark.parametrize('nodewise,ny', [(True, 60), (False, 60), (True, 62)])
 def test_batched_model_variant_identical(gpu, nodewise, ny):
     """The model kernel on two 32-column chunks per warp (packed FP32 pairs,
-    each lane rounded as fmaf) and on 4 x 8 spaxel tiles give bit-identical
+    each lane rounded as fmaf) and on 4 x 8 spaxel tiles (range-table masks
+    from per-plane ballots or from bit transposes) give bit-identical
     chi^2 and models, with an odd number of chunks (the last warp's second
     chunk is absent), on the node-wise fast path and the generic trait path,
     and with a window height that is not a multiple of 4 (the last row
@@ -301,7 +302,7 @@ def test_batched_model_variant_identical(gpu, nodewise, ny):
         w.extra = dict(w.extra, truth=dict(w.extra['truth'], spt_p=30.0, spt_s=300.0))
     data, err, _ = synthetic_data(w)
     out = []
-    for variant in (0, 1, 2):
+    for variant in (0, 1, 2, 3):
         ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=n, chunk=4, conv='direct',
                            model_variant=variant)
         bufs = ev.alloc_inputs(n)
@@ -333,3 +334,30 @@ def test_batched_evaluate_pieces_identical(gpu):
         got = ev.evaluate(w.params, n, pieces=pieces)
         assert np.array_equal(got, ref), pieces
     ev.close()
+
+
+def test_timing_modes_and_counters(gpu):
+    """Timing without counters leaves the counters at zero and the chi^2
+    unchanged; timing with counters counts the direct-mode kernels' work."""
+    import torch
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    w = _small_batch_workload(4)
+    data, err, _ = synthetic_data(w)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=4, conv='direct')
+    bufs = ev.alloc_inputs(4)
+    ev.upload(ev.pack(w.params, 4), bufs, 4)
+    plain = ev.evaluate_device(bufs, 4).clone()
+    ev.set_timing(True, counters=False)
+    timed = ev.evaluate_device(bufs, 4).clone()
+    stages = ev.stage_times()
+    assert stages and all(t > 0 and n == 1 for t, n in stages.values()), stages
+    assert all(v == 0 for v in ev.work_counters().values())
+    ev.set_timing(True, counters=True)
+    counted = ev.evaluate_device(bufs, 4).clone()
+    ev.stage_times()
+    c = ev.work_counters()
+    ev.set_timing(False)
+    assert c['psf_x_fma'] > 0 and c['psf_y_fma'] > 0 and c['residual_voxels'] > 0
+    assert c['lsf_fma'] > 0 and c['lines'] > 0
+    torch.testing.assert_close(timed, plain, rtol=0, atol=0)
+    torch.testing.assert_close(counted, plain, rtol=0, atol=0)
