@@ -13,8 +13,8 @@ Knobs (all change speed only, never results beyond fp32 rounding):
   before each item's FIR), or persistent over all (set, plane) items;
 * ``model_variant``: the direct mode's model kernel (0: one 32-column chunk
   per warp; 1: two chunks per warp on packed FP32 pairs; 2: a 4 x 8 spaxel
-  tile per warp; 3: 2 with the range-table masks by bit transposes; 4: 3
-  on one-warp blocks; the same values);
+  tile per warp; 3: 2 with the range-table masks by bit transposes; the
+  same values);
 * ``rows_k1``: spectral rows per shared-memory group of the model kernel.
 
 Coordinate descent from the defaults; every trial builds an evaluator and
@@ -131,7 +131,7 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
                 best_d, best_dt = cfg, t
         # the model kernel's variants
         base = dict(best_d)
-        for mv in (1, 2, 3, 4):
+        for mv in (1, 2, 3):
             cfg = dict(base, model_variant=mv)
             t = time_config(w, data, err, nsets, cfg)
             if t < best_dt:

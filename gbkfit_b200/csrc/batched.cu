@@ -411,17 +411,15 @@ static KaFn ka_fn(int Kz)
     return t[Kz / 2];
 }
 
-// form 0: ballot masks, 1: transposed masks, 2: transposed masks on one-warp blocks
-static KaFn ka_t_fn(int Kz, int form)
+static KaFn ka_t_fn(int Kz, bool tm)
 {
-    static KaFn t[3][KA_KMAX / 2 + 1] = {};
+    static KaFn t[2][KA_KMAX / 2 + 1] = {};
     static std::once_flag once;
     std::call_once(once, [] {
-        ka_t_register(t[0], false, false);
-        ka_t_register(t[1], true, false);
-        ka_t_register(t[2], true, true);
+        ka_t_register(t[0], false);
+        ka_t_register(t[1], true);
     });
-    return t[form][Kz / 2];
+    return t[tm ? 1 : 0][Kz / 2];
 }
 
 static KaFn ka2_fn(int Kz)
@@ -569,14 +567,13 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     k_iw<<<592, 256, 0, bt->ctx->stream>>>(P, bt->iw, (long long)P.Nz * P.Ny * P.Nx);
     GBK_CUDA_TRY(cudaGetLastError());
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
-    if (d->model_variant < 0 || d->model_variant > 4) return GBKB200_ERR_INVALID_ARG;
+    if (d->model_variant < 0 || d->model_variant > 3) return GBKB200_ERR_INVALID_ARG;
     // variants 2 and 3 (4 x 8 tiles) keep a plane's entries of its 4 rows in
-    // shared memory; 3 forms the masks by bit transposes; 4 is 3 on one-warp
-    // blocks storing the mask bytes to the table directly
+    // shared memory; 3 forms the masks by bit transposes
     const bool tiles = d->model_variant >= 2;
     if (tiles && (long long)P.Nz * 16 > 32 * 1024) return GBKB200_ERR_UNSUPPORTED;
     bt->ka = d->model_variant == 1 ? ka2_fn(P.Kz)
-             : tiles               ? ka_t_fn(P.Kz, d->model_variant - 2)
+             : tiles               ? ka_t_fn(P.Kz, d->model_variant == 3)
                                    : ka_fn(P.Kz);
     bt->ka_variant = d->model_variant;
     bt->kb = kb_fn(P.K, d->psf_variant);
@@ -889,15 +886,13 @@ extern "C" int gbkb200_batch_evaluate(gbkb200_batch* bt, int nsets, const float*
             const int cn = std::min(bt->chunk, nsets - s0);
             P.set0 = s0;
             stage_mark(bt, 0, true);
-            // variants 2 and 3: a block per (4 rows, chunk); 4: a block per
-            // (4 rows, chunk, warp); otherwise a warp per item
-            const bool tiles = bt->ka_variant >= 2, one_warp = bt->ka_variant == 4;
+            // variants 2 and 3: a block per (4 rows, chunk); otherwise a warp per item
+            const bool tiles = bt->ka_variant >= 2;
             const int items = P.Wy * (bt->ka_variant == 1 ? (P.nch + 1) / 2 : P.nch);
-            const int blocks = one_warp ? (P.Wy + 3) / 4 * P.nch * 4
-                               : tiles  ? (P.Wy + 3) / 4 * P.nch
-                                        : (items + KA_THREADS / 32 - 1) / (KA_THREADS / 32);
-            const size_t smem = tiles && !one_warp ? (size_t)P.Nz * 16 : 0;
-            bt->ka<<<dim3(blocks, cn), one_warp ? 32 : KA_THREADS, smem, st>>>(P, bt->ctx->d_status);
+            const int blocks = tiles ? (P.Wy + 3) / 4 * P.nch
+                                     : (items + KA_THREADS / 32 - 1) / (KA_THREADS / 32);
+            const size_t smem = tiles ? (size_t)P.Nz * 16 : 0;
+            bt->ka<<<dim3(blocks, cn), KA_THREADS, smem, st>>>(P, bt->ctx->d_status);
             stage_mark(bt, 0, false);
             stage_mark(bt, 4, true);
             launch_kb(bt, P, cn, st);

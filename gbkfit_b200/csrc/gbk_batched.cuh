@@ -263,36 +263,14 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
 // of 32 planes gets its masks at once, every lane forming its output range
 // as a 32-bit row and the warp transposing the 32 rows (plane_masks32): the
 // same masks for a few instructions per group instead of several per plane.
-// BW (warps per block) 1: a block per warp (grid 4 ceil(Wy / 4) nch), each
-// warp storing its byte of every entry of its 4 rows straight to global
-// memory (zero outside its output planes; the four warps of a row chunk own
-// distinct bytes), with no shared memory and no block barrier, so that a warp
-// that finishes early frees its slot for the next block at once.
-template<int KZ, bool TM, int BW>
-__global__ void __launch_bounds__(32 * BW, (KZ <= 15 ? 32 : 16) / BW) ka_lines_lsf_t(BatchKernelArgs P, int* status)
+template<int KZ, bool TM>
+__global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf_t(BatchKernelArgs P, int* status)
 {
-    static_assert(BW == 1 || BW == 4, "a block of 1 or 4 warps");
-    constexpr int NT = 32 * BW;
-    const int lane = threadIdx.x & 31;
-    const int warp = BW == 4 ? (int)(threadIdx.x >> 5) : (int)(blockIdx.x & 3);
-    const int tile = BW == 4 ? (int)blockIdx.x : (int)(blockIdx.x >> 2);
-    const int rg = tile / P.nch, chunk = tile % P.nch;               // ceil(Wy / 4) nch tiles
-    extern __shared__ unsigned s_ent[];                               // BW 4: (Nz, 4 rows)
-    if constexpr (BW == 4) {
-        for (int i = threadIdx.x; i < 4 * P.Nz; i += NT) s_ent[i] = 0u;
-        __syncthreads();
-    }
-    // this tile's entries: row r of plane z at xr[z xs + r nch], rows r < nrow
-    // (BW 1 stores into them while it runs, BW 4 once at the end)
-    auto entries = [&](int& nrow, long long& xs, int*& xr) {
-        nrow = min(4, P.Wy - 4 * rg);
-        xs = (long long)P.Wy * P.nch;
-        xr = P.xrt + ((long long)blockIdx.y * P.Nz * P.Wy + 4 * rg) * P.nch + chunk;
-    };
-    int nrow = 0;
-    long long xs = 0;
-    int* xr = nullptr;
-    if constexpr (BW == 1) entries(nrow, xs, xr);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rg = blockIdx.x / P.nch, chunk = blockIdx.x % P.nch;   // grid: ceil(Wy / 4) nch
+    extern __shared__ unsigned s_ent[];                               // (Nz, 4 rows)
+    for (int i = threadIdx.x; i < 4 * P.Nz; i += KA_THREADS) s_ent[i] = 0u;
+    __syncthreads();
     const int y = 4 * rg + (lane >> 3), x = chunk * 32 + 8 * warp + (lane & 7);
     const bool row_ok = y < P.Wy;
     const int c = blockIdx.y, b = P.set0 + c;
@@ -329,23 +307,12 @@ __global__ void __launch_bounds__(32 * BW, (KZ <= 15 ? 32 : 16) / BW) ka_lines_l
         zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, s));
         zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, s));
     }
-    // byte `warp` of the entries of plane z, rows 4 rg + r (r < 4): in shared
-    // memory (BW 4) or in the table (BW 1, rows inside the window)
+    // byte `warp` of the entries of plane z, rows 4 rg + r (r < 4)
     auto put = [&](int z, unsigned m) {
-        if constexpr (BW == 4) {
-            unsigned char* e = reinterpret_cast<unsigned char*>(s_ent + 4 * z) + warp;
+        unsigned char* e = reinterpret_cast<unsigned char*>(s_ent + 4 * z) + warp;
 #pragma unroll
-            for (int r = 0; r < 4; ++r) e[4 * r] = (unsigned char)(m >> (8 * r));
-        } else {
-            unsigned char* e = reinterpret_cast<unsigned char*>(xr + z * xs) + warp;
-            for (int r = 0; r < nrow; ++r) e[4 * r * P.nch] = (unsigned char)(m >> (8 * r));
-        }
+        for (int r = 0; r < 4; ++r) e[4 * r] = (unsigned char)(m >> (8 * r));
     };
-    if constexpr (BW == 1) {
-        // planes outside [zlo, zhi] hold none of this warp's columns
-        for (int zo = lane; zo < P.Nz; zo += 32)
-            if (zo < zlo || zo > zhi) put(zo, 0u);
-    }
     if (zlo <= zhi) {
         float lz[KZ];
 #pragma unroll
@@ -394,14 +361,14 @@ __global__ void __launch_bounds__(32 * BW, (KZ <= 15 ? 32 : 16) / BW) ka_lines_l
             }
         }
     }
-    if constexpr (BW == 4) {
-        // the block's entries: every plane of its rows in the window
-        __syncthreads();
-        entries(nrow, xs, xr);
-        for (int i = threadIdx.x; i < nrow * P.Nz; i += NT) {
-            const int z = i / nrow, r = i - z * nrow;
-            xr[z * xs + r * P.nch] = (int)s_ent[4 * z + r];
-        }
+    // the block's entries: every plane of its rows in the window
+    __syncthreads();
+    const int nrow = min(4, P.Wy - 4 * rg);
+    const long long xs = (long long)P.Wy * P.nch;
+    int* xr = P.xrt + ((long long)c * P.Nz * P.Wy + 4 * rg) * P.nch + chunk;
+    for (int i = threadIdx.x; i < nrow * P.Nz; i += KA_THREADS) {
+        const int z = i / nrow, r = i - z * nrow;
+        xr[z * xs + r * P.nch] = (int)s_ent[4 * z + r];
     }
     if (P.counters && lane == 0) {
         atomicAdd(&P.counters[GBK_CTR_KA_SPAXEL], 32ull);
@@ -1145,7 +1112,7 @@ void ka_register_long(KaFn* t);
 // t[Kz / 2]: the two-chunk model kernel (ka_lines_lsf2)
 void ka2_register(KaFn* t);
 // t[Kz / 2]: the model kernel on 4 x 8 spaxel tiles (ka_lines_lsf_t)
-void ka_t_register(KaFn* t, bool tm, bool one_warp);
+void ka_t_register(KaFn* t, bool tm);
 // t[Kz / 2]: the LSF FIR of given model cubes
 typedef void (*KcFn)(BatchKernelArgs, const float*);
 void kc_register(KcFn* t);

@@ -377,8 +377,7 @@ typedef struct {
                              * warp on packed FP32 pairs; 2 = a warp per 4 x 8 spaxel tile
                              * (shorter channel unions); 3 = 2 with the range-table masks
                              * from one bit transpose per 32 planes instead of a ballot
-                             * per plane; 4 = 3 on one-warp blocks storing their mask
-                             * bytes to the range table directly (no block barrier) */
+                             * per plane */
 } gbkb200_batch_desc;
 
 int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);

@@ -282,8 +282,7 @@ def test_batched_cubes_match_disk_path(gpu):
 def test_batched_model_variant_identical(gpu, nodewise, ny):
     """The model kernel on two 32-column chunks per warp (packed FP32 pairs,
     each lane rounded as fmaf) and on 4 x 8 spaxel tiles (range-table masks
-    from per-plane ballots or from bit transposes, blocks of four warps or
-    of one) give bit-identical
+    from per-plane ballots or from bit transposes) give bit-identical
     chi^2 and models, with an odd number of chunks (the last warp's second
     chunk is absent), on the node-wise fast path and the generic trait path,
     and with a window height that is not a multiple of 4 (the last row
@@ -303,7 +302,7 @@ def test_batched_model_variant_identical(gpu, nodewise, ny):
         w.extra = dict(w.extra, truth=dict(w.extra['truth'], spt_p=30.0, spt_s=300.0))
     data, err, _ = synthetic_data(w)
     out = []
-    for variant in (0, 1, 2, 3, 4):
+    for variant in (0, 1, 2, 3):
         ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=n, chunk=4, conv='direct',
                            model_variant=variant)
         bufs = ev.alloc_inputs(n)
