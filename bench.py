@@ -66,9 +66,11 @@ def direct_flops_per_eval(geom):
 # one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of a 128-set
 # wave of this workload, divided by 128; a launch of n sets moves about n times
 # this (the traffic grows with the sets processed).  Not measured by this run.
+# The model kernel's figure is that of the 4x8-tile form (its variants 2 and
+# 3 store the same bytes).
 NCU_DRAM_BYTES_PER_SET = {
-    'kb_psf_residual': 289.5e6 / 128,
-    'ka_lines_lsf': 211.5e6 / 128,
+    'kb_psf_residual': 288.8e6 / 128,
+    'ka_lines_lsf': 169.7e6 / 128,
 }
 
 # FLOPs of one residual voxel computed from the model: (m - d), x w, r^2 sum
