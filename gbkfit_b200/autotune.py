@@ -110,7 +110,8 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
     # direct separable convolution (when the PSF is rank 1): chunk, then band
     best_d, best_dt = None, float('inf')
     for chunk in (32, 64, 128, 256, 512):
-        cfg = dict(fft_size=(0, 0, 0), chunk=chunk, rows_k1=16, conv='direct', band=0)
+        cfg = dict(fft_size=(0, 0, 0), chunk=chunk, rows_k1=16, conv='direct', band=0,
+                   model_variant=0)
         t = time_config(w, data, err, nsets, cfg)
         if t < best_dt:
             best_d, best_dt = cfg, t

@@ -112,7 +112,12 @@ class BatchedSMDisk:
 
     def __init__(self, disk, geom, data, error=None, mask=None, weight=1.0, max_sets=512,
                  chunk=0, fft_size=(0, 0, 0), rows_k1=0, rows_k5=0, conv='auto', band=0, device=0,
-                 stream=None, psf_variant=0, model_variant=0):
+                 stream=None, psf_variant=0, model_variant=None):
+        # the direct mode's model kernel: by default the 4 x 8 tile kernel with
+        # transposed range masks (3), which keeps 16 bytes per output plane in
+        # shared memory (up to 2048 planes); beyond that one chunk per warp (0)
+        if model_variant is None:
+            model_variant = 3 if geom.size[2] * 16 <= 32 * 1024 else 0
         if disk.traits['rht']:
             raise ValueError("the batched evaluator takes thin disks only")
         self.disk = disk

@@ -89,7 +89,9 @@ def test_headline_set_vs_fp64_oracle(headline, oracle_built, i):
                                  dict(chunk=512, psf_variant=3), dict(chunk=512, psf_variant=4),
                                  dict(chunk=512, psf_variant=5),
                                  dict(chunk=512, band=64, psf_variant=2),
+                                 dict(chunk=512, model_variant=0),
                                  dict(chunk=512, model_variant=1), dict(chunk=512, model_variant=2),
+                                 dict(chunk=512, model_variant=3),
                                  dict(chunk=128, model_variant=2, psf_variant=6),
                                  dict(chunk=512, psf_variant=6), dict(chunk=512, band=48, psf_variant=6),
                                  dict(chunk=128, psf_variant=6), dict(chunk=512, psf_variant=7),
