@@ -933,10 +933,10 @@ def main():
     ap.add_argument('--chunk', type=int, default=0, help='force the sets per wave (default: tuned)')
     ap.add_argument('--psf-variant', type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5, 6, 7],
                     help='PSF kernel variant of the direct mode (default: tuned)')
-    ap.add_argument('--model-variant', type=int, default=-1, choices=[-1, 0, 1, 2, 3],
+    ap.add_argument('--model-variant', type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4],
                     help='model kernel of the direct mode: 0 one chunk per warp, 1 chunk '
-                         'pairs, 2 4x8 spaxel tiles, 3 tiles with transposed range masks '
-                         '(default: tuned)')
+                         'pairs, 2 4x8 spaxel tiles, 3 tiles with transposed range masks, '
+                         '4 as 3 with the scaled line exponent (default: tuned)')
     ap.add_argument('--band', type=int, default=0,
                     help='force the output rows per PSF block of the direct mode (default: tuned)')
     ap.add_argument('--workload', default='smdisk_batch128',

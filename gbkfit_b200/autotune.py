@@ -14,7 +14,8 @@ Knobs (all change speed only, never results beyond fp32 rounding):
 * ``model_variant``: the direct mode's model kernel (0: one 32-column chunk
   per warp; 1: two chunks per warp on packed FP32 pairs; 2: a 4 x 8 spaxel
   tile per warp; 3: 2 with the range-table masks by bit transposes; the
-  same values);
+  same values; 4: 3 with the line exponent from one multiply-add, the same
+  values up to fp32 rounding);
 * ``rows_k1``: spectral rows per shared-memory group of the model kernel.
 
 Coordinate descent from the defaults; every trial builds an evaluator and
@@ -132,7 +133,7 @@ def tune_batched(w, data, err, nsets, budget_s=60.0, use_cache=True):
                 best_d, best_dt = cfg, t
         # the model kernel's variants
         base = dict(best_d)
-        for mv in (1, 2, 3):
+        for mv in (1, 2, 3, 4):
             cfg = dict(base, model_variant=mv)
             t = time_config(w, data, err, nsets, cfg)
             if t < best_dt:

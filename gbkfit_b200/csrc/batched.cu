@@ -411,15 +411,17 @@ static KaFn ka_fn(int Kz)
     return t[Kz / 2];
 }
 
-static KaFn ka_t_fn(int Kz, bool tm)
+// form 0: ballot masks, 1: transposed masks, 2: transposed masks and the scaled line
+static KaFn ka_t_fn(int Kz, int form)
 {
-    static KaFn t[2][KA_KMAX / 2 + 1] = {};
+    static KaFn t[3][KA_KMAX / 2 + 1] = {};
     static std::once_flag once;
     std::call_once(once, [] {
-        ka_t_register(t[0], false);
-        ka_t_register(t[1], true);
+        ka_t_register(t[0], false, false);
+        ka_t_register(t[1], true, false);
+        ka_t_register(t[2], true, true);
     });
-    return t[tm ? 1 : 0][Kz / 2];
+    return t[form][Kz / 2];
 }
 
 static KaFn ka2_fn(int Kz)
@@ -567,13 +569,14 @@ static int setup_direct(gbkb200_batch* bt, const gbkb200_batch_desc* d)
     k_iw<<<592, 256, 0, bt->ctx->stream>>>(P, bt->iw, (long long)P.Nz * P.Ny * P.Nx);
     GBK_CUDA_TRY(cudaGetLastError());
     GBK_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));
-    if (d->model_variant < 0 || d->model_variant > 3) return GBKB200_ERR_INVALID_ARG;
-    // variants 2 and 3 (4 x 8 tiles) keep a plane's entries of its 4 rows in
-    // shared memory; 3 forms the masks by bit transposes
+    if (d->model_variant < 0 || d->model_variant > 4) return GBKB200_ERR_INVALID_ARG;
+    // variants 2-4 (4 x 8 tiles) keep a plane's entries of its 4 rows in
+    // shared memory; 3 forms the masks by bit transposes; 4 is 3 with the
+    // scaled line exponent
     const bool tiles = d->model_variant >= 2;
     if (tiles && (long long)P.Nz * 16 > 32 * 1024) return GBKB200_ERR_UNSUPPORTED;
     bt->ka = d->model_variant == 1 ? ka2_fn(P.Kz)
-             : tiles               ? ka_t_fn(P.Kz, d->model_variant == 3)
+             : tiles               ? ka_t_fn(P.Kz, d->model_variant - 2)
                                    : ka_fn(P.Kz);
     bt->ka_variant = d->model_variant;
     bt->kb = kb_fn(P.K, d->psf_variant);

@@ -263,7 +263,11 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf(B
 // of 32 planes gets its masks at once, every lane forming its output range
 // as a 32-bit row and the warp transposing the 32 rows (plane_masks32): the
 // same masks for a few instructions per group instead of several per plane.
-template<int KZ, bool TM>
+// SL (scaled line): the exponent as -t^2 with t = zf (dz s) + (z0 - v) s and
+// s = sqrt(log2(e) / (2 sigma^2)), one multiply-add and one multiply per
+// channel instead of a multiply-add, an add and two multiplies; the same line
+// up to fp32 rounding (not bit-identical to the other forms).
+template<int KZ, bool TM, bool SL = false>
 __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf_t(BatchKernelArgs P, int* status)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -291,10 +295,17 @@ __global__ void __launch_bounds__(KA_THREADS, (KZ <= 15 ? 8 : 4)) ka_lines_lsf_t
     }
     const float v = o.vv, z0 = a.spec_zero, dz = a.spec_step;
     const unsigned wlen = (unsigned)hi - (unsigned)lo;
+    const float sc = SL ? sqrtf(rinv) : 0.f;
+    const float dzs = dz * sc, cs = (z0 - v) * sc;
     auto line_f = [&](int z, float zf) {
-        const float d = (z0 + zf * dz) - v;
         float e;
-        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-(d * d) * rinv));
+        if constexpr (SL) {
+            const float t = fmaf(zf, dzs, cs);
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-(t * t)));
+        } else {
+            const float d = (z0 + zf * dz) - v;
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-(d * d) * rinv));
+        }
         return (unsigned)z - (unsigned)lo <= wlen ? amp * e : 0.f;
     };
     auto line = [&](int z) { return line_f(z, (float)z); };
@@ -1112,7 +1123,7 @@ void ka_register_long(KaFn* t);
 // t[Kz / 2]: the two-chunk model kernel (ka_lines_lsf2)
 void ka2_register(KaFn* t);
 // t[Kz / 2]: the model kernel on 4 x 8 spaxel tiles (ka_lines_lsf_t)
-void ka_t_register(KaFn* t, bool tm);
+void ka_t_register(KaFn* t, bool tm, bool sl);
 // t[Kz / 2]: the LSF FIR of given model cubes
 typedef void (*KcFn)(BatchKernelArgs, const float*);
 void kc_register(KcFn* t);

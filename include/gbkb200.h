@@ -371,13 +371,15 @@ typedef struct {
                              * copied in while the previous item runs); 7 = 0 on
                              * 256-thread blocks with twice the shared memory (2 blocks
                              * per SM); 0 = the first */
-    int model_variant;      /* direct mode, the model kernel (all give the same values):
+    int model_variant;      /* direct mode, the model kernel (0-3 give the same values):
                              * 0 = a warp per 32-column chunk stepping every lane through
                              * the union of the lanes' channel windows; 1 = two chunks per
                              * warp on packed FP32 pairs; 2 = a warp per 4 x 8 spaxel tile
                              * (shorter channel unions); 3 = 2 with the range-table masks
                              * from one bit transpose per 32 planes instead of a ballot
-                             * per plane */
+                             * per plane; 4 = 3 with the line's exponent as -t^2, t one
+                             * multiply-add per channel (the same values up to fp32
+                             * rounding) */
 } gbkb200_batch_desc;
 
 int gbkb200_batch_create(gbkb200_ctx* ctx, const gbkb200_batch_desc* desc, gbkb200_batch** out);

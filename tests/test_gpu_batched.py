@@ -361,3 +361,43 @@ def test_timing_modes_and_counters(gpu):
     assert c['lsf_fma'] > 0 and c['lines'] > 0
     torch.testing.assert_close(timed, plain, rtol=0, atol=0)
     torch.testing.assert_close(counted, plain, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize('nodewise', [True, False])
+def test_batched_model_variant_scaled_line(gpu, oracle_built, nodewise):
+    """The tile model kernel with the line's exponent as -t^2 (t one
+    multiply-add per channel) matches the kernel with the exponent from the
+    velocity difference within fp32 rounding, and the fp64 oracle."""
+    import torch
+    from oracle.oracle import scube_pipeline
+    from gbkfit_b200 import traits as T
+    from gbkfit_b200 import workloads
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    from gbkfit_b200.disk import Disk
+    n = 5
+    w = workloads.smdisk_batch128(nsets=n, size=(64, 62, 48), nnodes=16)
+    if not nodewise:
+        w.disk = Disk(False, False, w.disk.rnodes, traits=dict(
+            rpt=[T.bpt('nw_uniform')], vpt=[T.vpt('nw_tan_uniform')], dpt=[T.dpt('nw_uniform')],
+            spt=[T.spt('azrange')]))
+        w.params = dict(w.params, spt_p=np.full(n, 30.0), spt_s=np.full(n, 300.0))
+        w.extra = dict(w.extra, truth=dict(w.extra['truth'], spt_p=30.0, spt_s=300.0))
+    data, err, _ = synthetic_data(w)
+    out = []
+    for variant in (3, 4):
+        ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=n, chunk=4, conv='direct',
+                           model_variant=variant)
+        bufs = ev.alloc_inputs(n)
+        ev.upload(ev.pack(w.params, n), bufs, n)
+        model = torch.zeros((n,) + tuple(w.geom.size[::-1]), device='cuda')
+        chi2 = ev.evaluate_device(bufs, n, model=model).cpu().numpy().copy()
+        out.append((chi2, model.cpu().numpy()))
+        ev.close()
+    (c3, m3), (c4, m4) = out
+    assert np.all(np.abs(c4 - c3) <= 1e-5 * np.abs(c3)), (c3, c4)
+    for i in range(n):
+        assert np.abs(m4[i] - m3[i]).max() <= 1e-5 * np.abs(m3[i]).max(), i
+        p = w.disk.pack(workloads.set_params(w, i))
+        ref64 = scube_pipeline(p, w.geom, precision='f64')
+        ref32 = scube_pipeline(p, w.geom, precision='f32')
+        assert rel_err(m4[i], ref64) <= max(1e-5, 1.5 * rel_err(ref32, ref64)), i
