@@ -62,9 +62,13 @@ _lib.gbkb200_batch_timing.restype = c_int
 _lib.gbkb200_batch_counters.argtypes = [c_void_p, ctypes.c_ulonglong * 8]
 _lib.gbkb200_batch_counters.restype = c_int
 
+_lib.gbkb200_rows_from_nodes.argtypes = [c_void_p, c_int, c_int] + [c_void_p] * 6 + [
+    c_int, c_void_p, c_void_p]
+_lib.gbkb200_rows_from_nodes.restype = c_int
+
 BATCH_EXPORTED = ['gbkb200_batch_create', 'gbkb200_batch_evaluate', 'gbkb200_batch_info',
                   'gbkb200_batch_destroy', 'gbkb200_batch_set_timing', 'gbkb200_batch_timing',
-                  'gbkb200_batch_counters']
+                  'gbkb200_batch_counters', 'gbkb200_rows_from_nodes']
 
 # slots of gbkb200_batch_counters
 COUNTERS = ('lsf_fma', 'lines', 'psf_x_fma', 'psf_y_fma', 'residual_voxels', 'spaxels')
@@ -242,7 +246,11 @@ class BatchedSMDisk:
     def evaluate(self, params, nsets, pieces=None):
         """Host parameters -> host chi^2 (numpy), end to end.
 
-        The batch is split into pieces; each piece is packed into its own
+        With linear node interpolation (and pieces not given) the raw
+        parameter values of all sets are copied to the device in one transfer
+        and the input rows are built there (gbkb200_rows_from_nodes), so the
+        whole batch is evaluated as one piece.  Otherwise the batch is split
+        into pieces; each piece is packed into its own
         pinned host buffer, copied to the device in one transfer and
         evaluated asynchronously while the next piece is packed; chi^2 comes
         back through a pinned buffer and the call synchronises once.
@@ -254,6 +262,10 @@ class BatchedSMDisk:
         nsets = int(nsets)
         if nsets > self.max_sets:
             raise ValueError(f"nsets {nsets} > max_sets {self.max_sets}")
+        nd = self._node_rows() if pieces is None else None
+        if nd is not None and not all(np.ndim(params[p]) >= 1 and np.shape(params[p])[0] == nsets
+                                      for p in nd['raw']):
+            nd = None
         if pieces is None:
             if nsets >= 256:
                 first = max(32, nsets // 8 // 32 * 32)
@@ -268,6 +280,8 @@ class BatchedSMDisk:
             sizes = [int(s) for s in pieces]
             if sum(sizes) != nsets or min(sizes) < 1:
                 raise ValueError(f"piece sizes {sizes} do not make {nsets} sets")
+        if nd is not None:
+            return self._evaluate_nodes(nd, params, nsets)
         bounds = np.concatenate([[0], np.cumsum(sizes)]).astype(int)
         st = self._e2e_buffers(max(sizes), len(sizes))
         per_set = {k: (np.ndim(v) > 0 and np.shape(v)[0] == nsets) for k, v in params.items()}
@@ -286,6 +300,52 @@ class BatchedSMDisk:
                 self.last_h2d_bytes += hflat.numel() * 4
                 self.evaluate_device(dv, hi - lo, chi2=self.chi2[lo:hi])
             out = st['chi2'][:nsets]
+            out.copy_(self.chi2[:nsets], non_blocking=True)
+        self.stream.synchronize()
+        return out.numpy().copy()
+
+    def _node_rows(self):
+        """Tables (node_row_tables) and buffers of the device-side row
+        assembly, built once; None unless the disk interpolates linearly."""
+        if hasattr(self, '_nodes'):
+            return self._nodes
+        self._nodes = None
+        n = self.max_sets
+        tb = node_row_tables(self.disk, n)
+        if tb is None:
+            return None
+        k0, k1, w0, w1, base, stride = (tb[k] for k in ('k0', 'k1', 'w0', 'w1', 'base', 'stride'))
+        raw, nraw, blocks, start = tb['raw'], tb['nraw'], tb['blocks'], tb['total']
+        dev = self.dev
+        dflat = torch.empty(max(1, n * start), dtype=torch.float32, device=dev)
+        dv = {name: dflat[n * s0:n * (s0 + w)].view(n, w) for name, s0, w in blocks}
+        hraw = torch.empty((n, nraw), dtype=torch.float64, pin_memory=True)
+        t = {k: torch.from_numpy(v) for k, v in
+             dict(k0=k0, k1=k1, w0=w0, w1=w1, base=base, stride=stride).items()}
+        self._nodes = dict(raw=raw, nraw=nraw, width=len(k0), hraw=hraw, hraw_np=hraw.numpy(),
+                           draw=torch.empty((n, nraw), dtype=torch.float64, device=dev),
+                           tables={k: v.to(dev) for k, v in t.items()}, host_tables=t,
+                           dflat=dflat, dv=dv,
+                           chi2=torch.empty(n, dtype=torch.float32, pin_memory=True))
+        return self._nodes
+
+    def _evaluate_nodes(self, nd, params, nsets):
+        """evaluate() through the device-side row assembly (one piece)."""
+        hr = nd['hraw_np'][:nsets]
+        for pname, (ro, nin) in nd['raw'].items():
+            hr[:, ro:ro + nin] = np.asarray(params[pname], np.float64).reshape(nsets, nin)
+        t = nd['tables']
+        with torch.cuda.stream(self.stream):
+            nd['draw'][:nsets].copy_(nd['hraw'][:nsets], non_blocking=True)
+            self.last_h2d_bytes = nsets * nd['nraw'] * 8
+            check(_lib.gbkb200_rows_from_nodes(
+                nd['draw'].data_ptr(), nd['nraw'], nsets, t['k0'].data_ptr(),
+                t['k1'].data_ptr(), t['w0'].data_ptr(), t['w1'].data_ptr(),
+                t['base'].data_ptr(), t['stride'].data_ptr(), nd['width'],
+                nd['dflat'].data_ptr(), c_void_p(self.stream.cuda_stream)),
+                'gbkb200_rows_from_nodes')
+            self.evaluate_device(nd['dv'], nsets)
+            out = nd['chi2'][:nsets]
             out.copy_(self.chi2[:nsets], non_blocking=True)
         self.stream.synchronize()
         return out.numpy().copy()
@@ -509,6 +569,60 @@ def row_plan(disk):
         plan.append((kind, [(pname, size, nw, interp) for pname, size, nw in tab['plist']],
                      tab['npv']))
     return plan
+
+
+def node_row_tables(disk, n):
+    """The device-side row assembly's tables for a disk and a flat buffer of
+    n sets (None unless the disk interpolates linearly): the raw layout
+    {parameter: (offset, values per set)} of nraw values per set, and per
+    output column j its raw indices k0, k1 and weights w0, w1 (the two
+    weights of a sub-node's linear interpolation, the matrix pack_batch
+    multiplies by, or 1 and 0 for a value taken as it is), its flat offset
+    base (the name's block of n rows, then the column) and row stride; the
+    name blocks (name, first column, width) and the columns per set."""
+    if disk.interp != 'linear':
+        return None
+    from .disk import _linear_matrix
+    wm = _linear_matrix(disk.rnodes, disk.subrnodes)
+    raw, nraw = {}, 0
+    k0, k1, w0, w1, base, stride, blocks = [], [], [], [], [], [], []
+    start = 0
+    for name, entries, width in row_plan(disk):
+        col = 0
+        for pname, size, nw, _ in entries:
+            nin = wm.shape[0] if nw else size
+            if pname not in raw:
+                raw[pname] = (nraw, nin)
+                nraw += nin
+            ro = raw[pname][0]
+            if nw:
+                cols = []
+                for c in range(wm.shape[1]):
+                    nz = np.nonzero(wm[:, c])[0]
+                    if len(nz) > 2:
+                        return None
+                    i0 = int(nz[0]) if len(nz) else 0
+                    i1 = int(nz[1]) if len(nz) > 1 else i0
+                    cols.append((ro + i0, ro + i1, wm[i0, c] if len(nz) else 0.0,
+                                 wm[i1, c] if len(nz) > 1 else 0.0))
+            else:
+                cols = [(ro + c, ro + c, 1.0, 0.0) for c in range(size)]
+            for a, b, wa, wb in cols:
+                k0.append(a)
+                k1.append(b)
+                w0.append(wa)
+                w1.append(wb)
+                base.append(n * start + col)
+                stride.append(width)
+                col += 1
+        if col != width:
+            return None
+        blocks.append((name, start, width))
+        start += width
+    return dict(raw=raw, nraw=nraw, k0=np.asarray(k0, np.int32), k1=np.asarray(k1, np.int32),
+                w0=np.asarray(w0, np.float64), w1=np.asarray(w1, np.float64),
+                base=np.asarray(base, np.int64), stride=np.asarray(stride, np.int32),
+                blocks=blocks, total=start)
 
 
 def synthetic_data(w, device=0, seed=None):

@@ -428,6 +428,19 @@ int gbkb200_batch_info(const gbkb200_batch* b, int fft_size[3], int* chunk, size
                        int* conv_mode);
 int gbkb200_batch_destroy(gbkb200_batch* b);
 
+/* The batched evaluator's input rows from raw node values, on the device
+ * (replaces the host packing of the trait parameter arrays,
+ * gmodels/_disk.py:42-156, when the node -> sub-node interpolation is
+ * linear): for sets b < nsets and columns j < width,
+ *   out[base[j] + b stride[j]] = (float)(w0[j] raw[b raw_width + k0[j]]
+ *                                        + w1[j] raw[b raw_width + k1[j]])
+ * in fp64.  raw, the tables and out are device memory; enqueued on stream
+ * (a cudaStream_t), nothing is synchronised or allocated. */
+int gbkb200_rows_from_nodes(const double* raw, int raw_width, int nsets, const int* k0,
+                            const int* k1, const double* w0, const double* w1,
+                            const long long* base, const int* stride, int width, float* out,
+                            void* stream);
+
 /* Per-stage device timing (no reference counterpart; a measurement aid).
  * With timing enabled, evaluate records a CUDA event pair around every kernel
  * launch; do not capture evaluate into a graph while it is enabled.  Stages:

@@ -401,3 +401,23 @@ def test_batched_model_variant_scaled_line(gpu, oracle_built, nodewise):
         ref64 = scube_pipeline(p, w.geom, precision='f64')
         ref32 = scube_pipeline(p, w.geom, precision='f32')
         assert rel_err(m4[i], ref64) <= max(1e-5, 1.5 * rel_err(ref32, ref64)), i
+
+
+def test_evaluate_rows_from_nodes_matches_host_packing(gpu):
+    """evaluate() with the input rows built on the device from the raw node
+    values (linear interpolation) gives the chi^2 of the host-packed path,
+    on repeated calls and on a batch smaller than the evaluator's capacity."""
+    from gbkfit_b200.batched import BatchedSMDisk, synthetic_data
+    n = 40
+    w = _small_batch_workload(n)
+    data, err, _ = synthetic_data(w)
+    ev = BatchedSMDisk(w.disk, w.geom, data, err, max_sets=48, chunk=32, conv='direct')
+    got = ev.evaluate(w.params, n)
+    assert ev._node_rows() is not None
+    assert ev.last_h2d_bytes == n * ev._node_rows()['nraw'] * 8
+    ref = ev.evaluate(w.params, n, pieces=1)
+    np.testing.assert_allclose(got, ref, rtol=1e-6, atol=0)
+    assert np.array_equal(ev.evaluate(w.params, n), got)
+    sub = {k: (np.asarray(v)[:9] if np.ndim(v) and np.shape(v)[0] == n else v)
+           for k, v in w.params.items()}
+    np.testing.assert_allclose(ev.evaluate(sub, 9), got[:9], rtol=1e-6, atol=0)
