@@ -273,9 +273,10 @@ def autotune(w, data, err, nsets, budget_s=60.0):
 
 def run_e2e(args, w, data, err, cfg, nsets, total, world, local):
     """The same metric through the public API: every rank takes the whole batch
-    of host parameter dicts, packs and copies its share (pinned H2D),
-    evaluates it, reads its chi^2 back (D2H) and gathers all chi^2 values
-    (NCCL all_gather across the ranks)."""
+    of host parameter dicts, copies its share's raw parameter values (pinned
+    H2D; the input rows are built on the device), evaluates it, reads its
+    chi^2 back (D2H) and gathers all chi^2 values (NCCL all_gather across the
+    ranks)."""
     import torch
     from gbkfit_b200.batched import BatchedSMDisk
     from gbkfit_b200.sharded import ShardedEvaluator
